@@ -1,0 +1,114 @@
+"""Regenerate the golden fixtures from the reference X-TED_CPU.
+
+Run in a container that holds the reference tree (read at /root/reference)
+after ``make -C oracle all ref``:
+
+    python tests/golden/make_golden.py datasets    # -> datasets.json.gz
+    python tests/golden/make_golden.py synthetic   # -> synthetic.json.gz
+
+datasets: tree pair (0, 1) of every file of the reference's sampled datasets
+  (Sampled_Dataset/*, Sampled_Dataset_Extra_Large_Trees/*), which is the pair the
+  reference CLI computes (X-TED_CPU/TED_test.cpp:31). Labels are interned to
+  int ids per pair; the expected distance is the reference's own
+  ``standard_ted`` on the ORIGINAL label strings, cross-checked for the small
+  files against the ``The distance = d`` line of the reference CLI built from
+  the same sources.
+
+synthetic: seeded trees from the product generator (all four shapes, sizes
+  1..400, both label alphabets), expected distances from the reference
+  ``standard_ted`` on decimal-string labels.
+
+Every tree is stored as {"labels": [...], "parent": [...]} in preorder.
+"""
+from __future__ import annotations
+
+import glob
+import gzip
+import json
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "x-ted_b200"))
+
+import oracle  # noqa: E402
+from xted import trees  # noqa: E402
+
+REF = "/root/reference"
+
+
+def _tree_json(t):
+    return {"labels": t.labels.tolist(), "parent": t.parent().tolist()}
+
+
+def _cli_distance(lab_path, adj_path):
+    exe = os.path.join(REPO, "oracle", "_ref", "X-TED_CPU")
+    out = subprocess.run([exe, "8", lab_path, adj_path], capture_output=True, text=True,
+                         check=True).stdout
+    ds = [int(l.split("=")[1]) for l in out.splitlines() if l.startswith("The distance =")]
+    assert len(set(ds)) == 1, ds
+    return ds[0]
+
+
+def datasets():
+    files = sorted(glob.glob(os.path.join(REF, "Sampled_Dataset", "*", "*_nodes*.txt")))
+    files += sorted(glob.glob(os.path.join(REF, "Sampled_Dataset_Extra_Large_Trees", "*", "*",
+                                           "*_nodes_*.txt")))
+    cases = []
+    for lab in files:
+        base = os.path.basename(lab)
+        if "_adj" in base or "synthetic_tree" in base:
+            continue
+        adj = lab.replace("_nodes_", "_nodes_adj_") if "_nodes_" in base else \
+            lab.replace("_nodes.txt", "_nodes_adj.txt")
+        a, b, sa, sb = trees.load_pair(lab, adj, 0, 1)
+        assert trees.is_preorder(a) and trees.is_preorder(b), lab
+        d, _ = oracle.ref_distance_str(sa, a, sb, b, num_threads=8)
+        small = max(a.n, b.n) <= 1200
+        if small:
+            assert _cli_distance(lab, adj) == d, lab
+        name = os.path.relpath(lab, REF)
+        cases.append({"name": name, "a": _tree_json(a), "b": _tree_json(b), "distance": d,
+                      "cli_checked": small})
+        print(f"{name}: m={a.n} n={b.n} d={d}", flush=True)
+    with gzip.open(os.path.join(HERE, "datasets.json.gz"), "wt") as f:
+        json.dump({"source": "reference X-TED_CPU standard_ted, tree pair (0,1)", "cases": cases}, f)
+
+
+def synthetic():
+    from xted import gen  # product generator (needs the built library)
+    cases = []
+    seed = 20261203
+    shapes = ["random", "wide", "deep", "caterpillar"]
+    sizes = [1, 2, 3, 5, 8, 13, 21, 34, 55, 100, 150, 250, 400]
+    k = 0
+    for si, sa in enumerate(shapes):
+        for sb in shapes:
+            for na in sizes:
+                nb = sizes[(sizes.index(na) * 7 + si + 3) % len(sizes)]
+                alpha = 4 if k % 3 == 0 else (26 if k % 3 == 1 else 1000)
+                a = gen.tree(sa, na, seed + 2 * k, labels="uniform", alphabet=alpha)
+                b = gen.tree(sb, nb, seed + 2 * k + 1, labels="uniform", alphabet=alpha)
+                d, _ = oracle.ref_distance(a, b, num_threads=4)
+                cases.append({"name": f"{sa}{na}-{sb}{nb}-a{alpha}", "a": _tree_json(a),
+                              "b": _tree_json(b), "distance": d})
+                k += 1
+    # the plain single-pair workload: two 100-node random recursive trees, 26 labels
+    a = gen.tree("random", 100, 1, labels="uniform", alphabet=26)
+    b = gen.tree("random", 100, 2, labels="uniform", alphabet=26)
+    d, _ = oracle.ref_distance(a, b, num_threads=4)
+    cases.append({"name": "single-pair-100x100-seed1-2", "a": _tree_json(a), "b": _tree_json(b),
+                  "distance": d})
+    with gzip.open(os.path.join(HERE, "synthetic.json.gz"), "wt") as f:
+        json.dump({"source": "reference X-TED_CPU standard_ted on generator trees", "cases": cases},
+                  f)
+    print(f"{len(cases)} synthetic cases")
+
+
+if __name__ == "__main__":
+    what = sys.argv[1:] or ["datasets", "synthetic"]
+    for w in what:
+        {"datasets": datasets, "synthetic": synthetic}[w]()
