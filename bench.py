@@ -1,0 +1,350 @@
+"""Benchmark of the tree-edit-distance path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xted|reference]
+                    [--workload batched|single100|single1000|single20000]
+
+Default workload (the headline): 4,096 pairs, tree sizes log-uniform in
+[50, 2000], shapes uniform over {random recursive, wide-shallow, deep-narrow,
+caterpillar}, labels Zipf(1.1) over 1,000 ids (seeded synthetic stand-in; the
+reference publishes no dataset for it). A step is one pass of the DP over the
+whole batch.
+
+* value: pairs/s of the batched persistent launch with inputs resident in HBM
+  (xted_prepare_batch once, then K x xted_run_prepared), device time from CUDA
+  events on the launching stream, max over ranks; the distance tables
+  (several GB) exceed L2, so no flush is needed between steps.
+* e2e: the same metric through the public batch call from host trees
+  (planning, host->device copy of the step's inputs from pinned memory, DP,
+  device->host copy of the distances), wall clock per step.
+* plain_per_pair: one pair per call (xted_distance), on a strided sample.
+* cpu_baseline: the reference X-TED_CPU (oracle/_ref, its own standard_ted,
+  all host cores, pairs in sequence as the reference runs them) on a strided
+  sample, rank 0 at N = 1 only.
+
+Multi-GPU (torchrun): every rank runs its own 4,096-pair batch (pairs are
+independent; no data-path collective), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "x-ted_b200"))
+
+METRIC = "pairs/s + forest-DP GCUPS, batched vs plain per-pair on 1 B200; serve p99 ms"
+BYTES_PER_CELL = 4  # one 4-byte tree-distance read (forest cell) or write (tree cell)
+
+
+def _peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_from_profile():
+    """Per-launch DRAM traffic of the DP kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "xted_dp_kernel_batched.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(float(line.split(":", 1)[1].strip()))
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(name: str, rank: int):
+    from xted import gen
+    if name == "batched":
+        return gen.mixed_batch(4096, seed=4 + 1000 * rank), {
+            "workload": "4096 mixed pairs, sizes log-uniform 50-2000, 4 shapes, Zipf(1.1) over 1000 labels",
+            "npairs": 4096, "seed": 4 + 1000 * rank}
+    if name == "single100":
+        return [gen.single_pair_100()], {"workload": "one pair, 100 vs 100 random recursive, 26 labels"}
+    if name == "single1000":
+        return [gen.single_pair_1000()], {"workload": "one pair, 1000 wide-shallow vs 1000 deep-narrow, "
+                                                       "Zipf(1.1) over 10000 labels"}
+    if name == "single20000":
+        return [gen.single_pair_20000(shape="random"), gen.single_pair_20000(shape="caterpillar")], {
+            "workload": "20000 vs 20000 random recursive + 20000 vs 20000 caterpillar, 64 labels"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference(pairs, budget_s: float, stride: int):
+    """The reference X-TED_CPU on a strided sample, all host cores per pair
+    (pairs in sequence, the reference's own mode). Returns (pairs/s, info)."""
+    import oracle
+    ncpu = os.cpu_count() or 1
+    sample = pairs[::stride]
+    if oracle.ref_available():
+        kind = "reference"
+
+        def run(a, b):
+            return oracle.ref_distance(a, b, num_threads=ncpu)[0]
+    else:
+        kind = "port"
+        ncpu = 1
+
+        def run(a, b):
+            return oracle.distance(a, b)
+    done = 0
+    t0 = time.perf_counter()
+    for a, b in sample:
+        run(a, b)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return done / dt, {"kind": kind, "cores": ncpu, "pairs": done, "seconds": round(dt, 3),
+                       "sample": f"every {stride}th pair of the workload, first {done} "
+                                 f"(time budget {budget_s:.0f} s), pairs in sequence, "
+                                 f"{ncpu} threads per pair"}
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    pairs, cfg = make_workload(args.workload, 0)
+    stride = 32 if len(pairs) > 256 else 1
+    for _ in range(args.warmup):
+        cpu_reference(pairs[:1], 30.0, 1)
+    vals = []
+    info = None
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        v, info = cpu_reference(pairs, args.ref_budget, stride)
+        vals.append(v)
+    wall = time.perf_counter() - t_all
+    value = statistics.mean(vals)
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * wall / args.steps, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+           "data": "synthetic", "config": cfg,
+           "cpu_baseline": {"value": round(value, 3), "unit": "pairs/s", "cores": info["cores"],
+                            "kind": info["kind"], "sample": info["sample"]},
+           "e2e": {"value": round(value, 3), "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="xted", choices=["xted", "reference"])
+    ap.add_argument("--workload", default="batched")
+    ap.add_argument("--plain-stride", type=int, default=16)
+    ap.add_argument("--ref-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import xted
+    pairs, cfg = make_workload(args.workload, rank)
+    ctx = xted.Context(device=local)
+    npairs = len(pairs)
+
+    # ---- device-resident throughput (value) ----
+    ctx.prepare_batch(pairs)
+    plan_ms = ctx.stats()["host_plan_ms"]
+    for _ in range(max(args.warmup, 3)):
+        ref_out = ctx.run_prepared()
+    import torch
+    barrier(world)
+    torch.cuda.synchronize()
+    dev_ms, dp_ms = 0.0, 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            out = ctx.run_prepared()
+            st = ctx.stats()
+            dev_ms += st["device_ms"]
+            dp_ms += st["dp_ms"]
+            assert (out == ref_out).all(), "results changed between steps"
+    torch.cuda.synchronize()
+    barrier(world)
+    dev_ms_max = reduce_max(dev_ms, world)
+    value = npairs * world * args.steps / (dev_ms_max / 1000.0)
+    cells = st["cells"]
+    gcups = reduce_sum(cells, world) * args.steps / (dev_ms_max / 1000.0) / 1e9
+
+    # ---- end to end through the public batch call ----
+    ctx.distance_batch(pairs)
+    barrier(world)
+    torch.cuda.synchronize()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        got = ctx.distance_batch(pairs)
+        e2e_s += time.perf_counter() - t0
+        assert (got == ref_out).all()
+    st_e2e = ctx.stats()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_max = reduce_max(e2e_s, world)
+    e2e_value = npairs * world * args.steps / e2e_max
+
+    # ---- plain per-pair path on a strided sample ----
+    plain = None
+    if npairs > 1 and args.plain_stride > 0:
+        sample = pairs[::args.plain_stride]
+        for a, b in sample[:2]:
+            ctx.distance(a, b)
+        t0 = time.perf_counter()
+        pdev = 0.0
+        for a, b in sample:
+            ctx.distance(a, b)
+            pdev += ctx.stats()["device_ms"]
+        pw = time.perf_counter() - t0
+        plain = {"pairs_per_s": round(len(sample) / pw, 2), "device_pairs_per_s": round(len(sample) / (pdev / 1e3), 2),
+                 "sample": f"every {args.plain_stride}th pair ({len(sample)} pairs), one xted_distance call each"}
+
+    # ---- CPU baseline (reference X-TED_CPU), rank 0 at N = 1 ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        stride = 32 if npairs > 256 else 1
+        v, info = cpu_reference(pairs, args.ref_budget, stride)
+        cpu = {"value": round(v, 3), "unit": "pairs/s", "cores": info["cores"], "kind": info["kind"],
+               "sample": info["sample"]}
+
+    if rank != 0:
+        return
+    peak, peak_src = _peaks()
+    kernel_s = dp_ms / args.steps / 1000.0
+    achieved = cells * BYTES_PER_CELL / kernel_s / 1e9
+    traffic = _traffic_from_profile()
+    res = {
+        "metric": METRIC, "value": round(value, 2), "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": dict(cfg, l2="distance tables exceed L2 (no flush)", parallelism=f"pairs sharded, dp{world}"),
+        "gcups": round(gcups, 2), "cells_per_step": cells, "cells_right_path": st["cells_right"],
+        "e2e": {"value": round(e2e_value, 2), "unit": "pairs/s", "h2d_bytes_per_step": st_e2e["h2d_bytes"],
+                "d2h_bytes_per_step": st_e2e["d2h_bytes"], "host_plan_ms": round(st_e2e["host_plan_ms"], 2)},
+        "plain_per_pair": plain,
+        "batched_vs_plain": round(value / plain["device_pairs_per_s"], 2) if plain else None,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "xted_dp_kernel", "bytes_per_cell": BYTES_PER_CELL},
+        "cpu_baseline": cpu,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "tasks": st["tasks"], "units": st["units"], "grid": st["grid"], "host_plan_ms": round(plan_ms, 2),
+    }
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

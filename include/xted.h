@@ -1,0 +1,149 @@
+/*
+ * xted.h -- C ABI of the B200-native unit-cost tree edit distance library.
+ *
+ * Drop-in for the reference X-TED entry point
+ *   int standard_ted(vector<string>& x_node, vector<vector<int>>& x_adj,
+ *                    vector<string>& y_node, vector<vector<int>>& y_adj,
+ *                    int num_threads, int parallel_version)
+ * (X-TED_CPU/TED.cpp:177, declared X-TED_CPU/TED_C++.h:21; GPU twin
+ * X-TED_GPU/TED.cu:116, X-TED_GPU/TED_C++.h:28), re-expressed as plain C:
+ * pointers and sizes only. A C++ wrapper with the reference's exact signature
+ * is in include/xted.hpp.
+ *
+ * Trees are ordered, labelled and numbered in preorder (root = 0), the
+ * reference's input contract (README.md:31-44). Children of node v are
+ * child_idx[child_off[v] .. child_off[v+1]) in left-to-right order. Labels
+ * are int32 ids; the reference only tests label strings for equality
+ * (X-TED_CPU/TED.cpp:153-159), so interning strings to ids is exact.
+ * Unlike the reference (which clears the caller's label vectors,
+ * X-TED_CPU/TED.cpp:160-161) the library never writes to caller input.
+ *
+ * Every function returns 0 on success or a negative XTED_E* code; none
+ * throws or exits. A context is not thread-safe: use one per host thread, or
+ * lock around calls.
+ */
+#ifndef XTED_H
+#define XTED_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XTED_OK 0
+#define XTED_EINVAL (-1)   /* malformed tree, bad size or argument        */
+#define XTED_ENOMEM (-2)   /* device or host allocation failed / over limit */
+#define XTED_ETIMEOUT (-3) /* a bounded device wait ran out               */
+#define XTED_ECUDA (-4)    /* a CUDA runtime call failed                  */
+#define XTED_ENODEV (-5)   /* no usable sm_100 device                     */
+#define XTED_ENOTFOUND (-6) /* unknown serving ticket                     */
+#define XTED_EAGAIN (-7)   /* serving queue full; retry later             */
+
+/* Largest tree accepted (nodes). Bounds the int32 key arithmetic of the
+ * row scan and keeps the per-pair distance table addressable. */
+#define XTED_MAX_NODES 65535
+
+typedef struct xted_tree {
+    const int32_t *labels;    /* [n] label ids                              */
+    const int32_t *child_off; /* [n+1] CSR offsets, child_off[0] == 0       */
+    const int32_t *child_idx; /* [n-1] children in preorder, left to right  */
+    int32_t n;                /* number of nodes (0 = empty tree)           */
+} xted_tree;
+
+/* Decomposition of the keyroot tables. The distance is identical for all
+ * three (tree edit distance is invariant under mirroring both trees); only
+ * the amount of work differs. */
+#define XTED_ORIENT_AUTO 0  /* per pair, the cheaper of the two            */
+#define XTED_ORIENT_RIGHT 1 /* right-path keyroots, X-TED_CPU's choice      */
+#define XTED_ORIENT_LEFT 2  /* left-path keyroots (classic Zhang-Shasha)    */
+
+typedef struct xted_opts {
+    int32_t device;         /* CUDA device ordinal                          */
+    int32_t orientation;    /* XTED_ORIENT_*                                */
+    int32_t narrow_width;   /* widest column chunk run by one warp (1..256);
+                               0 runs every chunk on a whole thread block   */
+    int32_t run_rows;       /* target rows per row run (>= 1)               */
+    int32_t ctas_per_sm;    /* persistent blocks per SM (0 = occupancy max) */
+    int32_t reserved;
+    double wait_timeout_s;  /* bound on every device-side wait              */
+    int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
+} xted_opts;
+
+typedef struct xted_ctx xted_ctx;
+
+/* Statistics of the last distance/batch call. */
+typedef struct xted_stats {
+    int64_t pairs;
+    int64_t cells;          /* interior forest-table cells executed          */
+    int64_t cells_right;    /* cells X-TED's right-path decomposition needs  */
+    int64_t tasks;          /* block-level tasks in the device queue         */
+    int64_t units;          /* warp/block work units                         */
+    int64_t h2d_bytes, d2h_bytes;
+    double host_plan_ms;    /* host planning time                            */
+    double device_ms;       /* device time of one run: counter reset, DP launch
+                               and gather (CUDA events on the launch stream) */
+    double total_ms;        /* wall time of the call                         */
+    int32_t levels_max;     /* deepest keyroot-level count of any pair        */
+    int32_t grid;           /* persistent blocks launched                    */
+    double dp_ms;           /* device time of the DP kernel alone            */
+} xted_stats;
+
+void xted_opts_default(xted_opts *opts);
+const char *xted_strerror(int code);
+
+int xted_create(xted_ctx **ctx, const xted_opts *opts);
+int xted_destroy(xted_ctx *ctx);
+
+/* One pair; synchronous. Matches standard_ted, including its empty-tree
+ * rules (m == 0 -> n, n == 0 -> m; X-TED_CPU/TED.cpp:181-186). */
+int xted_distance(xted_ctx *ctx, const xted_tree *a, const xted_tree *b, int32_t *out);
+
+/* npairs pairs (a[i], b[i]) in one persistent device launch; synchronous. */
+int xted_distance_batch(xted_ctx *ctx, const xted_tree *a, const xted_tree *b, int32_t npairs,
+                        int32_t *out);
+
+/* Plans npairs pairs and uploads everything the device needs; the inputs then
+ * stay resident in HBM. xted_run_prepared recomputes that batch from the
+ * resident inputs (repeated evaluation; device-only timing). The prepared
+ * batch lives until the next prepare or batch call on the context. */
+int xted_prepare_batch(xted_ctx *ctx, const xted_tree *a, const xted_tree *b, int32_t npairs);
+int xted_run_prepared(xted_ctx *ctx, int32_t *out);
+
+int xted_last_stats(const xted_ctx *ctx, xted_stats *out);
+
+/* Cell count of a pair under each decomposition, without computing it:
+ * out[0] = right path (X-TED), out[1] = left path, out[2] = the chosen one. */
+int xted_pair_cells(const xted_tree *a, const xted_tree *b, int32_t orientation, int64_t *out3);
+
+/* Checks that a tree is a well-formed preorder CSR. */
+int xted_validate(const xted_tree *t);
+
+/* Seeded synthetic trees (the benchmark workloads). shape: 0 random
+ * recursive, 1 wide-shallow, 2 deep-narrow, 3 caterpillar. label_kind: 0
+ * uniform over `alphabet` ids, 1 Zipf(s = 1.1) over `alphabet` ids. Writes
+ * n labels, n+1 offsets and n-1 children into caller buffers. */
+int xted_gen_tree(int32_t shape, int32_t n, uint64_t seed, int32_t label_kind, int32_t alphabet,
+                  int32_t *labels, int32_t *child_off, int32_t *child_idx);
+
+/* ---- serving: a resident corpus and exact top-k queries ---- */
+
+/* Uploads a corpus (replacing any previous one) and precomputes its
+ * keyroot metadata on the device. */
+int xted_corpus_load(xted_ctx *ctx, const xted_tree *trees, int32_t ntrees);
+
+/* Queues a query for the k nearest corpus trees by TED. Returns at once. */
+int xted_query_submit(xted_ctx *ctx, const xted_tree *q, int32_t k, uint64_t *ticket);
+
+/* Advances the serving loop and reports a query. *done = 1 when ids/dists
+ * (k entries each, ascending distance, ties by corpus index) are final. */
+int xted_query_poll(xted_ctx *ctx, uint64_t ticket, int32_t *ids, int32_t *dists, int32_t *done);
+
+/* Blocks until every submitted query is finished. */
+int xted_serve_drain(xted_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XTED_H */

@@ -1,0 +1,175 @@
+"""Parity of the CUDA path with the oracle, through the C ABI (needs a B200).
+
+Integer min-plus arithmetic: every distance must match bit-exactly (tolerance 0).
+"""
+import random
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import brute
+import xted
+from xted import gen, trees
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_tree(rng, n, alpha, shape):
+    if n == 0:
+        return trees.Tree(np.zeros(0, np.int32), np.zeros(1, np.int32), np.zeros(0, np.int32))
+    adj = [[] for _ in range(n)]
+    for i in range(1, n):
+        if shape == 0:
+            p = rng.randrange(i)
+        elif shape == 1:
+            p = rng.randrange(min(i, 8))
+        else:
+            p = max(0, i - 1 - rng.randrange(3))
+        if rng.random() < 0.5:
+            adj[p].append(i)
+        else:
+            adj[p].insert(0, i)
+    order, st = [], [0]
+    while st:
+        v = st.pop()
+        order.append(v)
+        st.extend(reversed(adj[v]))
+    new = {v: k for k, v in enumerate(order)}
+    labels = [0] * n
+    out = [[] for _ in range(n)]
+    for v in range(n):
+        labels[new[v]] = rng.randrange(alpha)
+        out[new[v]] = [new[c] for c in adj[v]]
+    return trees.from_adjacency(labels, out)
+
+
+def test_single_pair_100_matches_oracle(ctx):
+    a, b = gen.single_pair_100()
+    assert ctx.distance(a, b) == oracle.distance(a, b)
+
+
+def test_golden_datasets(ctx, golden_datasets):
+    pairs = [(a, b) for _, a, b, _ in golden_datasets]
+    want = [d for *_, d in golden_datasets]
+    got = ctx.distance_batch(pairs)
+    bad = [(golden_datasets[i][0], int(got[i]), want[i]) for i in range(len(want)) if got[i] != want[i]]
+    assert not bad, bad[:5]
+
+
+def test_golden_datasets_one_by_one(ctx, golden_datasets):
+    for name, a, b, d in golden_datasets[:12]:
+        assert ctx.distance(a, b) == d, name
+
+
+def test_golden_synthetic(ctx, golden_synthetic):
+    pairs = [(a, b) for _, a, b, _ in golden_synthetic]
+    want = np.array([d for *_, d in golden_synthetic])
+    got = ctx.distance_batch(pairs)
+    assert np.array_equal(got, want), [(golden_synthetic[i][0], got[i], want[i])
+                                       for i in np.nonzero(got != want)[0][:5]]
+
+
+@pytest.mark.parametrize("orientation", [xted.ORIENT_RIGHT, xted.ORIENT_LEFT, xted.ORIENT_AUTO])
+@pytest.mark.parametrize("narrow_width,run_rows", [(0, 1), (7, 3), (32, 64), (256, 17), (256, 64)])
+def test_forced_granularities(orientation, narrow_width, run_rows):
+    """Every executor (warp-narrow of each width class, block-wide) and every
+    decomposition, forced, on the same random pairs."""
+    rng = random.Random(1000 * orientation + narrow_width + run_rows)
+    pairs = []
+    for _ in range(24):
+        pairs.append((_rand_tree(rng, rng.choice([0, 1, 2, 5, 30, 90, 200, 420]), rng.randint(1, 6), rng.randrange(3)),
+                      _rand_tree(rng, rng.choice([1, 3, 8, 50, 130, 300, 700]), rng.randint(1, 6), rng.randrange(3))))
+    want = [oracle.distance(a, b) for a, b in pairs]
+    with xted.Context(orientation=orientation, narrow_width=narrow_width, run_rows=run_rows) as c:
+        got = c.distance_batch(pairs)
+    assert list(got) == want
+
+
+def test_brute_force_small(ctx):
+    rng = random.Random(3)
+    pairs = [(_rand_tree(rng, rng.randint(0, 9), rng.randint(1, 3), rng.randrange(3)),
+              _rand_tree(rng, rng.randint(0, 9), rng.randint(1, 3), rng.randrange(3))) for _ in range(300)]
+    got = ctx.distance_batch(pairs)
+    for (a, b), d in zip(pairs, got):
+        assert d == brute.distance(a, b)
+    brute.clear_cache()
+
+
+def test_batch_equals_singles_and_order(ctx):
+    rng = random.Random(8)
+    pairs = [(_rand_tree(rng, rng.randint(1, 150), 4, rng.randrange(3)),
+              _rand_tree(rng, rng.randint(1, 150), 4, rng.randrange(3))) for _ in range(40)]
+    batch = ctx.distance_batch(pairs)
+    singles = [ctx.distance(a, b) for a, b in pairs]
+    assert list(batch) == singles
+    perm = list(range(len(pairs)))
+    rng.shuffle(perm)
+    again = ctx.distance_batch([pairs[i] for i in perm])
+    assert [int(again[k]) for k in range(len(perm))] == [singles[i] for i in perm]
+
+
+def test_empty_and_tiny(ctx):
+    e = trees.Tree(np.zeros(0, np.int32), np.zeros(1, np.int32), np.zeros(0, np.int32))
+    one = trees.from_adjacency([7], [[]])
+    other = trees.from_adjacency([8], [[]])
+    t = gen.tree("deep", 33, 5)
+    assert ctx.distance(e, e) == 0
+    assert ctx.distance(e, t) == 33
+    assert ctx.distance(t, e) == 33
+    assert ctx.distance(one, one) == 0
+    assert ctx.distance(one, other) == 1
+    assert ctx.distance(one, t) == oracle.distance(one, t)
+
+
+def test_standard_ted_mirror_interface():
+    # the reference's own calling convention: string labels + adjacency lists
+    x_node = ["a", "b", "c", "d", "e"]
+    x_adj = [[1, 2], [], [3, 4], [], []]
+    y_node = ["a", "c", "d", "x"]
+    y_adj = [[1, 3], [2], [], []]
+    a = trees.from_adjacency(trees.Interner()(x_node), x_adj)
+    d = xted.standard_ted(x_node, x_adj, y_node, y_adj, 8, 1)
+    intern = trees.Interner()
+    assert d == oracle.distance(trees.from_adjacency(intern(x_node), x_adj),
+                                trees.from_adjacency(intern(y_node), y_adj))
+    assert x_node == ["a", "b", "c", "d", "e"]  # inputs are not cleared
+    assert xted.standard_ted([], [], y_node, y_adj) == 4
+    del a
+
+
+def test_mixed_workload_sample(ctx):
+    pairs = gen.mixed_batch(64, seed=77, hi=600)
+    got = ctx.distance_batch(pairs)
+    want = oracle.distance_batch(pairs, nthreads=8)
+    assert np.array_equal(got, want)
+
+
+def test_single_pair_1000_mixed_shapes(ctx):
+    a, b = gen.single_pair_1000()
+    assert ctx.distance(a, b) == oracle.distance(a, b)
+
+
+def test_prepared_batch_repeatable(ctx):
+    pairs = gen.mixed_batch(48, seed=5, hi=400)
+    ctx.prepare_batch(pairs)
+    r1 = ctx.run_prepared()
+    r2 = ctx.run_prepared()
+    assert np.array_equal(r1, r2)
+    assert np.array_equal(r1, oracle.distance_batch(pairs, nthreads=8))
+
+
+def test_large_pair_properties(ctx):
+    """20,000-node pairs: size-independent properties (the oracle would take
+    minutes here): identity, symmetry, bounds, and agreement of both
+    decompositions on a 4,000-node pair with the oracle."""
+    a, b = gen.single_pair_20000(shape="caterpillar")
+    assert ctx.distance(a, a) == 0
+    d_ab = ctx.distance(a, b)
+    assert d_ab == ctx.distance(b, a)
+    assert 0 <= d_ab <= len(a) + len(b)
+    r, s = gen.tree("random", 4000, 41, "uniform", 64), gen.tree("random", 4000, 42, "uniform", 64)
+    want = oracle.distance(r, s)
+    for orient in (xted.ORIENT_RIGHT, xted.ORIENT_LEFT):
+        with xted.Context(orientation=orient) as c:
+            assert c.distance(r, s) == want

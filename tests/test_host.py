@@ -1,0 +1,125 @@
+"""Host-side logic and the C ABI surface (CPU only; no device calls)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+import xted
+from xted import gen, trees
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_node_process_matches_reference_rule():
+    # X-TED_CPU/dataset_preprocess.cpp:68-81: a token is emitted only at a space
+    assert trees.node_process("a b c ") == ["a", "b", "c"]
+    assert trees.node_process("a b c") == ["a", "b"]
+    assert trees.node_process("a  b ") == ["a", "", "b"]
+
+
+def test_pre_process_matches_reference_format():
+    assert trees.pre_process("[[1, 2], [], [3, 4], [], []]") == [[1, 2], [], [3, 4], [], []]
+    assert trees.pre_process("[[]]") == [[]]
+    assert trees.pre_process("[[1], [2], []]") == [[1], [2], []]
+
+
+def test_from_parent_roundtrip():
+    t = gen.tree("random", 300, 9)
+    u = trees.from_parent(t.labels, t.parent())
+    assert np.array_equal(t.off, u.off) and np.array_equal(t.idx, u.idx)
+
+
+@pytest.mark.parametrize("shape", ["random", "wide", "deep", "caterpillar"])
+def test_generator_valid_and_deterministic(shape):
+    for n in (1, 2, 17, 500):
+        t = gen.tree(shape, n, 77, "zipf", 1000)
+        assert len(t) == n
+        assert trees.is_preorder(t)
+        assert xted.validate(t)
+        u = gen.tree(shape, n, 77, "zipf", 1000)
+        assert np.array_equal(t.labels, u.labels) and np.array_equal(t.idx, u.idx)
+        assert t.labels.min() >= 0 and t.labels.max() < 1000
+
+
+def _depths(t):
+    d = np.zeros(len(t), np.int64)
+    for v in range(len(t)):
+        for c in t.idx[t.off[v]:t.off[v + 1]]:
+            d[c] = d[v] + 1
+    return d
+
+
+def test_generator_shapes():
+    w = gen.tree("wide", 1000, 1)
+    assert _depths(w).max() <= 4 and w.off[1] - w.off[0] == 40
+    d = gen.tree("deep", 1000, 1)
+    assert _depths(d).max() >= 99
+    c = gen.tree("caterpillar", 1000, 1)
+    # spine child is the last child of every spine node
+    assert c.off[1] - c.off[0] == 10 and c.idx[c.off[1] - 1] == 10
+    assert _depths(c).max() == 100
+
+
+def test_validate_rejects_malformed():
+    ok = trees.from_adjacency([0, 1, 2], [[1, 2], [], []])
+    assert xted.validate(ok)
+    bad_order = trees.Tree(np.array([0, 1, 2], np.int32), np.array([0, 2, 2, 2], np.int32),
+                           np.array([2, 1], np.int32))  # children out of preorder
+    assert not xted.validate(bad_order)
+    bad_range = trees.Tree(np.array([0, 1], np.int32), np.array([0, 1, 1], np.int32), np.array([5], np.int32))
+    assert not xted.validate(bad_range)
+    bad_count = trees.Tree(np.array([0, 1, 2], np.int32), np.array([0, 1, 1, 1], np.int32), np.array([1], np.int32))
+    assert not xted.validate(bad_count)
+    not_pre = trees.from_adjacency([0, 1, 2, 3], [[1, 3], [], [], []])  # node 2 unreachable
+    assert not xted.validate(not_pre)
+
+
+def test_pair_cells_match_oracle_keyroot_sums():
+    for s in ("random", "wide", "deep", "caterpillar"):
+        a = gen.tree(s, 400, 3)
+        b = gen.tree("random", 250, 4)
+        cr, cl, chosen = xted.pair_cells(a, b)
+        assert cr == oracle.tree_stats(a)[2] * oracle.tree_stats(b)[2]
+        assert cl == oracle.tree_stats(trees.mirror(a))[2] * oracle.tree_stats(trees.mirror(b))[2]
+        assert chosen == min(cr, cl)
+
+
+def _declared_functions():
+    hdr = open(os.path.join(REPO, "include", "xted.h")).read()
+    return sorted(set(re.findall(r"^\w[\w\s\*]*?\b(xted_\w+)\s*\(", hdr, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = _declared_functions()
+    assert "xted_distance" in names and "xted_query_poll" in names
+    L = ctypes.CDLL(xted.LIB_PATH)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_context_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(xted.XtedError) as e:
+        xted.Context()
+    assert e.value.code == xted.XTED_ENODEV
+
+
+def test_planner_emulation_matches_oracle(tmp_path):
+    """Compiles the product planner with a CPU emulation of the unit execution
+    (tests/cpp/plan_emu.cpp) and checks distances and plan invariants."""
+    obj = tmp_path / "xo.o"
+    exe = tmp_path / "plan_emu"
+    subprocess.run(["gcc", "-O2", "-c", os.path.join(REPO, "oracle", "xted_oracle.c"), "-o", str(obj)], check=True)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I/usr/local/cuda/include",
+                    os.path.join(REPO, "tests", "cpp", "plan_emu.cpp"),
+                    os.path.join(REPO, "x-ted_b200", "csrc", "plan.cpp"), str(obj), "-o", str(exe), "-lpthread"],
+                   check=True)
+    r = subprocess.run([str(exe), "120", "250", "99"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("ok")

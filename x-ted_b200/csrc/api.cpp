@@ -1,0 +1,404 @@
+// api.cpp -- the C ABI (include/xted.h): context, device memory, launches.
+//
+// xted_distance / xted_distance_batch replace the reference's
+// standard_ted (X-TED_CPU/TED.cpp:177-190; X-TED_GPU/TED.cu:116-128): the
+// planner (plan.cpp) lays out every keyroot table of every pair as device
+// tasks, one cooperative launch of the persistent DP kernel (kernels.cu)
+// drains them, and a gather kernel reads Dtree[0][0] of each pair
+// (X-TED_CPU/TED.cpp:188). Errors are returned, never printed or exited on
+// (the reference prints CUDA errors and continues, X-TED_GPU/utils/cuda_utils.h:35-41,
+// or exits, X-TED_GPU/help.h:6-14).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/xted.h"
+#include "ctx.h"
+#include "plan.h"
+
+namespace xted {
+int dp_occupancy(int *blocks_per_sm);
+cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s);
+cudaError_t launch_gather(const XPair *pairs, const int32_t *trivial, const int32_t *dt, int npairs,
+                          int32_t *out, cudaStream_t s);
+}  // namespace xted
+
+using namespace xted;
+
+namespace {
+
+inline double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+namespace xted {
+
+int ctx_dev_reserve(xted_ctx *c, DevBuf &b, size_t bytes) {
+    if (b.cap >= bytes) return XTED_OK;
+    size_t want = align_up(std::max(bytes, b.cap + b.cap / 2), (size_t)2 << 20);
+    if (c->opts.mem_limit > 0) {
+        const int64_t limit = c->opts.mem_limit;
+        if (c->held - (int64_t)b.cap + (int64_t)want > limit) want = align_up(bytes, 256);
+        if (c->held - (int64_t)b.cap + (int64_t)want > limit) return XTED_ENOMEM;
+    }
+    if (b.p) {
+        cudaFree(b.p);
+        c->held -= (int64_t)b.cap;
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        return XTED_ENOMEM;
+    }
+    b.p = p;
+    b.cap = want;
+    c->held += (int64_t)want;
+    return XTED_OK;
+}
+
+int ctx_host_reserve(HostBuf &b, size_t bytes) {
+    if (b.cap >= bytes) return XTED_OK;
+    size_t want = align_up(std::max(bytes, b.cap + b.cap / 2), (size_t)1 << 20);
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    if (cudaHostAlloc(&b.p, want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return XTED_ENOMEM;
+    }
+    b.cap = want;
+    return XTED_OK;
+}
+
+// Copies the plan's pools into one pinned buffer and uploads it; fills the
+// pointer fields of the kernel parameters.
+int ctx_upload_plan(xted_ctx *c, const Plan &P, XKernelParams &K, size_t *h2d) {
+    struct Sec { const void *src; size_t bytes; size_t off; };
+    Sec sec[9] = {
+        {P.rowinfo.data(), P.rowinfo.size() * sizeof(int2h), 0},
+        {P.colinfo.data(), P.colinfo.size() * sizeof(int4h), 0},
+        {P.krd.data(), P.krd.size() * sizeof(int32_t), 0},
+        {P.runs.data(), P.runs.size() * sizeof(XRun), 0},
+        {P.chunks.data(), P.chunks.size() * sizeof(XChunk), 0},
+        {P.pairs.data(), P.pairs.size() * sizeof(XPair), 0},
+        {P.units.data(), P.units.size() * sizeof(XUnit), 0},
+        {P.tasks.data(), P.tasks.size() * sizeof(XTask), 0},
+        {P.trivial.data(), P.trivial.size() * sizeof(int32_t), 0},
+    };
+    size_t total = 0;
+    for (auto &s : sec) {
+        s.off = total;
+        total = align_up(total + std::max(s.bytes, (size_t)16), 256);
+    }
+    int rc = ctx_host_reserve(c->stage, total);
+    if (rc) return rc;
+    rc = ctx_dev_reserve(c, c->meta, total);
+    if (rc) return rc;
+    char *h = (char *)c->stage.p;
+    for (auto &s : sec)
+        if (s.bytes) std::memcpy(h + s.off, s.src, s.bytes);
+    if (cudaMemcpyAsync(c->meta.p, h, total, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return XTED_ECUDA;
+    char *d = (char *)c->meta.p;
+    K.rowinfo = (const int2 *)(d + sec[0].off);
+    K.colinfo = (const int4 *)(d + sec[1].off);
+    K.krd = (const int32_t *)(d + sec[2].off);
+    K.runs = (const XRun *)(d + sec[3].off);
+    K.chunks = (const XChunk *)(d + sec[4].off);
+    K.pairs = (const XPair *)(d + sec[5].off);
+    K.units = (const XUnit *)(d + sec[6].off);
+    K.tasks = (const XTask *)(d + sec[7].off);
+    c->d_trivial = (const int32_t *)(d + sec[8].off);
+    *h2d = total;
+    return XTED_OK;
+}
+
+// Uploads a plan and sizes every device buffer it needs; the kernel
+// parameters are kept in the context so the plan can be run repeatedly.
+int ctx_prepare(xted_ctx *c, const Plan &P) {
+    c->prepared = false;
+    const int npairs = (int)P.pairs.size();
+    XKernelParams &K = c->kp;
+    std::memset(&K, 0, sizeof(K));
+    size_t h2d = 0;
+    int rc = ctx_upload_plan(c, P, K, &h2d);
+    if (rc) return rc;
+    rc = ctx_dev_reserve(c, c->dt, (size_t)std::max<int64_t>(P.dt_elems, 1) * sizeof(int32_t));
+    if (rc) return rc;
+    // per-block scratch: far-row stacks (+ rows of the generic wide path)
+    int64_t per = (int64_t)P.stack_rows * (XTED_WARPS * XTED_NARROW_MAX);
+    if (P.max_wide > 0 && P.max_wide <= XTED_WIDE_REG_MAX)
+        per = std::max<int64_t>(per, (int64_t)P.stack_rows * P.max_wide);
+    if (P.max_wide > XTED_WIDE_REG_MAX)
+        per = std::max<int64_t>(per, 2 * (int64_t)P.max_wide + 1 + (int64_t)P.stack_rows * P.max_wide);
+    per = (int64_t)align_up((size_t)per, 64);
+    rc = ctx_dev_reserve(c, c->scratch, (size_t)per * (size_t)c->grid * sizeof(int32_t));
+    if (rc) return rc;
+    // counters: [0] queue head, [1] error, [2..5] error info, then finished[npairs], out[npairs]
+    rc = ctx_dev_reserve(c, c->counters, (8 + 2 * (size_t)npairs) * sizeof(int32_t));
+    if (rc) return rc;
+    rc = ctx_host_reserve(c->result, ((size_t)npairs + 8) * sizeof(int32_t));
+    if (rc) return rc;
+    int32_t *cnt = (int32_t *)c->counters.p;
+    K.dt = (int32_t *)c->dt.p;
+    K.scratch = (int32_t *)c->scratch.p;
+    K.scratch_per_cta = per;
+    K.stack_rows = P.stack_rows;
+    K.ntasks = (int32_t)P.tasks.size();
+    K.task_next = cnt;
+    K.error = cnt + 1;
+    K.error_info = cnt + 2;
+    K.finished = cnt + 8;
+    K.timeout_ns = (uint64_t)(c->opts.wait_timeout_s * 1e9);
+    c->npairs = npairs;
+    c->h2d_bytes = (int64_t)h2d;
+    c->prepared = true;
+    return XTED_OK;
+}
+
+// Runs the prepared plan: counter reset, the persistent DP launch, the
+// gather, and the copy of results + error word to pinned memory. Synchronous.
+int ctx_run(xted_ctx *c, int32_t *out) {
+    if (!c->prepared) return XTED_EINVAL;
+    const XKernelParams &K = c->kp;
+    const int npairs = c->npairs;
+    int32_t *cnt = (int32_t *)c->counters.p;
+    int32_t *d_out = cnt + 8 + npairs;
+    int32_t *hres = (int32_t *)c->result.p;
+    const size_t res_bytes = (size_t)npairs * sizeof(int32_t);
+    cudaEventRecord(c->ev0, c->stream);
+    if (cudaMemsetAsync(cnt, 0, (8 + (size_t)npairs) * sizeof(int32_t), c->stream) != cudaSuccess)
+        return XTED_ECUDA;
+    cudaEventRecord(c->evk0, c->stream);
+    if (K.ntasks > 0) {
+        cudaError_t e = launch_dp(K, c->grid, c->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return XTED_ECUDA;
+        }
+    }
+    cudaEventRecord(c->evk1, c->stream);
+    if (launch_gather(K.pairs, c->d_trivial, K.dt, npairs, d_out, c->stream) != cudaSuccess)
+        return XTED_ECUDA;
+    cudaEventRecord(c->ev1, c->stream);
+    cudaMemcpyAsync(hres, cnt, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+    if (npairs) cudaMemcpyAsync(hres + 8, d_out, res_bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return XTED_ECUDA;
+    }
+    float ms = 0.f, kms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    cudaEventElapsedTime(&kms, c->evk0, c->evk1);
+    c->stats.device_ms = ms;
+    c->stats.dp_ms = kms;
+    c->stats.h2d_bytes = c->h2d_bytes;
+    c->stats.d2h_bytes = (int64_t)(res_bytes + 8 * sizeof(int32_t));
+    c->stats.grid = c->grid;
+    std::memcpy(c->err_info, hres + 2, sizeof(c->err_info));
+    if (hres[1] != 0) return hres[1];
+    if (npairs) std::memcpy(out, hres + 8, res_bytes);
+    return XTED_OK;
+}
+
+}  // namespace xted
+
+extern "C" {
+
+void xted_opts_default(xted_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->device = 0;
+    o->orientation = XTED_ORIENT_AUTO;
+    o->narrow_width = XTED_NARROW_MAX;
+    o->run_rows = 64;
+    o->ctas_per_sm = 0;
+    o->wait_timeout_s = 20.0;
+    o->mem_limit = 0;
+}
+
+const char *xted_strerror(int code) {
+    switch (code) {
+        case XTED_OK: return "ok";
+        case XTED_EINVAL: return "invalid argument or malformed tree";
+        case XTED_ENOMEM: return "out of memory (device, host or the context's limit)";
+        case XTED_ETIMEOUT: return "a bounded device wait timed out";
+        case XTED_ECUDA: return "CUDA runtime error";
+        case XTED_ENODEV: return "no usable sm_100 CUDA device";
+        case XTED_ENOTFOUND: return "unknown ticket";
+        case XTED_EAGAIN: return "serving queue full";
+        default: return "unknown error";
+    }
+}
+
+int xted_create(xted_ctx **out, const xted_opts *opts) {
+    if (!out) return XTED_EINVAL;
+    *out = nullptr;
+    xted_opts o;
+    if (opts) o = *opts;
+    else xted_opts_default(&o);
+    if (o.narrow_width < 0 || o.narrow_width > XTED_NARROW_MAX || o.run_rows < 1 ||
+        o.orientation < 0 || o.orientation > 2 || o.wait_timeout_s <= 0 || o.ctas_per_sm < 0)
+        return XTED_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || o.device < 0 || o.device >= ndev) {
+        cudaGetLastError();
+        return XTED_ENODEV;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess || prop.major != 10) return XTED_ENODEV;
+    if (cudaSetDevice(o.device) != cudaSuccess) return XTED_ECUDA;
+    xted_ctx *c = new (std::nothrow) xted_ctx();
+    if (!c) return XTED_ENOMEM;
+    c->opts = o;
+    c->sms = prop.multiProcessorCount;
+    int occ = 0;
+    if (dp_occupancy(&occ) != 0 || occ < 1) {
+        delete c;
+        return XTED_ECUDA;
+    }
+    if (o.ctas_per_sm > 0) occ = std::min(occ, o.ctas_per_sm);
+    c->grid = occ * c->sms;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->evk0) != cudaSuccess || cudaEventCreate(&c->evk1) != cudaSuccess) {
+        delete c;
+        return XTED_ECUDA;
+    }
+    *out = c;
+    return XTED_OK;
+}
+
+int xted_destroy(xted_ctx *c) {
+    if (!c) return XTED_OK;
+    cudaSetDevice(c->opts.device);
+    xted::serve_shutdown(c);
+    cudaStreamSynchronize(c->stream);
+    for (DevBuf *b : {&c->meta, &c->dt, &c->scratch, &c->counters})
+        if (b->p) cudaFree(b->p);
+    for (HostBuf *b : {&c->stage, &c->result})
+        if (b->p) cudaFreeHost(b->p);
+    for (cudaEvent_t e : {c->ev0, c->ev1, c->evk0, c->evk1})
+        if (e) cudaEventDestroy(e);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return XTED_OK;
+}
+
+int xted_distance_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs,
+                        int32_t *out) {
+    if (!c || npairs < 0 || (npairs > 0 && (!a || !b || !out))) return XTED_EINVAL;
+    const double t0 = now_ms();
+    if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
+    std::vector<TreeView> A((size_t)npairs), B((size_t)npairs);
+    for (int p = 0; p < npairs; p++) {
+        A[(size_t)p] = TreeView{a[p].n, a[p].labels, a[p].child_off, a[p].child_idx};
+        B[(size_t)p] = TreeView{b[p].n, b[p].labels, b[p].child_off, b[p].child_idx};
+    }
+    PlanOptions po;
+    po.orientation = c->opts.orientation;
+    po.narrow_width = c->opts.narrow_width;
+    po.run_rows = c->opts.run_rows;
+    Plan &P = c->plan;
+    int rc = make_plan(A.data(), B.data(), npairs, po, P);
+    const double t1 = now_ms();
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    if (rc) return rc;
+    c->stats.host_plan_ms = t1 - t0;
+    rc = ctx_prepare(c, P);
+    if (!rc) rc = ctx_run(c, out);
+    c->stats.pairs = npairs;
+    c->stats.cells = P.cells;
+    c->stats.cells_right = P.cells_right;
+    c->stats.tasks = (int64_t)P.tasks.size();
+    c->stats.units = (int64_t)P.units.size();
+    c->stats.levels_max = P.levels_max;
+    c->stats.total_ms = now_ms() - t0;
+    return rc;
+}
+
+int xted_prepare_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs) {
+    if (!c || npairs < 0 || (npairs > 0 && (!a || !b))) return XTED_EINVAL;
+    if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
+    std::vector<TreeView> A((size_t)npairs), B((size_t)npairs);
+    for (int p = 0; p < npairs; p++) {
+        A[(size_t)p] = TreeView{a[p].n, a[p].labels, a[p].child_off, a[p].child_idx};
+        B[(size_t)p] = TreeView{b[p].n, b[p].labels, b[p].child_off, b[p].child_idx};
+    }
+    PlanOptions po;
+    po.orientation = c->opts.orientation;
+    po.narrow_width = c->opts.narrow_width;
+    po.run_rows = c->opts.run_rows;
+    const double t0 = now_ms();
+    int rc = make_plan(A.data(), B.data(), npairs, po, c->plan);
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    if (rc) return rc;
+    c->stats.host_plan_ms = now_ms() - t0;
+    rc = ctx_prepare(c, c->plan);
+    if (rc) return rc;
+    // the upload is asynchronous on the context stream; finish it here so a
+    // following xted_run_prepared times device work only
+    return cudaStreamSynchronize(c->stream) == cudaSuccess ? XTED_OK : XTED_ECUDA;
+}
+
+int xted_run_prepared(xted_ctx *c, int32_t *out) {
+    if (!c || !out) return XTED_EINVAL;
+    if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
+    const Plan &P = c->plan;
+    const int rc = ctx_run(c, out);
+    c->stats.pairs = (int64_t)P.pairs.size();
+    c->stats.cells = P.cells;
+    c->stats.cells_right = P.cells_right;
+    c->stats.tasks = (int64_t)P.tasks.size();
+    c->stats.units = (int64_t)P.units.size();
+    c->stats.levels_max = P.levels_max;
+    return rc;
+}
+
+int xted_distance(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t *out) {
+    return xted_distance_batch(c, a, b, 1, out);
+}
+
+int xted_last_stats(const xted_ctx *c, xted_stats *out) {
+    if (!c || !out) return XTED_EINVAL;
+    *out = c->stats;
+    return XTED_OK;
+}
+
+int xted_pair_cells(const xted_tree *a, const xted_tree *b, int32_t orientation, int64_t *out3) {
+    if (!a || !b || !out3 || orientation < 0 || orientation > 2) return XTED_EINVAL;
+    TreeView A{a->n, a->labels, a->child_off, a->child_idx};
+    TreeView B{b->n, b->labels, b->child_off, b->child_idx};
+    int rc = validate_tree(A);
+    if (!rc) rc = validate_tree(B);
+    if (rc) return rc;
+    int64_t sa[2], sb[2];
+    keyroot_sums(A, sa);
+    keyroot_sums(B, sb);
+    out3[0] = sa[0] * sb[0];
+    out3[1] = sa[1] * sb[1];
+    out3[2] = orientation == XTED_ORIENT_RIGHT ? out3[0]
+              : orientation == XTED_ORIENT_LEFT ? out3[1]
+                                                : std::min(out3[0], out3[1]);
+    return XTED_OK;
+}
+
+int xted_validate(const xted_tree *t) {
+    if (!t) return XTED_EINVAL;
+    return validate_tree(TreeView{t->n, t->labels, t->child_off, t->child_idx});
+}
+
+}  // extern "C"

@@ -1,0 +1,532 @@
+// kernels.cu -- the keyroot-table dynamic program on sm_100a.
+//
+// One persistent kernel drains a device queue of tasks (see xted_internal.h).
+// A task is one wide unit run by the whole 256-thread block, or up to eight
+// narrow units, one per warp. A unit computes the forest tables of a run of
+// A-keyroots against a chunk of B-segments, row by row from the bottom:
+//
+//   reference recurrence (X-TED_CPU/parallel_computing.cpp:17-43):
+//     tree cell   D[i][j] = min(D[i+1][j+1] + cost(i,j), D[i+1][j] + 1, D[i][j+1] + 1),
+//                 Dtree[i][j] = D[i][j]
+//     forest cell D[i][j] = min(Dtree[i][j] + D[orl(i)+1][orl(j)+1], D[i+1][j] + 1,
+//                               D[i][j+1] + 1)
+//
+// Row formulation: with A[j] = min(first term, D[i+1][j] + 1), row i is the
+// min-plus suffix scan D[i][j] = min_{k >= j} (A[k] + (k - j)) closed by the
+// border D[i][je] = imax - i. Every column carries a key c + BIG*seg, so one
+// unsegmented suffix-min of A + key over a whole chunk yields every segment
+// (table) at once: values from a later segment are at least BIG too large.
+// The row above (D[i+1][*]) lives in registers; rows that later rows will use
+// as D[orl(i)+1][*] are pushed on a per-warp stack in global scratch (its
+// depth is the number of keyroots on a root path). Dtree is read with
+// ld.global.cg (L2), because other blocks write it during the launch.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/xted.h"
+#include "xted_internal.h"
+
+namespace xted {
+
+#define FULLMASK 0xffffffffu
+
+__device__ __forceinline__ int ld_acquire(const int32_t *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void set_error(const XKernelParams &P, int code, int a, int b, int c) {
+    if (atomicCAS(P.error, 0, code) == 0) {
+        P.error_info[0] = a;
+        P.error_info[1] = b;
+        P.error_info[2] = c;
+    }
+}
+
+// Waits until *p >= target. Bounded by time and by iterations; returns false
+// (and the caller gives up) on timeout or when another block reported an error.
+__device__ bool wait_ge(const XKernelParams &P, const int32_t *p, int target) {
+    if (ld_acquire(p) >= target) return true;
+    const uint64_t t0 = global_ns();
+    unsigned ns = 64;
+    for (long it = 0; it < (1L << 26); it++) {
+        __nanosleep(ns);
+        if (ns < 2048) ns <<= 1;
+        if (ld_acquire(p) >= target) return true;
+        if (*(volatile int32_t *)P.error != 0) return false;
+        if (global_ns() - t0 > P.timeout_ns) break;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int warp_suffix_min(int v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int o = __shfl_down_sync(FULLMASK, v, d);
+        if (lane + d < 32) v = min(v, o);
+    }
+    return v;
+}
+
+__device__ __forceinline__ int warp_prefix_sum(int v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int o = __shfl_up_sync(FULLMASK, v, d);
+        if (lane >= d) v += o;
+    }
+    return v;
+}
+
+// Per-column state of one thread: W consecutive columns of the chunk.
+template <int W>
+struct Cols {
+    int node[W], lab[W], foff[W], dend[W], key[W];
+    unsigned far;   // bit k: column k is a far column (pushed with stack rows)
+    unsigned valid; // bit k: column k exists
+};
+
+// Loads the thread's columns [c0, c0+W) of a chunk. `before` = segment ends
+// strictly before column c0 (computed by the caller's scan).
+template <int W>
+__device__ __forceinline__ void load_cols(const XKernelParams &P, const XChunk &ch, int c0,
+                                          Cols<W> &C) {
+    C.far = 0;
+    C.valid = 0;
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        const int c = c0 + k;
+        if (c < ch.width) {
+            const int4 ci = __ldg(&P.colinfo[ch.col_lo + c]);
+            C.node[k] = ci.x;
+            C.lab[k] = ci.y;
+            C.foff[k] = ci.z & XTED_COL_FOFF_MASK;
+            C.dend[k] = ci.w;
+            if (ci.z & XTED_COL_FARCOL) C.far |= 1u << k;
+            C.valid |= 1u << k;
+        } else {
+            C.node[k] = 0;
+            C.lab[k] = 0;
+            C.foff[k] = 1;
+            C.dend[k] = 2;  // never a segment end, never a tree column
+        }
+    }
+}
+
+template <int W>
+__device__ __forceinline__ int count_ends(const Cols<W> &C) {
+    int e = 0;
+#pragma unroll
+    for (int k = 0; k < W; k++) e += ((C.valid >> k) & 1u) && C.dend[k] == 1;
+    return e;
+}
+
+template <int W>
+__device__ __forceinline__ void set_keys(Cols<W> &C, int c0, int before) {
+    int seg = before;
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        C.key[k] = (c0 + k) + XTED_KEY_BIG * seg;
+        if (((C.valid >> k) & 1u) && C.dend[k] == 1) seg++;
+    }
+}
+
+// The per-row cell work shared by both executors: builds v = A + key for the
+// thread's columns and their local suffix minima. Returns the thread's minimum.
+template <int W>
+__device__ __forceinline__ int row_cells(const Cols<W> &C, const int (&prev)[W], const int (&cur_dt)[W],
+                                         int dnext, bool trow, int rl, int bord, int rowfar,
+                                         const int32_t *top, int c0, int (&loc)[W]) {
+    int run = XTED_INF;
+#pragma unroll
+    for (int k = W - 1; k >= 0; k--) {
+        const int up = prev[k];
+        int diag = (k == W - 1) ? dnext : prev[k + 1];
+        const bool segend = C.dend[k] == 1;
+        if (segend) diag = bord - 1;
+        const bool tcol = C.foff[k] == C.dend[k];
+        int a;
+        if (trow && tcol) {
+            a = diag + (rl != C.lab[k]);
+        } else {
+            int far;
+            if (trow) far = C.dend[k] - C.foff[k];
+            else if (tcol) far = rowfar;
+            else far = ((C.valid >> k) & 1u) ? top[c0 + k + C.foff[k]] : 0;
+            a = cur_dt[k] + far;
+        }
+        int A = min(a, up + 1);
+        if (segend) A = min(A, bord + 1);
+        const int v = ((C.valid >> k) & 1u) ? A + C.key[k] : XTED_INF;
+        run = min(run, v);
+        loc[k] = run;
+    }
+    return run;
+}
+
+// ---------------------------------------------------------------------------
+// Narrow unit: one warp, chunk width <= 32*W.
+// ---------------------------------------------------------------------------
+template <int W>
+__device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane,
+                           int32_t *stk) {
+    const XRun run = P.runs[u.run];
+    const XChunk ch = P.chunks[u.chunk];
+    const int c0 = lane * W;
+    Cols<W> C;
+    load_cols<W>(P, ch, c0, C);
+    {
+        const int e = count_ends<W>(C);
+        const int incl = warp_prefix_sum(e, lane);
+        set_keys<W>(C, c0, incl - e);
+    }
+    const int n = pr.n;
+    const int32_t *dt_in = P.dt + pr.dt_off;
+    int32_t *dt_out = P.dt + pr.dt_off;
+    const int2 *rows = P.rowinfo + pr.row_base;
+    const int stride = XTED_NARROW_MAX;
+
+    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+        const int i0 = __ldg(&P.krd[kr]);
+        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        int prev[W], nxt[W];
+#pragma unroll
+        for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        int sp = 0;
+        {
+            const int32_t *drow = dt_in + (int64_t)(imax - 1) * n;
+#pragma unroll
+            for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
+        }
+        int2 rnext = __ldg(&rows[imax - 1]);
+        for (int i = imax - 1; i >= i0; i--) {
+            int cur[W];
+#pragma unroll
+            for (int k = 0; k < W; k++) cur[k] = nxt[k];
+            const int2 ri = rnext;
+            if (i > i0) {
+                const int32_t *drow = dt_in + (int64_t)(i - 1) * n;
+#pragma unroll
+                for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
+                rnext = __ldg(&rows[i - 1]);
+            }
+            const int ro = ri.y & XTED_ROW_ORL_MASK;
+            const bool trow = ro == imax - 1;
+            const int bord = imax - i;
+            const int rowfar = imax - ro - 1;
+            const int32_t *top = stk + (sp > 0 ? sp - 1 : 0) * stride;
+            const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
+            int loc[W];
+            const int mine = row_cells<W>(C, prev, cur, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
+            const int incl = warp_suffix_min(mine, lane);
+            int carry = __shfl_down_sync(FULLMASK, incl, 1);
+            if (lane == 31) carry = XTED_INF;
+            int32_t *orow = dt_out + (int64_t)i * n;
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+                const int d = min(loc[k], carry) - C.key[k];
+                prev[k] = d;
+                if (trow && C.foff[k] == C.dend[k] && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
+            }
+            __syncwarp();
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) sp--;
+            if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
+                if (sp < P.stack_rows) {
+                    int32_t *dst = stk + sp * stride + c0;
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if ((C.far >> k) & 1u) dst[k] = prev[k];
+                } else if (lane == 0) {
+                    set_error(P, XTED_ENOMEM, 1, sp, P.stack_rows);
+                }
+                sp++;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Wide unit: the whole block, chunk width <= 256*W.
+// ---------------------------------------------------------------------------
+struct WideShared {
+    int wtot[XTED_WARPS];       // per-warp suffix minima of the current row
+    int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
+    int ends[XTED_WARPS];
+};
+
+template <int W>
+__device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
+                         WideShared &S) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const XRun run = P.runs[u.run];
+    const XChunk ch = P.chunks[u.chunk];
+    const int c0 = tid * W;
+    const int stride = ch.width;
+    Cols<W> C;
+    load_cols<W>(P, ch, c0, C);
+    {
+        const int e = count_ends<W>(C);
+        const int incl = warp_prefix_sum(e, lane);
+        if (lane == 31) S.ends[warp] = incl;
+        __syncthreads();
+        int before = incl - e;
+        for (int w = 0; w < warp; w++) before += S.ends[w];
+        set_keys<W>(C, c0, before);
+    }
+    const int n = pr.n;
+    const int32_t *dt_in = P.dt + pr.dt_off;
+    int32_t *dt_out = P.dt + pr.dt_off;
+    const int2 *rows = P.rowinfo + pr.row_base;
+
+    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+        const int i0 = __ldg(&P.krd[kr]);
+        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        int prev[W], nxt[W];
+#pragma unroll
+        for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        if (lane == 0) S.first[warp] = prev[0];
+        if (tid == 0) S.first[XTED_WARPS] = 0;
+        int sp = 0;
+        {
+            const int32_t *drow = dt_in + (int64_t)(imax - 1) * n;
+#pragma unroll
+            for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
+        }
+        int2 rnext = __ldg(&rows[imax - 1]);
+        __syncthreads();
+        for (int i = imax - 1; i >= i0; i--) {
+            int cur[W];
+#pragma unroll
+            for (int k = 0; k < W; k++) cur[k] = nxt[k];
+            const int2 ri = rnext;
+            if (i > i0) {
+                const int32_t *drow = dt_in + (int64_t)(i - 1) * n;
+#pragma unroll
+                for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
+                rnext = __ldg(&rows[i - 1]);
+            }
+            const int ro = ri.y & XTED_ROW_ORL_MASK;
+            const bool trow = ro == imax - 1;
+            const int bord = imax - i;
+            const int rowfar = imax - ro - 1;
+            const int32_t *top = stk + (int64_t)(sp > 0 ? sp - 1 : 0) * stride;
+            int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
+            if (lane == 31) dnext = S.first[warp + 1];
+            int loc[W];
+            const int mine = row_cells<W>(C, prev, cur, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
+            const int incl = warp_suffix_min(mine, lane);
+            if (lane == 0) S.wtot[warp] = incl;
+            __syncthreads();
+            int carry = __shfl_down_sync(FULLMASK, incl, 1);
+            if (lane == 31) carry = XTED_INF;
+            for (int w = warp + 1; w < XTED_WARPS; w++) carry = min(carry, S.wtot[w]);
+            int32_t *orow = dt_out + (int64_t)i * n;
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+                const int d = min(loc[k], carry) - C.key[k];
+                prev[k] = d;
+                if (trow && C.foff[k] == C.dend[k] && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
+            }
+            if (lane == 0) S.first[warp] = prev[0];
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) sp--;
+            if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
+                if (sp < P.stack_rows) {
+                    int32_t *dst = stk + (int64_t)sp * stride + c0;
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if ((C.far >> k) & 1u) dst[k] = prev[k];
+                } else if (tid == 0) {
+                    set_error(P, XTED_ENOMEM, 2, sp, P.stack_rows);
+                }
+                sp++;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane,
+                                int32_t *stk) {
+    const int width = P.chunks[u.chunk].width;
+    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk);
+    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk);
+    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk);
+    else run_narrow<8>(P, pr, u, lane, stk);
+}
+
+// ---------------------------------------------------------------------------
+// Wide unit wider than the register path (one segment of > 2048 columns):
+// the same row step with the row above, the local minima and the far-row
+// stack in block-private global scratch (L1-resident), metadata re-read per row.
+// Scratch layout: prev[width + 1] | loc[width] | stack[stack_rows][width].
+// ---------------------------------------------------------------------------
+__device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *scr,
+                             WideShared &S) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const XRun run = P.runs[u.run];
+    const XChunk ch = P.chunks[u.chunk];
+    const int width = ch.width;
+    const int per = (width + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS;
+    const int c0 = tid * per;
+    const int c1 = min(c0 + per, width);
+    int32_t *prevb = scr;
+    int32_t *locb = scr + width + 1;
+    int32_t *stk = scr + 2 * width + 1;
+    const int4 *cols = P.colinfo + ch.col_lo;
+    const int n = pr.n;
+    const int32_t *dt_in = P.dt + pr.dt_off;
+    int32_t *dt_out = P.dt + pr.dt_off;
+    const int2 *rows = P.rowinfo + pr.row_base;
+    // single segment: key = column index
+    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+        const int i0 = __ldg(&P.krd[kr]);
+        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        for (int c = c0; c < c1; c++) prevb[c] = __ldg(&cols[c]).w;
+        if (tid == 0) prevb[width] = 0;
+        int sp = 0;
+        __syncthreads();
+        for (int i = imax - 1; i >= i0; i--) {
+            const int2 ri = __ldg(&rows[i]);
+            const int ro = ri.y & XTED_ROW_ORL_MASK;
+            const bool trow = ro == imax - 1;
+            const int bord = imax - i;
+            const int rowfar = imax - ro - 1;
+            const int32_t *top = stk + (int64_t)(sp > 0 ? sp - 1 : 0) * width;
+            const int32_t *drow = dt_in + (int64_t)i * n;
+            int run_min = XTED_INF;
+            int diag_next = prevb[c1];  // D[i+1][c1]
+            for (int c = c1 - 1; c >= c0; c--) {
+                const int4 ci = __ldg(&cols[c]);
+                const int foff = ci.z & XTED_COL_FOFF_MASK, dend = ci.w;
+                const int up = prevb[c];
+                int diag = diag_next;
+                diag_next = up;
+                const bool segend = dend == 1;
+                if (segend) diag = bord - 1;
+                const bool tcol = foff == dend;
+                int a;
+                if (trow && tcol) {
+                    a = diag + (ri.x != ci.y);
+                } else {
+                    int far = trow ? dend - foff : (tcol ? rowfar : top[c + foff]);
+                    a = __ldcg(drow + ci.x) + far;
+                }
+                int A = min(a, up + 1);
+                if (segend) A = min(A, bord + 1);
+                run_min = min(run_min, A + c);
+                locb[c] = run_min;
+            }
+            const int incl = warp_suffix_min(run_min, lane);
+            if (lane == 0) S.wtot[warp] = incl;
+            __syncthreads();
+            int carry = __shfl_down_sync(FULLMASK, incl, 1);
+            if (lane == 31) carry = XTED_INF;
+            for (int w = warp + 1; w < XTED_WARPS; w++) carry = min(carry, S.wtot[w]);
+            int32_t *orow = dt_out + (int64_t)i * n;
+            const bool pop = i != i0 && (ri.y & XTED_ROW_ISKR);
+            const bool push = i > i0 && (ri.y & XTED_ROW_PREVLEAF);
+            const int spush = pop ? sp - 1 : sp;
+            if (push && spush >= P.stack_rows && tid == 0) set_error(P, XTED_ENOMEM, 3, spush, P.stack_rows);
+            for (int c = c0; c < c1; c++) {
+                const int4 ci = __ldg(&cols[c]);
+                const int d = min(locb[c], carry) - c;
+                prevb[c] = d;
+                if (trow && (ci.z & XTED_COL_FOFF_MASK) == ci.w) orow[ci.x] = d;
+                if (push && spush < P.stack_rows && (ci.z & XTED_COL_FARCOL))
+                    stk[(int64_t)spush * width + c] = d;
+            }
+            sp = push ? spush + 1 : spush;
+            __syncthreads();
+        }
+    }
+}
+
+__device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
+                              WideShared &S) {
+    const int width = P.chunks[u.chunk].width;
+    if (width <= 256) run_wide<1>(P, pr, u, stk, S);
+    else if (width <= 512) run_wide<2>(P, pr, u, stk, S);
+    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S);
+    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S);
+    else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S);
+    else if (threadIdx.x == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
+}
+
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
+    __shared__ int s_task;
+    __shared__ WideShared S;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int32_t *scratch = P.scratch + (int64_t)blockIdx.x * P.scratch_per_cta;
+    for (;;) {
+        if (tid == 0) {
+            int t = -1;
+            if (*(volatile int32_t *)P.error == 0) {
+                t = atomicAdd(P.task_next, 1);
+                if (t >= P.ntasks) {
+                    t = -1;
+                } else {
+                    const XTask T = P.tasks[t];
+                    if (!wait_ge(P, &P.finished[T.pair], T.need)) {
+                        set_error(P, XTED_ETIMEOUT, t, T.pair, T.need);
+                        t = -1;
+                    }
+                }
+            }
+            s_task = t;
+        }
+        __syncthreads();
+        const int t = s_task;
+        if (t < 0) break;
+        const XTask T = P.tasks[t];
+        const XPair pr = P.pairs[T.pair];
+        if (T.kind_n & XTED_TASK_WIDE) {
+            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S);
+        } else {
+            const int nu = (int)(T.kind_n & 0xffff);
+            if (warp < nu)
+                dispatch_narrow(P, pr, P.units[T.unit_lo + warp], lane,
+                                scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX);
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicAdd(&P.finished[T.pair], 1);
+    }
+}
+
+// Result of pair p: Dtree[0][0] of its table (X-TED_CPU/TED.cpp:188).
+__global__ void xted_gather_kernel(const XPair *pairs, const int32_t *trivial, const int32_t *dt,
+                                   int npairs, int32_t *out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int tv = trivial[p];
+    out[p] = tv >= 0 ? tv : __ldcg(dt + pairs[p].dt_off);
+}
+
+// ---- host-side launch helpers ----
+int dp_occupancy(int *blocks_per_sm) {
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, xted_dp_kernel,
+                                                               XTED_CTA_THREADS, 0);
+}
+
+cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
+    XKernelParams p = P;
+    void *args[] = {&p};
+    return cudaLaunchCooperativeKernel((const void *)xted_dp_kernel, dim3(grid),
+                                       dim3(XTED_CTA_THREADS), args, 0, s);
+}
+
+cudaError_t launch_gather(const XPair *pairs, const int32_t *trivial, const int32_t *dt, int npairs,
+                          int32_t *out, cudaStream_t s) {
+    if (npairs <= 0) return cudaSuccess;
+    xted_gather_kernel<<<(npairs + 255) / 256, 256, 0, s>>>(pairs, trivial, dt, npairs, out);
+    return cudaGetLastError();
+}
+
+}  // namespace xted

@@ -1,0 +1,102 @@
+// xted_internal.h -- data layout shared by the host planner and the kernels.
+//
+// Terminology (reference names in brackets):
+//   row tree A (m nodes) and column tree B (n nodes) of one pair;
+//   orl(v)      rightmost leaf of v's subtree = v + size(v) - 1
+//               [outermost_right_leaves, X-TED_CPU/TED.cpp:21-42];
+//   keyroot     root or a node that is not the last child of its parent
+//               [key_roots, X-TED_CPU/TED.cpp:46-77];
+//   kdepth(k)   keyroot level: 1 + max kdepth of keyroots strictly inside
+//               sub(k), 0 if none [X-TED_CPU/parallel_computing.cpp:93-119];
+//   table (i0,j0) the forest-distance table of one keyroot pair, whose level
+//               is kdepth(i0) + kdepth(j0) [parallel_computing.cpp:121-123].
+//
+// Work decomposition. All keyroots of B with the same kdepth have disjoint
+// subtrees ("segments"); their columns are concatenated per depth into one
+// column list. A *chunk* is a run of whole segments of one depth. A *row run*
+// is a run of whole keyroots of A of one depth. A *unit* = (row run, chunk):
+// every table (i0, j0) with i0 in the run and j0 in the chunk, computed row by
+// row (rows descending, a min-plus suffix scan across the chunk's columns).
+// A *task* is what one thread block claims from the device queue: one wide
+// unit (chunk wider than a warp can hold) or up to 8 narrow units (one per
+// warp), all of one pair and one level.
+#pragma once
+
+#include <stdint.h>
+#include <vector_types.h>  // int2, int4 (CUDA toolkit header, host-includable)
+
+#define XTED_CTA_THREADS 256
+#define XTED_WARPS (XTED_CTA_THREADS / 32)
+#define XTED_NARROW_MAX 256       // widest chunk one warp holds in registers (8 per lane)
+#define XTED_WIDE_REG_MAX 2048    // widest chunk one block holds in registers (8 per thread)
+#define XTED_KEY_BIG (1 << 17)    // key step between segments of one chunk
+#define XTED_INF 0x3fffffff
+
+// rowinfo.y bit layout: orl in the low 20 bits.
+#define XTED_ROW_ORL_MASK 0x000fffff
+#define XTED_ROW_ISKR (1u << 29)     // node is a keyroot
+#define XTED_ROW_PREVLEAF (1u << 30) // node i-1 is a leaf
+
+// colinfo.z bit layout: foff = orl(j) + 1 - j in the low 20 bits.
+#define XTED_COL_FOFF_MASK 0x000fffff
+#define XTED_COL_FARCOL (1u << 30)   // column j-1 is a leaf inside the segment: a far column
+
+// colinfo: x = node j (index in B), y = label(j), z = foff | flags, w = dend = je - j
+// (je = orl(j0) + 1 for the segment's keyroot j0).
+// rowinfo: x = label(i), y = orl(i) | flags.
+
+struct XRun {      // a run of keyroots of one depth of a row tree
+    int32_t kr_lo; // index into the keyroot pool (global)
+    int32_t kr_hi;
+    int32_t rows;  // total rows = sum of subtree sizes
+    int32_t depth;
+};
+
+struct XChunk {     // a run of whole segments of one depth of a column tree
+    int32_t col_lo; // index into the column pool (global)
+    int32_t width;
+    int32_t depth;
+    int32_t nseg;
+};
+
+struct XPair {
+    int64_t dt_off;   // element offset of this pair's m x n distance table
+    int32_t m, n;     // rows (A) and columns (B)
+    int32_t row_base; // index of A's node 0 in the rowinfo pool
+    int32_t pad;
+};
+
+struct XUnit {
+    int32_t run;   // global run index (row tree)
+    int32_t chunk; // global chunk index (column tree)
+};
+
+#define XTED_TASK_WIDE 0x80000000u
+
+struct XTask {
+    int32_t pair;
+    int32_t need;     // tasks of this pair at lower levels that must finish first
+    uint32_t kind_n;  // XTED_TASK_WIDE | number of units
+    int32_t unit_lo;  // first unit
+};
+
+struct XKernelParams {
+    const int2 *rowinfo;  // per node of every row tree
+    const int4 *colinfo;  // per column position of every column tree
+    const int32_t *krd;   // keyroots grouped by depth (node ids within their tree)
+    const XRun *runs;
+    const XChunk *chunks;
+    const XPair *pairs;
+    const XUnit *units;
+    const XTask *tasks;
+    int32_t *dt;          // all distance tables
+    int32_t *scratch;     // per-block far-row stacks (and wide generic rows)
+    int64_t scratch_per_cta; // int32 elements
+    int32_t stack_rows;   // stack capacity in rows
+    int32_t ntasks;
+    int32_t *task_next;   // queue head
+    int32_t *finished;    // per pair finished-task counters
+    int32_t *error;       // 0 = ok; else an XTED error code
+    int32_t *error_info;  // [4] diagnostics of the first error
+    uint64_t timeout_ns;  // bound on each dependency wait
+};

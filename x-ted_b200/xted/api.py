@@ -1,0 +1,157 @@
+"""Host-side interface of the tree-edit-distance path.
+
+``standard_ted`` mirrors the reference entry point
+``int standard_ted(vector<string>& x_node, vector<vector<int>>& x_adj,
+vector<string>& y_node, vector<vector<int>>& y_adj, int num_threads,
+int parallel_version)`` (X-TED_CPU/TED.cpp:177, X-TED_GPU/TED.cu:116):
+same arguments, same meaning, same empty-tree rules. Two differences are
+deliberate: the label lists are not cleared (the reference clears them,
+X-TED_CPU/TED.cpp:160-161), and malformed input raises ``XtedError``
+(XTED_EINVAL) instead of being undefined behaviour. ``num_threads`` and
+``parallel_version`` are accepted and ignored, as X-TED_GPU ignores them.
+
+``Context`` wraps one ``xted_ctx`` (one device, one stream).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .trees import Interner, Tree, from_adjacency
+
+_CTX: Optional["Context"] = None
+
+
+class Context:
+    def __init__(self, device: int = 0, orientation: int = _lib.ORIENT_AUTO,
+                 narrow_width: Optional[int] = None, run_rows: Optional[int] = None,
+                 ctas_per_sm: int = 0, wait_timeout_s: float = 20.0, mem_limit: int = 0):
+        L = _lib.lib()
+        o = _lib.COpts()
+        L.xted_opts_default(ctypes.byref(o))
+        o.device = device
+        o.orientation = orientation
+        if narrow_width is not None:
+            o.narrow_width = narrow_width
+        if run_rows is not None:
+            o.run_rows = run_rows
+        o.ctas_per_sm = ctas_per_sm
+        o.wait_timeout_s = wait_timeout_s
+        o.mem_limit = mem_limit
+        self.opts = o
+        h = ctypes.c_void_p()
+        _lib.check(L.xted_create(ctypes.byref(h), ctypes.byref(o)), "xted_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().xted_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def distance(self, a: Tree, b: Tree) -> int:
+        keep: list = []
+        ca, cb = _lib.ctree(a, keep), _lib.ctree(b, keep)
+        out = ctypes.c_int32(0)
+        _lib.check(_lib.lib().xted_distance(self._h, ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(out)),
+                   "xted_distance")
+        return int(out.value)
+
+    @staticmethod
+    def _views(pairs):
+        """C tree arrays for a pair list; a tree object shared by several pairs
+        is passed once, so the library preprocesses it once."""
+        keep: list = []
+        n = len(pairs)
+        A = (_lib.CTree * max(n, 1))()
+        B = (_lib.CTree * max(n, 1))()
+        cache = {}
+
+        def view(t):
+            k = id(t)
+            if k not in cache:
+                cache[k] = _lib.ctree(t, keep)
+            return cache[k]
+
+        for p, (a, b) in enumerate(pairs):
+            A[p] = view(a)
+            B[p] = view(b)
+        return A, B, keep
+
+    def distance_batch(self, pairs: Sequence[Tuple[Tree, Tree]]) -> np.ndarray:
+        n = len(pairs)
+        A, B, keep = self._views(pairs)
+        out = np.zeros(max(n, 1), np.int32)
+        _lib.check(_lib.lib().xted_distance_batch(self._h, A, B, n, out.ctypes.data_as(_lib._i32p)),
+                   "xted_distance_batch")
+        return out[:n]
+
+    def prepare_batch(self, pairs: Sequence[Tuple[Tree, Tree]]) -> None:
+        """Plan and upload a batch once (inputs resident on the device)."""
+        A, B, keep = self._views(pairs)
+        self._prepared_n = len(pairs)
+        _lib.check(_lib.lib().xted_prepare_batch(self._h, A, B, len(pairs)), "xted_prepare_batch")
+
+    def run_prepared(self) -> np.ndarray:
+        out = np.zeros(max(self._prepared_n, 1), np.int32)
+        _lib.check(_lib.lib().xted_run_prepared(self._h, out.ctypes.data_as(_lib._i32p)), "xted_run_prepared")
+        return out[:self._prepared_n]
+
+    def stats(self) -> dict:
+        s = _lib.CStats()
+        _lib.check(_lib.lib().xted_last_stats(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+
+def default_context() -> Context:
+    global _CTX
+    if _CTX is None:
+        _CTX = Context()
+    return _CTX
+
+
+def pair_cells(a: Tree, b: Tree, orientation: int = _lib.ORIENT_AUTO) -> Tuple[int, int, int]:
+    keep: list = []
+    ca, cb = _lib.ctree(a, keep), _lib.ctree(b, keep)
+    out = (ctypes.c_int64 * 3)()
+    _lib.check(_lib.lib().xted_pair_cells(ctypes.byref(ca), ctypes.byref(cb), orientation, out))
+    return int(out[0]), int(out[1]), int(out[2])
+
+
+def validate(t: Tree) -> bool:
+    keep: list = []
+    c = _lib.ctree(t, keep)
+    return _lib.lib().xted_validate(ctypes.byref(c)) == _lib.XTED_OK
+
+
+def standard_ted(x_node: Sequence[str], x_adj: Sequence[Sequence[int]], y_node: Sequence[str],
+                 y_adj: Sequence[Sequence[int]], num_threads: int = 0, parallel_version: int = 0,
+                 ctx: Optional[Context] = None) -> int:
+    """The reference's entry point (X-TED_CPU/TED.cpp:177-190) on the GPU."""
+    m, n = len(x_adj), len(y_adj)
+    if m == 0:  # X-TED_CPU/TED.cpp:181-186
+        return n
+    if n == 0:
+        return m
+    intern = Interner()
+    a = from_adjacency(intern(x_node), x_adj)
+    b = from_adjacency(intern(y_node), y_adj)
+    return (ctx or default_context()).distance(a, b)
