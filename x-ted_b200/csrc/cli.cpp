@@ -1,0 +1,157 @@
+// cli.cpp -- the X-TED_GPU and X-TED_CPU command lines over the C ABI.
+//
+//   X-TED_GPU <labels.txt> <adj.txt>              (X-TED_GPU/main.cu:4-14)
+//   X-TED_CPU <threads> <labels.txt> <adj.txt>    (X-TED_CPU/main.cpp:4-16)
+//
+// Same argv, same input files, same work as the reference harness
+// (X-TED_CPU/TED_test.cpp:3-49, X-TED_GPU/test_TED.cu:3-56): every line of
+// both files is read, tree pair (0, 1) is computed, and the test is repeated
+// 20 times. Both binaries compute on the GPU; <threads> is accepted and
+// ignored. Per repetition the CPU-named binary prints the reference CPU
+// lines "Total Time for Parallel Computing = X ms" and "The distance = d"
+// (parallel_computing.cpp:184, TED_test.cpp:45); the GPU-named binary prints
+// "Measured time for total parallel execution = X ms" (parallel_X_TED.cu:392),
+// "The distance = d" (which X-TED_GPU never prints) and a blank line
+// (main.cu:11). X is the device time of the tree-distance launch.
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/xted.h"
+
+namespace {
+
+std::vector<std::string> read_lines(const char *path) {
+    std::vector<std::string> out;
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) out.push_back(line);
+    return out;
+}
+
+// Labels: a token ends at each space (X-TED_CPU/dataset_preprocess.cpp:68-81).
+std::vector<std::string> labels_of(const std::string &s) {
+    std::vector<std::string> out;
+    std::string part;
+    for (char ch : s) {
+        if (ch != ' ') part.push_back(ch);
+        else {
+            out.push_back(part);
+            part.clear();
+        }
+    }
+    return out;
+}
+
+// "[[1, 2], [], ...]" -> child lists (X-TED_CPU/dataset_preprocess.cpp:3-66).
+bool adjacency_of(const std::string &line, std::vector<std::vector<int>> &adj) {
+    adj.clear();
+    if (line.size() < 2) return false;
+    const std::string s = line.substr(1, line.size() - 2);
+    size_t i = 0;
+    while (i < s.size()) {
+        if (s[i] != '[') {
+            i++;
+            continue;
+        }
+        size_t k = s.find(']', i);
+        if (k == std::string::npos) return false;
+        std::vector<int> kids;
+        std::string word;
+        for (size_t p = i + 1; p < k; p++) {
+            char ch = s[p];
+            if (ch == ',') {
+                if (!word.empty()) kids.push_back(std::atoi(word.c_str()));
+                word.clear();
+            } else if (ch != ' ') {
+                word.push_back(ch);
+            }
+        }
+        if (!word.empty()) kids.push_back(std::atoi(word.c_str()));
+        adj.push_back(kids);
+        i = k + 1;
+    }
+    return true;
+}
+
+struct CSR {
+    std::vector<int32_t> lab, off, idx;
+};
+
+bool build(const std::vector<std::string> &labs, const std::vector<std::vector<int>> &adj,
+           std::unordered_map<std::string, int32_t> &ids, CSR &t) {
+    if (labs.size() != adj.size()) return false;
+    t.lab.clear();
+    for (const auto &s : labs) t.lab.push_back(ids.emplace(s, (int32_t)ids.size()).first->second);
+    t.off.assign(adj.size() + 1, 0);
+    t.idx.clear();
+    for (size_t v = 0; v < adj.size(); v++) {
+        t.off[v + 1] = t.off[v] + (int32_t)adj[v].size();
+        for (int c : adj[v]) t.idx.push_back(c);
+    }
+    if (t.idx.empty()) t.idx.push_back(0);
+    if (t.lab.empty()) t.lab.push_back(0);
+    return true;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+#ifdef XTED_CLI_CPU
+    const int first = 2;
+    if (argc < 4) {
+        std::fprintf(stderr, "usage: %s <threads> <labels.txt> <adj.txt>\n", argv[0]);
+        return 2;
+    }
+#else
+    const int first = 1;
+    if (argc < 3) {
+        std::fprintf(stderr, "usage: %s <labels.txt> <adj.txt>\n", argv[0]);
+        return 2;
+    }
+#endif
+    xted_ctx *ctx = nullptr;
+    int rc = xted_create(&ctx, nullptr);
+    if (rc) {
+        std::fprintf(stderr, "xted: %s\n", xted_strerror(rc));
+        return 1;
+    }
+    for (int rep = 0; rep < 20; rep++) {
+        const std::vector<std::string> nodes = read_lines(argv[first]);
+        const std::vector<std::string> adjs = read_lines(argv[first + 1]);
+        if (nodes.size() < 2 || adjs.size() < 2) continue;  // the harness only computes pair (0, 1)
+        std::vector<std::vector<int>> a_adj, b_adj;
+        std::unordered_map<std::string, int32_t> ids;
+        CSR A, B;
+        if (!adjacency_of(adjs[0], a_adj) || !adjacency_of(adjs[1], b_adj) ||
+            !build(labels_of(nodes[0]), a_adj, ids, A) || !build(labels_of(nodes[1]), b_adj, ids, B)) {
+            std::fprintf(stderr, "xted: malformed input\n");
+            xted_destroy(ctx);
+            return 1;
+        }
+        xted_tree ta{A.lab.data(), A.off.data(), A.idx.data(), (int32_t)a_adj.size()};
+        xted_tree tb{B.lab.data(), B.off.data(), B.idx.data(), (int32_t)b_adj.size()};
+        int32_t d = 0;
+        rc = xted_distance(ctx, &ta, &tb, &d);
+        if (rc) {
+            std::fprintf(stderr, "xted: %s\n", xted_strerror(rc));
+            xted_destroy(ctx);
+            return 1;
+        }
+        xted_stats st;
+        xted_last_stats(ctx, &st);
+#ifdef XTED_CLI_CPU
+        std::printf("Total Time for Parallel Computing = %g ms\n", st.dp_ms);
+        std::printf("The distance = %d\n", d);
+#else
+        std::printf("Measured time for total parallel execution = %g ms\n", st.dp_ms);
+        std::printf("The distance = %d\n", d);
+        std::printf("\n");
+#endif
+    }
+    xted_destroy(ctx);
+    return 0;
+}
