@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -163,6 +164,15 @@ int ctx_prepare(xted_ctx *c, const Plan &P) {
     K.error_info = cnt + 2;
     K.finished = cnt + 8;
     K.timeout_ns = (uint64_t)(c->opts.wait_timeout_s * 1e9);
+    // Optional per-task trace (XTED_TRACE=<file>): timestamps of every task,
+    // written as raw uint64 quadruples after each run.
+    const char *tr = std::getenv("XTED_TRACE");
+    K.trace = nullptr;
+    if (tr && *tr && K.ntasks > 0) {
+        rc = ctx_dev_reserve(c, c->trace, (size_t)K.ntasks * 4 * sizeof(unsigned long long));
+        if (rc) return rc;
+        K.trace = (unsigned long long *)c->trace.p;
+    }
     c->npairs = npairs;
     c->h2d_bytes = (int64_t)h2d;
     c->prepared = true;
@@ -209,6 +219,16 @@ int ctx_run(xted_ctx *c, int32_t *out) {
     c->stats.d2h_bytes = (int64_t)(res_bytes + 8 * sizeof(int32_t));
     c->stats.grid = c->grid;
     std::memcpy(c->err_info, hres + 2, sizeof(c->err_info));
+    if (K.trace) {
+        std::vector<unsigned long long> tr((size_t)K.ntasks * 4);
+        if (cudaMemcpy(tr.data(), K.trace, tr.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost) ==
+            cudaSuccess) {
+            if (FILE *f = std::fopen(std::getenv("XTED_TRACE"), "wb")) {
+                std::fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
+                std::fclose(f);
+            }
+        }
+    }
     if (hres[1] != 0) return hres[1];
     if (npairs) std::memcpy(out, hres + 8, res_bytes);
     return XTED_OK;
@@ -287,7 +307,7 @@ int xted_destroy(xted_ctx *c) {
     cudaSetDevice(c->opts.device);
     xted::serve_shutdown(c);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&c->meta, &c->dt, &c->scratch, &c->counters})
+    for (DevBuf *b : {&c->meta, &c->dt, &c->scratch, &c->counters, &c->trace})
         if (b->p) cudaFree(b->p);
     for (HostBuf *b : {&c->stage, &c->result})
         if (b->p) cudaFreeHost(b->p);

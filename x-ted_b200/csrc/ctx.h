@@ -31,7 +31,7 @@ struct xted_ctx {
     int grid = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
-    xted::DevBuf meta, dt, scratch, counters;
+    xted::DevBuf meta, dt, scratch, counters, trace;
     xted::HostBuf stage, result;
     const int32_t *d_trivial = nullptr;
     int64_t held = 0;  // device bytes held by this context

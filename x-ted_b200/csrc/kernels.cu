@@ -472,6 +472,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
                 if (t >= P.ntasks) {
                     t = -1;
                 } else {
+                    if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
                     const XTask T = P.tasks[t];
                     if (!wait_ge(P, &P.finished[T.pair], T.need)) {
                         set_error(P, XTED_ETIMEOUT, t, T.pair, T.need);
@@ -486,6 +487,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         if (t < 0) break;
         const XTask T = P.tasks[t];
         const XPair pr = P.pairs[T.pair];
+        if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
         if (T.kind_n & XTED_TASK_WIDE) {
             dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S);
         } else {
@@ -496,7 +498,15 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         }
         __threadfence();
         __syncthreads();
-        if (tid == 0) atomicAdd(&P.finished[T.pair], 1);
+        if (tid == 0) {
+            atomicAdd(&P.finished[T.pair], 1);
+            if (P.trace) {
+                unsigned sm;
+                asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+                P.trace[4 * (int64_t)t + 2] = global_ns();
+                P.trace[4 * (int64_t)t + 3] = (unsigned long long)sm | ((unsigned long long)T.kind_n << 32);
+            }
+        }
     }
 }
 
