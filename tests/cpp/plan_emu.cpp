@@ -1,60 +1,208 @@
-// plan_emu.cpp -- TEST INFRASTRUCTURE: checks the host planner on the CPU.
+// plan_emu.cpp -- TEST INFRASTRUCTURE: checks the batch planner on the CPU.
 //
-// Builds plans for random batches with the product planner (plan.cpp) and
-// executes every unit with the same row formulation the kernels use (row
-// scan with segment keys, far-row stack), sequentially in queue order. It
-// checks the plan's invariants (dependency order, single write of every
-// tree cell, every read cell already written, stack discipline) and the
-// distances against the oracle's restatement of X-TED_CPU.
+// Runs the planner's per-tree / per-pair / per-level functions (plan_core.h,
+// the same code the device planning kernels run one-per-thread) sequentially,
+// orders the level entries by their keys, and executes every unit with the row
+// formulation of the kernels (columns derived from node records, row scan with
+// segment keys, far-row stack), task by task in queue order. It checks the
+// plan's invariants (dependency order, single write of every tree cell, every
+// read cell already written, stack discipline, unit coverage) and the distances
+// against the oracle's restatement of X-TED_CPU.
 //   usage: plan_emu <iterations> <max_nodes> <seed>
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <numeric>
 #include <random>
 #include <vector>
 
 #include "../../include/xted.h"
-#include "../../x-ted_b200/csrc/plan.h"
+#include "../../x-ted_b200/csrc/plan_core.h"
 
 extern "C" int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx, int n,
                            const int32_t *lb, const int32_t *boff, const int32_t *bidx);
 using namespace xted;
 
-#define FAIL(...)                     \
-    do {                              \
-        std::printf(__VA_ARGS__);     \
-        std::printf("\n");            \
-        std::exit(1);                 \
+#define FAIL(...)                 \
+    do {                          \
+        std::printf(__VA_ARGS__); \
+        std::printf("\n");        \
+        std::exit(1);             \
     } while (0)
 
-static void run_unit(const Plan &P, const XPair &pr, const XUnit &u, std::vector<int32_t> &dtv) {
-    int32_t *dt = dtv.data() + pr.dt_off;
-    const XRun run = P.runs[(size_t)u.run];
-    const XChunk ch = P.chunks[(size_t)u.chunk];
-    const int W = ch.width, n = pr.n;
+struct HostPlan {
+    std::vector<int32_t> raw, pair_trees;
+    std::vector<DTree> trees;
+    std::vector<int32_t> size, depth, parent, krd, cumw, opar, okd, oka;
+    std::vector<int2> node;
+    std::vector<XRun> runs;
+    std::vector<XChunk> chunks;
+    std::vector<DDepth> depths;
+    std::vector<DOTree> ot;
+    std::vector<DPair> pairs;
+    std::vector<DLevel> lv;
+    std::vector<XUnit> units;
+    std::vector<XTask> tasks;
+    int stack_rows = 1;
+};
+
+static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<std::vector<int32_t>> &O,
+                 const std::vector<std::vector<int32_t>> &I, const std::vector<int> &nn,
+                 const std::vector<int32_t> &pair_trees, int orientation, int narrow_width, int run_rows,
+                 HostPlan &H) {
+    const int T = (int)nn.size();
+    int64_t N = 0;
+    H.trees.resize((size_t)T);
+    for (int t = 0; t < T; t++) {
+        DTree &d = H.trees[(size_t)t];
+        d.n = nn[(size_t)t];
+        d.raw = (int32_t)H.raw.size();
+        d.nbase = (int32_t)N;
+        d.t = t;
+        const int n = d.n;
+        for (int k = 0; k < n; k++) H.raw.push_back(L[(size_t)t][(size_t)k]);
+        for (int k = 0; k <= n; k++) H.raw.push_back(O[(size_t)t][(size_t)k]);
+        for (int k = 0; k + 1 < n; k++) H.raw.push_back(I[(size_t)t][(size_t)k]);
+        H.raw.push_back(0);
+        N += n;
+    }
+    const size_t N2 = 2 * (size_t)std::max<int64_t>(N, 1);
+    H.size.assign((size_t)N + 1, 0);
+    H.depth.assign((size_t)N + 1, 0);
+    H.parent.assign((size_t)N + 1, 0);
+    H.node.assign(N2, int2{0, 0});
+    H.krd.assign(N2, 0);
+    H.cumw.assign(N2, 0);
+    H.opar.assign(N2, 0);
+    H.okd.assign(N2, 0);
+    H.oka.assign(N2, 0);
+    H.runs.assign(N2, XRun{});
+    H.chunks.assign(N2, XChunk{});
+    H.depths.assign(N2 + 2 * (size_t)T, DDepth{});
+    H.ot.assign(2 * (size_t)T, DOTree{});
+    PlanPools P;
+    P.raw = H.raw.data();
+    P.trees = H.trees.data();
+    P.ntrees = T;
+    P.size = H.size.data();
+    P.depth = H.depth.data();
+    P.parent = H.parent.data();
+    P.node = H.node.data();
+    P.krd = H.krd.data();
+    P.cumw = H.cumw.data();
+    P.runs = H.runs.data();
+    P.chunks = H.chunks.data();
+    P.opar = H.opar.data();
+    P.okd = H.okd.data();
+    P.oka = H.oka.data();
+    P.depths = H.depths.data();
+    P.otrees = H.ot.data();
+    P.run_rows = run_rows;
+    P.narrow_width = narrow_width;
+    for (int t = 0; t < T; t++) tree_basic(P, t, H.trees.data());
+    for (int o = 0; o < 2 * T; o++) orient_tree(P, o);
+    const int np = (int)pair_trees.size() / 2;
+    H.pairs.resize((size_t)np);
+    int64_t dt = 0, ent = 0;
+    for (int p = 0; p < np; p++) {
+        pair_setup(H.trees.data(), H.ot.data(), pair_trees.data(), orientation, p, H.pairs.data());
+        DPair &q = H.pairs[(size_t)p];
+        q.lvl_base = (int32_t)ent;
+        q.dt_off = dt;
+        ent += q.L;
+        if (q.trivial < 0) {
+            dt += (int64_t)H.trees[(size_t)q.ta].n * H.trees[(size_t)q.tb].n;
+            H.stack_rows = std::max(H.stack_rows, H.ot[2 * (size_t)q.ta + q.o].maxka + 1);
+        }
+    }
+    H.lv.resize((size_t)ent);
+    LevelCtx C{H.ot.data(), H.depths.data(), H.runs.data(), H.chunks.data(), H.pairs.data(), narrow_width};
+    std::vector<int64_t> chain((size_t)np, 0);
+    int64_t chain_max = 0;
+    for (int p = 0; p < np; p++) {
+        const DPair &q = H.pairs[(size_t)p];
+        int64_t acc = 0;
+        int32_t need = 0;
+        for (int d = 0; d < q.L; d++) {
+            DLevel &E = H.lv[(size_t)(q.lvl_base + d)];
+            E.pair = p;
+            E.level = d;
+            double est;
+            level_count(C, E, &est);
+            const int64_t e = (int64_t)(est / 64.0) + 1;
+            E.key = acc;
+            E.need = need;
+            acc += e;
+            need += E.ntasks;
+        }
+        chain[(size_t)p] = acc;
+        chain_max = std::max(chain_max, acc);
+    }
+    std::vector<int32_t> order((size_t)ent);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<int64_t> key((size_t)ent);
+    for (size_t e = 0; e < (size_t)ent; e++) key[e] = H.lv[e].key + (chain_max - chain[(size_t)H.lv[e].pair]) / 4;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return key[(size_t)x] < key[(size_t)y]; });
+    int64_t toff = 0, uoff = 0;
+    for (int32_t e : order) {
+        H.lv[(size_t)e].task_off = (int32_t)toff;
+        toff += H.lv[(size_t)e].ntasks;
+    }
+    for (auto &E : H.lv) {
+        E.unit_off = (int32_t)uoff;
+        uoff += (int64_t)E.nwide + E.nnarrow;
+    }
+    H.units.assign((size_t)uoff, XUnit{-1, -1});
+    H.tasks.assign((size_t)toff, XTask{-1, -1, 0, -1});
+    for (auto &E : H.lv) level_fill(C, E, H.units.data(), H.tasks.data());
+}
+
+// One unit, exactly as the kernels compute it (columns derived like load_cols).
+static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vector<int32_t> &dtv,
+                     int narrow_width, bool wide_task) {
+    const DOTree &A = H.ot[2 * (size_t)q.ta + q.o], &B = H.ot[2 * (size_t)q.tb + q.o];
+    int32_t *dt = dtv.data() + q.dt_off;
+    const XRun run = H.runs[(size_t)u.run];
+    const XChunk ch = H.chunks[(size_t)u.chunk];
+    if (!wide_task && ch.width > narrow_width) FAIL("narrow unit wider than the narrow limit");
+    if (wide_task && ch.width <= narrow_width) FAIL("wide unit narrower than the narrow limit");
+    const int W = ch.width, n = B.n;
+    const int2 *cn = H.node.data() + B.node_base;
+    const int2 *rn = H.node.data() + A.node_base;
     std::vector<int> node(W), lab(W), foff(W), dend(W), key(W);
     std::vector<char> far(W);
-    int seg = 0;
+    int seg = 0, s = ch.k_lo;
+    int j0 = H.krd[(size_t)s], je = (cn[j0].y & XTED_ROW_ORL_MASK) + 1, j = j0;
+    if (H.cumw[(size_t)s] + W > H.cumw[(size_t)(ch.k_lo + ch.nseg - 1)] +
+                                    ((cn[H.krd[(size_t)(ch.k_lo + ch.nseg - 1)]].y & XTED_ROW_ORL_MASK) + 1 -
+                                     H.krd[(size_t)(ch.k_lo + ch.nseg - 1)]))
+        FAIL("chunk width exceeds its segments");
     for (int c = 0; c < W; c++) {
-        const int4h ci = P.colinfo[(size_t)(ch.col_lo + c)];
-        node[c] = ci.x;
-        lab[c] = ci.y;
-        foff[c] = ci.z & XTED_COL_FOFF_MASK;
-        far[c] = (ci.z & XTED_COL_FARCOL) != 0;
-        dend[c] = ci.w;
+        if (j >= je) {
+            s++;
+            j0 = H.krd[(size_t)s];
+            je = (cn[j0].y & XTED_ROW_ORL_MASK) + 1;
+            j = j0;
+        }
+        node[c] = j;
+        lab[c] = cn[j].x;
+        foff[c] = (cn[j].y & XTED_ROW_ORL_MASK) + 1 - j;
+        dend[c] = je - j;
+        far[c] = j > j0 && (cn[j].y & XTED_ROW_PREVLEAF);
         key[c] = c + XTED_KEY_BIG * seg;
         if (dend[c] == 1) seg++;
+        j++;
     }
-    if (seg != ch.nseg) FAIL("chunk segment count %d != %d", seg, ch.nseg);
-    std::vector<std::vector<int>> stk((size_t)P.stack_rows, std::vector<int>((size_t)W, -777));
+    if (seg != ch.nseg || s != ch.k_lo + ch.nseg - 1) FAIL("chunk segment count mismatch");
+    std::vector<std::vector<int>> stk((size_t)H.stack_rows, std::vector<int>((size_t)W, -777));
     std::vector<int> prev(W), cur(W), loc(W);
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
-        const int i0 = P.krd[(size_t)kr];
-        const int imax = (P.rowinfo[(size_t)(pr.row_base + i0)].y & XTED_ROW_ORL_MASK) + 1;
+        const int i0 = H.krd[(size_t)kr];
+        const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
         for (int c = 0; c < W; c++) prev[c] = dend[c];
         int sp = 0;
         for (int i = imax - 1; i >= i0; i--) {
-            const int2h ri = P.rowinfo[(size_t)(pr.row_base + i)];
+            const int2 ri = rn[i];
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i, rowfar = imax - ro - 1;
@@ -79,9 +227,9 @@ static void run_unit(const Plan &P, const XPair &pr, const XUnit &u, std::vector
                     if (dv < 0) FAIL("tree distance (%d,%d) read before it was written", i, node[c]);
                     a = dv + fv;
                 }
-                int A = std::min(a, prev[c] + 1);
-                if (se) A = std::min(A, bord + 1);
-                runmin = std::min(runmin, A + key[c]);
+                int Av = std::min(a, prev[c] + 1);
+                if (se) Av = std::min(Av, bord + 1);
+                runmin = std::min(runmin, Av + key[c]);
                 loc[c] = runmin;
             }
             for (int c = 0; c < W; c++) {
@@ -95,7 +243,7 @@ static void run_unit(const Plan &P, const XPair &pr, const XUnit &u, std::vector
             }
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) sp--;
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
-                if (sp >= P.stack_rows) FAIL("far-row stack overflow (%d rows)", P.stack_rows);
+                if (sp >= H.stack_rows) FAIL("far-row stack overflow (%d rows)", H.stack_rows);
                 for (int c = 0; c < W; c++) stk[(size_t)sp][(size_t)c] = far[c] ? prev[c] : -777;
                 sp++;
             }
@@ -106,19 +254,17 @@ static void run_unit(const Plan &P, const XPair &pr, const XUnit &u, std::vector
 
 static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int32_t> &lab,
                 std::vector<int32_t> &off, std::vector<int32_t> &idx) {
-    if (n == 0) {
-        lab.assign(1, 0);
-        off.assign(1, 0);
-        idx.assign(1, 0);
-        return;
-    }
+    lab.clear();
+    off.assign(1, 0);
+    idx.clear();
+    if (n == 0) return;
     std::vector<std::vector<int>> ch((size_t)n);
     for (int i = 1; i < n; i++) {
         int p;
-        if (shape == 0) p = (int)(g() % (uint64_t)i);                      // random recursive
-        else if (shape == 1) p = i < 6 ? 0 : (int)(g() % (uint64_t)std::min(i, 20));  // bushy
-        else if (shape == 2) p = i - 1 - (int)(g() % (uint64_t)std::min(i, 3));       // deep
-        else p = std::max(0, i - 1 - (int)(g() % 2));                      // path-like
+        if (shape == 0) p = (int)(g() % (uint64_t)i);                                   // random recursive
+        else if (shape == 1) p = i < 6 ? 0 : (int)(g() % (uint64_t)std::min(i, 20));   // bushy
+        else if (shape == 2) p = i - 1 - (int)(g() % (uint64_t)std::min(i, 3));        // deep
+        else p = std::max(0, i - 1 - (int)(g() % 2));                                  // path-like
         if (g() % 2) ch[(size_t)p].insert(ch[(size_t)p].begin(), i);
         else ch[(size_t)p].push_back(i);
     }
@@ -133,13 +279,11 @@ static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int
     for (int k = 0; k < n; k++) nid[(size_t)order[(size_t)k]] = k;
     lab.assign((size_t)n, 0);
     off.assign((size_t)n + 1, 0);
-    idx.clear();
     for (int k = 0; k < n; k++) {
         lab[(size_t)k] = (int32_t)(g() % (uint64_t)alpha);
         for (int c : ch[(size_t)order[(size_t)k]]) idx.push_back(nid[(size_t)c]);
         off[(size_t)k + 1] = (int32_t)idx.size();
     }
-    if (idx.empty()) idx.push_back(0);
 }
 
 int main(int argc, char **argv) {
@@ -147,49 +291,53 @@ int main(int argc, char **argv) {
     const int maxn = argc > 2 ? std::atoi(argv[2]) : 300;
     std::mt19937_64 g(argc > 3 ? (uint64_t)std::atoll(argv[3]) : 12345);
     int64_t pairs_checked = 0;
+    const int nws[4] = {0, 7, 64, XTED_NARROW_MAX};
     for (int it = 0; it < iters; it++) {
-        const int npairs = 1 + (int)(g() % 5);
-        std::vector<std::vector<int32_t>> L((size_t)2 * npairs), O((size_t)2 * npairs), I((size_t)2 * npairs);
-        std::vector<TreeView> A((size_t)npairs), B((size_t)npairs);
-        for (int p = 0; p < npairs; p++)
-            for (int s = 0; s < 2; s++) {
-                const size_t k = (size_t)(2 * p + s);
-                const int n = (g() % 4 == 0) ? (int)(g() % 9) : 1 + (int)(g() % (uint64_t)maxn);
-                gen(n, g, 1 + (int)(g() % 6), (int)(g() % 4), L[k], O[k], I[k]);
-                TreeView t{n, L[k].data(), O[k].data(), I[k].data()};
-                (s ? B : A)[(size_t)p] = t;
-            }
-        if (npairs > 1 && g() % 3 == 0) B[0] = A[1];  // shared tree objects
-        PlanOptions opt;
-        opt.orientation = it % 3;
-        const int nws[4] = {0, 7, 64, XTED_NARROW_MAX};
-        opt.narrow_width = nws[it % 4];
-        opt.run_rows = 1 + (int)(g() % 100);
-        Plan P;
-        const int rc = make_plan(A.data(), B.data(), npairs, opt, P);
-        if (rc) FAIL("make_plan returned %d", rc);
-        std::vector<int32_t> dt((size_t)std::max<int64_t>(P.dt_elems, 1), -1);
+        const int ntrees = 1 + (int)(g() % 8);
+        std::vector<std::vector<int32_t>> L((size_t)ntrees), O((size_t)ntrees), I((size_t)ntrees);
+        std::vector<int> nn((size_t)ntrees);
+        for (int t = 0; t < ntrees; t++) {
+            nn[(size_t)t] = (g() % 4 == 0) ? (int)(g() % 9) : 1 + (int)(g() % (uint64_t)maxn);
+            gen(nn[(size_t)t], g, 1 + (int)(g() % 6), (int)(g() % 4), L[(size_t)t], O[(size_t)t], I[(size_t)t]);
+        }
+        const int npairs = 1 + (int)(g() % 6);
+        std::vector<int32_t> pt;
+        for (int p = 0; p < 2 * npairs; p++) pt.push_back((int32_t)(g() % (uint64_t)ntrees));
+        const int orient = it % 3, nw = nws[it % 4], rr = 1 + (int)(g() % 100);
+        HostPlan H;
+        plan(L, O, I, nn, pt, orient, nw, rr, H);
+        int64_t dts = 0;
+        for (auto &q : H.pairs)
+            if (q.trivial < 0) dts += (int64_t)H.trees[(size_t)q.ta].n * H.trees[(size_t)q.tb].n;
+        std::vector<int32_t> dt((size_t)std::max<int64_t>(dts, 1), -1);
         std::vector<int> fin((size_t)npairs, 0);
-        for (const XTask &t : P.tasks) {
+        std::vector<int> unit_seen(H.units.size(), 0);
+        for (const XTask &t : H.tasks) {
+            if (t.pair < 0) FAIL("task slot never filled");
             if (fin[(size_t)t.pair] < t.need) FAIL("task queued before its dependencies");
             const int nu = (int)(t.kind_n & 0xffff);
-            if (nu < 1 || nu > XTED_WARPS) FAIL("bad unit count %d", nu);
-            for (int u = 0; u < nu; u++) {
-                const XUnit &un = P.units[(size_t)(t.unit_lo + u)];
-                const int w = P.chunks[(size_t)un.chunk].width;
-                const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
-                if (!wide && w > opt.narrow_width) FAIL("narrow unit wider than the narrow limit");
-                run_unit(P, P.pairs[(size_t)t.pair], un, dt);
+            const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
+            if (nu < 1 || nu > XTED_TASK_UNITS || (wide && nu != 1)) FAIL("bad unit count %d", nu);
+            for (int k = 0; k < nu; k++) {
+                unit_seen[(size_t)(t.unit_lo + k)]++;
+                run_unit(H, H.pairs[(size_t)t.pair], H.units[(size_t)(t.unit_lo + k)], dt, nw, wide);
             }
             fin[(size_t)t.pair]++;
         }
+        for (int v : unit_seen)
+            if (v != 1) FAIL("unit covered %d times", v);
         for (int p = 0; p < npairs; p++) {
-            const int got = P.trivial[(size_t)p] >= 0 ? P.trivial[(size_t)p] : dt[(size_t)P.pairs[(size_t)p].dt_off];
-            const int want = xo_distance(A[(size_t)p].n, A[(size_t)p].labels, A[(size_t)p].off, A[(size_t)p].idx,
-                                         B[(size_t)p].n, B[(size_t)p].labels, B[(size_t)p].off, B[(size_t)p].idx);
+            const DPair &q = H.pairs[(size_t)p];
+            const int got = q.trivial >= 0 ? q.trivial : dt[(size_t)q.dt_off];
+            const int a = pt[2 * (size_t)p], b = pt[2 * (size_t)p + 1];
+            const int32_t z = 0;
+            const int want = xo_distance(nn[(size_t)a], nn[(size_t)a] ? L[(size_t)a].data() : &z, O[(size_t)a].data(),
+                                         I[(size_t)a].empty() ? &z : I[(size_t)a].data(), nn[(size_t)b],
+                                         nn[(size_t)b] ? L[(size_t)b].data() : &z, O[(size_t)b].data(),
+                                         I[(size_t)b].empty() ? &z : I[(size_t)b].data());
             if (got != want)
-                FAIL("distance mismatch it=%d pair=%d m=%d n=%d got=%d want=%d", it, p, A[(size_t)p].n,
-                     B[(size_t)p].n, got, want);
+                FAIL("distance mismatch it=%d pair=%d m=%d n=%d got=%d want=%d", it, p, nn[(size_t)a],
+                     nn[(size_t)b], got, want);
             pairs_checked++;
         }
     }

@@ -84,67 +84,22 @@ int ctx_host_reserve(HostBuf &b, size_t bytes) {
     return XTED_OK;
 }
 
-// Copies the plan's pools into one pinned buffer and uploads it; fills the
-// pointer fields of the kernel parameters.
-int ctx_upload_plan(xted_ctx *c, const Plan &P, XKernelParams &K, size_t *h2d) {
-    struct Sec { const void *src; size_t bytes; size_t off; };
-    Sec sec[9] = {
-        {P.rowinfo.data(), P.rowinfo.size() * sizeof(int2h), 0},
-        {P.colinfo.data(), P.colinfo.size() * sizeof(int4h), 0},
-        {P.krd.data(), P.krd.size() * sizeof(int32_t), 0},
-        {P.runs.data(), P.runs.size() * sizeof(XRun), 0},
-        {P.chunks.data(), P.chunks.size() * sizeof(XChunk), 0},
-        {P.pairs.data(), P.pairs.size() * sizeof(XPair), 0},
-        {P.units.data(), P.units.size() * sizeof(XUnit), 0},
-        {P.tasks.data(), P.tasks.size() * sizeof(XTask), 0},
-        {P.trivial.data(), P.trivial.size() * sizeof(int32_t), 0},
-    };
-    size_t total = 0;
-    for (auto &s : sec) {
-        s.off = total;
-        total = align_up(total + std::max(s.bytes, (size_t)16), 256);
-    }
-    int rc = ctx_host_reserve(c->stage, total);
-    if (rc) return rc;
-    rc = ctx_dev_reserve(c, c->meta, total);
-    if (rc) return rc;
-    char *h = (char *)c->stage.p;
-    for (auto &s : sec)
-        if (s.bytes) std::memcpy(h + s.off, s.src, s.bytes);
-    if (cudaMemcpyAsync(c->meta.p, h, total, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
-        return XTED_ECUDA;
-    char *d = (char *)c->meta.p;
-    K.rowinfo = (const int2 *)(d + sec[0].off);
-    K.colinfo = (const int4 *)(d + sec[1].off);
-    K.krd = (const int32_t *)(d + sec[2].off);
-    K.runs = (const XRun *)(d + sec[3].off);
-    K.chunks = (const XChunk *)(d + sec[4].off);
-    K.pairs = (const XPair *)(d + sec[5].off);
-    K.units = (const XUnit *)(d + sec[6].off);
-    K.tasks = (const XTask *)(d + sec[7].off);
-    c->d_trivial = (const int32_t *)(d + sec[8].off);
-    *h2d = total;
-    return XTED_OK;
-}
-
-// Uploads a plan and sizes every device buffer it needs; the kernel
-// parameters are kept in the context so the plan can be run repeatedly.
-int ctx_prepare(xted_ctx *c, const Plan &P) {
+// Plans a batch on the device (prep.cu) and sizes every buffer the DP launch
+// needs; the kernel parameters stay in the context so the batch can be run
+// repeatedly from device-resident inputs.
+int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs) {
     c->prepared = false;
-    const int npairs = (int)P.pairs.size();
     XKernelParams &K = c->kp;
-    std::memset(&K, 0, sizeof(K));
-    size_t h2d = 0;
-    int rc = ctx_upload_plan(c, P, K, &h2d);
+    int rc = dev_plan(c, a, b, npairs, K);
     if (rc) return rc;
-    rc = ctx_dev_reserve(c, c->dt, (size_t)std::max<int64_t>(P.dt_elems, 1) * sizeof(int32_t));
+    rc = ctx_dev_reserve(c, c->dt, (size_t)std::max<int64_t>(c->plan_dt_elems, 1) * sizeof(int32_t));
     if (rc) return rc;
+    const int64_t stack_rows = c->plan_stack_rows, max_wide = c->plan_max_wide;
     // per-block scratch: far-row stacks (+ rows of the generic wide path)
-    int64_t per = (int64_t)P.stack_rows * (XTED_WARPS * XTED_NARROW_MAX);
-    if (P.max_wide > 0 && P.max_wide <= XTED_WIDE_REG_MAX)
-        per = std::max<int64_t>(per, (int64_t)P.stack_rows * P.max_wide);
-    if (P.max_wide > XTED_WIDE_REG_MAX)
-        per = std::max<int64_t>(per, 2 * (int64_t)P.max_wide + 1 + (int64_t)P.stack_rows * P.max_wide);
+    int64_t per = stack_rows * (XTED_WARPS * XTED_NARROW_MAX);
+    if (max_wide > 0 && max_wide <= XTED_WIDE_REG_MAX) per = std::max<int64_t>(per, stack_rows * max_wide);
+    if (max_wide > XTED_WIDE_REG_MAX)  // prev | loc | column records (int4) | stack
+        per = std::max<int64_t>(per, 2 * max_wide + 8 + 4 * max_wide + stack_rows * max_wide);
     per = (int64_t)align_up((size_t)per, 64);
     rc = ctx_dev_reserve(c, c->scratch, (size_t)per * (size_t)c->grid * sizeof(int32_t));
     if (rc) return rc;
@@ -157,8 +112,7 @@ int ctx_prepare(xted_ctx *c, const Plan &P) {
     K.dt = (int32_t *)c->dt.p;
     K.scratch = (int32_t *)c->scratch.p;
     K.scratch_per_cta = per;
-    K.stack_rows = P.stack_rows;
-    K.ntasks = (int32_t)P.tasks.size();
+    K.stack_rows = (int32_t)stack_rows;
     K.task_next = cnt;
     K.error = cnt + 1;
     K.error_info = cnt + 2;
@@ -174,7 +128,6 @@ int ctx_prepare(xted_ctx *c, const Plan &P) {
         K.trace = (unsigned long long *)c->trace.p;
     }
     c->npairs = npairs;
-    c->h2d_bytes = (int64_t)h2d;
     c->prepared = true;
     return XTED_OK;
 }
@@ -232,6 +185,16 @@ int ctx_run(xted_ctx *c, int32_t *out) {
     if (hres[1] != 0) return hres[1];
     if (npairs) std::memcpy(out, hres + 8, res_bytes);
     return XTED_OK;
+}
+
+void fill_stats(xted_ctx *c, double plan_ms) {
+    c->stats.pairs = c->npairs;
+    c->stats.cells = c->plan_cells;
+    c->stats.cells_right = c->plan_cells_right;
+    c->stats.tasks = c->kp.ntasks;
+    c->stats.units = c->plan_units;
+    c->stats.levels_max = c->plan_levels_max;
+    c->stats.host_plan_ms = plan_ms;
 }
 
 }  // namespace xted
@@ -323,29 +286,12 @@ int xted_distance_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int
     if (!c || npairs < 0 || (npairs > 0 && (!a || !b || !out))) return XTED_EINVAL;
     const double t0 = now_ms();
     if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
-    std::vector<TreeView> A((size_t)npairs), B((size_t)npairs);
-    for (int p = 0; p < npairs; p++) {
-        A[(size_t)p] = TreeView{a[p].n, a[p].labels, a[p].child_off, a[p].child_idx};
-        B[(size_t)p] = TreeView{b[p].n, b[p].labels, b[p].child_off, b[p].child_idx};
-    }
-    PlanOptions po;
-    po.orientation = c->opts.orientation;
-    po.narrow_width = c->opts.narrow_width;
-    po.run_rows = c->opts.run_rows;
-    Plan &P = c->plan;
-    int rc = make_plan(A.data(), B.data(), npairs, po, P);
+    int rc = ctx_prepare(c, a, b, npairs);
     const double t1 = now_ms();
     std::memset(&c->stats, 0, sizeof(c->stats));
     if (rc) return rc;
-    c->stats.host_plan_ms = t1 - t0;
-    rc = ctx_prepare(c, P);
-    if (!rc) rc = ctx_run(c, out);
-    c->stats.pairs = npairs;
-    c->stats.cells = P.cells;
-    c->stats.cells_right = P.cells_right;
-    c->stats.tasks = (int64_t)P.tasks.size();
-    c->stats.units = (int64_t)P.units.size();
-    c->stats.levels_max = P.levels_max;
+    rc = ctx_run(c, out);
+    fill_stats(c, t1 - t0);
     c->stats.total_ms = now_ms() - t0;
     return rc;
 }
@@ -353,38 +299,20 @@ int xted_distance_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int
 int xted_prepare_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs) {
     if (!c || npairs < 0 || (npairs > 0 && (!a || !b))) return XTED_EINVAL;
     if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
-    std::vector<TreeView> A((size_t)npairs), B((size_t)npairs);
-    for (int p = 0; p < npairs; p++) {
-        A[(size_t)p] = TreeView{a[p].n, a[p].labels, a[p].child_off, a[p].child_idx};
-        B[(size_t)p] = TreeView{b[p].n, b[p].labels, b[p].child_off, b[p].child_idx};
-    }
-    PlanOptions po;
-    po.orientation = c->opts.orientation;
-    po.narrow_width = c->opts.narrow_width;
-    po.run_rows = c->opts.run_rows;
     const double t0 = now_ms();
-    int rc = make_plan(A.data(), B.data(), npairs, po, c->plan);
+    int rc = ctx_prepare(c, a, b, npairs);
     std::memset(&c->stats, 0, sizeof(c->stats));
     if (rc) return rc;
-    c->stats.host_plan_ms = now_ms() - t0;
-    rc = ctx_prepare(c, c->plan);
-    if (rc) return rc;
-    // the upload is asynchronous on the context stream; finish it here so a
-    // following xted_run_prepared times device work only
+    c->prep_ms = now_ms() - t0;
+    c->stats.host_plan_ms = c->prep_ms;
     return cudaStreamSynchronize(c->stream) == cudaSuccess ? XTED_OK : XTED_ECUDA;
 }
 
 int xted_run_prepared(xted_ctx *c, int32_t *out) {
     if (!c || !out) return XTED_EINVAL;
     if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
-    const Plan &P = c->plan;
     const int rc = ctx_run(c, out);
-    c->stats.pairs = (int64_t)P.pairs.size();
-    c->stats.cells = P.cells;
-    c->stats.cells_right = P.cells_right;
-    c->stats.tasks = (int64_t)P.tasks.size();
-    c->stats.units = (int64_t)P.units.size();
-    c->stats.levels_max = P.levels_max;
+    fill_stats(c, c->prep_ms);
     return rc;
 }
 

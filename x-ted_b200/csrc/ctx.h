@@ -5,9 +5,12 @@
 
 #include <cstdint>
 #include <memory>
+#include <unordered_map>
+#include <vector>
 
 #include "../../include/xted.h"
 #include "plan.h"
+#include "plan_core.h"
 
 namespace xted {
 
@@ -22,6 +25,7 @@ struct HostBuf {
 };
 
 struct ServeState;  // serve.cpp
+struct DTree;       // plan_core.h
 
 }  // namespace xted
 
@@ -31,18 +35,25 @@ struct xted_ctx {
     int grid = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
-    xted::DevBuf meta, dt, scratch, counters, trace;
-    xted::HostBuf stage, result;
+    xted::DevBuf meta, levels, work, dt, scratch, counters, trace;
+    xted::HostBuf stage, result, summary;
     const int32_t *d_trivial = nullptr;
     int64_t held = 0;  // device bytes held by this context
-    xted::Plan plan;
     xted_stats stats{};
     int32_t err_info[4] = {0, 0, 0, 0};
     xted::ServeState *serve = nullptr;  // owned; released by serve_shutdown
+    // device planning: host-side bookkeeping of the current batch
+    std::unordered_map<xted::TreeKey, int, xted::TreeKeyHash> tree_ids;
+    std::vector<xted::TreeView> uniq;
+    std::vector<int32_t> pair_trees;
+    std::vector<xted::DTree> htrees;
+    int64_t plan_dt_elems = 0, plan_cells = 0, plan_cells_right = 0, plan_units = 0;
+    int32_t plan_stack_rows = 1, plan_max_wide = 0, plan_levels_max = 0;
     // the prepared plan (xted_prepare_batch / every batch call)
     XKernelParams kp{};
     int32_t npairs = 0;
     int64_t h2d_bytes = 0;
+    double prep_ms = 0;
     bool prepared = false;
 };
 
@@ -50,8 +61,10 @@ namespace xted {
 
 int ctx_dev_reserve(xted_ctx *c, DevBuf &b, size_t bytes);
 int ctx_host_reserve(HostBuf &b, size_t bytes);
-int ctx_prepare(xted_ctx *c, const Plan &P);
+int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs);
+int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs, XKernelParams &K);
 int ctx_run(xted_ctx *c, int32_t *out);
+void fill_stats(xted_ctx *c, double plan_ms);
 void serve_shutdown(xted_ctx *c);
 
 }  // namespace xted

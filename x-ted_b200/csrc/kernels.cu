@@ -92,24 +92,48 @@ struct Cols {
     unsigned valid; // bit k: column k exists
 };
 
-// Loads the thread's columns [c0, c0+W) of a chunk. `before` = segment ends
-// strictly before column c0 (computed by the caller's scan).
+// Loads the thread's columns [c0, c0+W) of a chunk: finds the segment of
+// column c0 by binary search over the segments' column positions, then walks
+// the keyroots' subtrees, deriving each column from the column tree's node
+// records (label, orl, previous-node-is-leaf flag).
 template <int W>
-__device__ __forceinline__ void load_cols(const XKernelParams &P, const XChunk &ch, int c0,
+__device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &pr, const XChunk &ch, int c0,
                                           Cols<W> &C) {
     C.far = 0;
     C.valid = 0;
+    const int2 *nodes = P.rowinfo + pr.col_base;
+    int s = ch.k_lo, j = 0, j0 = 0, je = 0;
+    if (c0 < ch.width) {
+        const int32_t pos0 = __ldg(&P.cumw[ch.k_lo]) + c0;
+        int lo = ch.k_lo, hi = ch.k_lo + ch.nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&P.cumw[mid]) <= pos0) lo = mid;
+            else hi = mid - 1;
+        }
+        s = lo;
+        j0 = __ldg(&P.krd[s]);
+        je = (__ldg(&nodes[j0]).y & XTED_ROW_ORL_MASK) + 1;
+        j = j0 + (pos0 - __ldg(&P.cumw[s]));
+    }
 #pragma unroll
     for (int k = 0; k < W; k++) {
         const int c = c0 + k;
         if (c < ch.width) {
-            const int4 ci = __ldg(&P.colinfo[ch.col_lo + c]);
-            C.node[k] = ci.x;
-            C.lab[k] = ci.y;
-            C.foff[k] = ci.z & XTED_COL_FOFF_MASK;
-            C.dend[k] = ci.w;
-            if (ci.z & XTED_COL_FARCOL) C.far |= 1u << k;
+            if (j >= je) {
+                s++;
+                j0 = __ldg(&P.krd[s]);
+                je = (__ldg(&nodes[j0]).y & XTED_ROW_ORL_MASK) + 1;
+                j = j0;
+            }
+            const int2 nd = __ldg(&nodes[j]);
+            C.node[k] = j;
+            C.lab[k] = nd.x;
+            C.foff[k] = (nd.y & XTED_ROW_ORL_MASK) + 1 - j;
+            C.dend[k] = je - j;
+            if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) C.far |= 1u << k;
             C.valid |= 1u << k;
+            j++;
         } else {
             C.node[k] = 0;
             C.lab[k] = 0;
@@ -171,16 +195,53 @@ __device__ __forceinline__ int row_cells(const Cols<W> &C, const int (&prev)[W],
 }
 
 // ---------------------------------------------------------------------------
+// Row prefetch. Tree distances of the rows a unit will reach next do not
+// depend on the unit's own work (they were written at lower levels), so each
+// thread keeps XTED_PREFETCH rows of its columns in flight with cp.async into
+// a shared-memory ring, plus the row's node record (copied by one thread).
+// L1-allocating copies are safe here: every task starts after an acquire of
+// its pair's counter and a block barrier, the pattern grid-wide sync relies on.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async4(int32_t *smem, const int32_t *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+#define NARROW_SLOT (XTED_NARROW_MAX + 8)  // ints per ring slot: columns, then the row record
+#define WIDE_SLOT (XTED_WIDE_REG_MAX + 8)
+#define RING_INTS ((XTED_WARPS * XTED_PREFETCH * NARROW_SLOT) > (XTED_PREFETCH * WIDE_SLOT) \
+                       ? (XTED_WARPS * XTED_PREFETCH * NARROW_SLOT)                          \
+                       : (XTED_PREFETCH * WIDE_SLOT))
+
+// Issues the copies of row r (this thread's columns; one thread: the record).
+template <int W>
+__device__ __forceinline__ void issue_row(const Cols<W> &C, const int32_t *dt, int n, const int2 *rows, int r,
+                                          int32_t *slot, int rec_at, int c0, bool rec) {
+    const int32_t *drow = dt + (int64_t)r * n;
+#pragma unroll
+    for (int k = 0; k < W; k++)
+        if ((C.valid >> k) & 1u) cp_async4(slot + c0 + k, drow + C.node[k]);
+    if (rec) cp_async8(slot + rec_at, rows + r);
+}
+
+// ---------------------------------------------------------------------------
 // Narrow unit: one warp, chunk width <= 32*W.
 // ---------------------------------------------------------------------------
 template <int W>
-__device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane,
-                           int32_t *stk) {
+__device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
+                           int32_t *ring) {
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = lane * W;
     Cols<W> C;
-    load_cols<W>(P, ch, c0, C);
+    load_cols<W>(P, pr, ch, c0, C);
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -191,31 +252,36 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     int32_t *dt_out = P.dt + pr.dt_off;
     const int2 *rows = P.rowinfo + pr.row_base;
     const int stride = XTED_NARROW_MAX;
+    constexpr int PF = XTED_PREFETCH;
 
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
-        int prev[W], nxt[W];
+        int prev[W];
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k];
         int sp = 0;
-        {
-            const int32_t *drow = dt_in + (int64_t)(imax - 1) * n;
+        __syncwarp();  // the ring's previous readers are done
 #pragma unroll
-            for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
+        for (int q = 0; q < PF - 1; q++) {
+            const int r = imax - 1 - q;
+            if (r >= i0) issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, stride, c0, lane == 0);
+            cp_async_commit();
         }
-        int2 rnext = __ldg(&rows[imax - 1]);
         for (int i = imax - 1; i >= i0; i--) {
+            {
+                const int r = i - (PF - 1);
+                if (r >= i0)
+                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, stride, c0, lane == 0);
+                cp_async_commit();
+            }
+            cp_async_wait<PF - 1>();
+            __syncwarp();
+            const int32_t *slot = ring + (i & (PF - 1)) * NARROW_SLOT;
             int cur[W];
 #pragma unroll
-            for (int k = 0; k < W; k++) cur[k] = nxt[k];
-            const int2 ri = rnext;
-            if (i > i0) {
-                const int32_t *drow = dt_in + (int64_t)(i - 1) * n;
-#pragma unroll
-                for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
-                rnext = __ldg(&rows[i - 1]);
-            }
+            for (int k = 0; k < W; k++) cur[k] = slot[c0 + k];
+            const int2 ri = *(const int2 *)(slot + stride);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
@@ -250,6 +316,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             __syncwarp();
         }
     }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -262,15 +329,16 @@ struct WideShared {
 };
 
 template <int W>
-__device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
-                         WideShared &S) {
+__device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
+                         int32_t *ring) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = tid * W;
     const int stride = ch.width;
+    constexpr int PF = XTED_PREFETCH;
     Cols<W> C;
-    load_cols<W>(P, ch, c0, C);
+    load_cols<W>(P, pr, ch, c0, C);
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -288,30 +356,35 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
-        int prev[W], nxt[W];
+        int prev[W];
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        int sp = 0;
+        __syncthreads();  // the ring's and S.first's previous readers are done
         if (lane == 0) S.first[warp] = prev[0];
         if (tid == 0) S.first[XTED_WARPS] = 0;
-        int sp = 0;
-        {
-            const int32_t *drow = dt_in + (int64_t)(imax - 1) * n;
 #pragma unroll
-            for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
+        for (int q = 0; q < PF - 1; q++) {
+            const int r = imax - 1 - q;
+            if (r >= i0)
+                issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, XTED_WIDE_REG_MAX, c0, tid == 0);
+            cp_async_commit();
         }
-        int2 rnext = __ldg(&rows[imax - 1]);
+        cp_async_wait<PF - 2>();
         __syncthreads();
         for (int i = imax - 1; i >= i0; i--) {
+            {
+                const int r = i - (PF - 1);
+                if (r >= i0)
+                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, XTED_WIDE_REG_MAX, c0,
+                                 tid == 0);
+                cp_async_commit();
+            }
+            const int32_t *slot = ring + (i & (PF - 1)) * WIDE_SLOT;
             int cur[W];
 #pragma unroll
-            for (int k = 0; k < W; k++) cur[k] = nxt[k];
-            const int2 ri = rnext;
-            if (i > i0) {
-                const int32_t *drow = dt_in + (int64_t)(i - 1) * n;
-#pragma unroll
-                for (int k = 0; k < W; k++) nxt[k] = ((C.valid >> k) & 1u) ? __ldcg(drow + C.node[k]) : 0;
-                rnext = __ldg(&rows[i - 1]);
-            }
+            for (int k = 0; k < W; k++) cur[k] = slot[c0 + k];
+            const int2 ri = *(const int2 *)(slot + XTED_WIDE_REG_MAX);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
@@ -347,18 +420,20 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
                 }
                 sp++;
             }
-            __syncthreads();
+            cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
+            __syncthreads();          // ... and everyone's, the record and the stack push
         }
     }
+    cp_async_wait<0>();
 }
 
-__device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane,
-                                int32_t *stk) {
+__device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
+                                int32_t *ring) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk);
-    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk);
-    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk);
-    else run_narrow<8>(P, pr, u, lane, stk);
+    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk, ring);
+    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk, ring);
+    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk, ring);
+    else run_narrow<8>(P, pr, u, lane, stk, ring);
 }
 
 // ---------------------------------------------------------------------------
@@ -378,8 +453,20 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     const int c1 = min(c0 + per, width);
     int32_t *prevb = scr;
     int32_t *locb = scr + width + 1;
-    int32_t *stk = scr + 2 * width + 1;
-    const int4 *cols = P.colinfo + ch.col_lo;
+    int4 *cols = (int4 *)(scr + ((2 * width + 4) & ~3));
+    int32_t *stk = (int32_t *)(cols + width);
+    {   // derive this thread's columns once per unit (single segment: keyroot k_lo)
+        const int2 *nodes = P.rowinfo + pr.col_base;
+        const int j0 = __ldg(&P.krd[ch.k_lo]);
+        const int je = j0 + width;
+        for (int c = c0; c < c1; c++) {
+            const int j = j0 + c;
+            const int2 nd = __ldg(&nodes[j]);
+            uint32_t z = (uint32_t)((nd.y & XTED_ROW_ORL_MASK) + 1 - j);
+            if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) z |= XTED_COL_FARCOL;
+            cols[c] = make_int4(j, nd.x, (int)z, je - j);
+        }
+    }
     const int n = pr.n;
     const int32_t *dt_in = P.dt + pr.dt_off;
     int32_t *dt_out = P.dt + pr.dt_off;
@@ -388,7 +475,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
-        for (int c = c0; c < c1; c++) prevb[c] = __ldg(&cols[c]).w;
+        for (int c = c0; c < c1; c++) prevb[c] = cols[c].w;
         if (tid == 0) prevb[width] = 0;
         int sp = 0;
         __syncthreads();
@@ -403,7 +490,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
             int run_min = XTED_INF;
             int diag_next = prevb[c1];  // D[i+1][c1]
             for (int c = c1 - 1; c >= c0; c--) {
-                const int4 ci = __ldg(&cols[c]);
+                const int4 ci = cols[c];
                 const int foff = ci.z & XTED_COL_FOFF_MASK, dend = ci.w;
                 const int up = prevb[c];
                 int diag = diag_next;
@@ -435,7 +522,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
             const int spush = pop ? sp - 1 : sp;
             if (push && spush >= P.stack_rows && tid == 0) set_error(P, XTED_ENOMEM, 3, spush, P.stack_rows);
             for (int c = c0; c < c1; c++) {
-                const int4 ci = __ldg(&cols[c]);
+                const int4 ci = cols[c];
                 const int d = min(locb[c], carry) - c;
                 prevb[c] = d;
                 if (trow && (ci.z & XTED_COL_FOFF_MASK) == ci.w) orow[ci.x] = d;
@@ -449,19 +536,20 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
 }
 
 __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
-                              WideShared &S) {
+                              WideShared &S, int32_t *ring) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 256) run_wide<1>(P, pr, u, stk, S);
-    else if (width <= 512) run_wide<2>(P, pr, u, stk, S);
-    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S);
-    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S);
+    if (width <= 256) run_wide<1>(P, pr, u, stk, S, ring);
+    else if (width <= 512) run_wide<2>(P, pr, u, stk, S, ring);
+    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S, ring);
+    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S, ring);
     else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S);
     else if (threadIdx.x == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
 }
 
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
-    __shared__ int s_task;
+    __shared__ int s_task, s_next;
     __shared__ WideShared S;
+    __shared__ __align__(16) int32_t s_ring[RING_INTS];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int32_t *scratch = P.scratch + (int64_t)blockIdx.x * P.scratch_per_cta;
     for (;;) {
@@ -481,6 +569,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
                 }
             }
             s_task = t;
+            s_next = 0;
         }
         __syncthreads();
         const int t = s_task;
@@ -489,12 +578,19 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         const XPair pr = P.pairs[T.pair];
         if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
         if (T.kind_n & XTED_TASK_WIDE) {
-            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S);
+            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S, s_ring);
         } else {
+            // the block's warps take the task's units one at a time
             const int nu = (int)(T.kind_n & 0xffff);
-            if (warp < nu)
-                dispatch_narrow(P, pr, P.units[T.unit_lo + warp], lane,
-                                scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX);
+            int32_t *stk = scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX;
+            int32_t *ring = s_ring + warp * (XTED_PREFETCH * NARROW_SLOT);
+            for (;;) {
+                int k = 0;
+                if (lane == 0) k = atomicAdd(&s_next, 1);
+                k = __shfl_sync(FULLMASK, k, 0);
+                if (k >= nu) break;
+                dispatch_narrow(P, pr, P.units[T.unit_lo + k], lane, stk, ring);
+            }
         }
         __threadfence();
         __syncthreads();

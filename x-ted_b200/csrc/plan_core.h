@@ -1,0 +1,374 @@
+// plan_core.h -- keyroot preprocessing and work decomposition, as functions of
+// one tree, one pair or one level so they run one-per-thread on the device
+// (prep.cu) and sequentially on the host in the planner's CPU test.
+//
+// Reference counterparts:
+//   orl(v) = v + size(v) - 1                  X-TED_CPU/TED.cpp:21-42
+//   keyroots = root + non-last children       X-TED_CPU/TED.cpp:46-77 (topmost node per orl)
+//   kdepth: bottom-up over parent pointers    X-TED_CPU/parallel_computing.cpp:93-119
+//   level of table (i0,j0) = kdepth(i0)+kdepth(j0)   parallel_computing.cpp:121-123
+// The left-path decomposition is the right-path one on the mirrored tree
+// (children reversed), whose preorder id of node v is n-1-post(v) with
+// post(v) = v - depth(v) + size(v) - 1.
+#pragma once
+
+#include <stdint.h>
+
+#include "xted_internal.h"
+
+#ifdef __CUDACC__
+#define XT_HD __host__ __device__
+#else
+#define XT_HD
+#endif
+
+namespace xted {
+
+// One input tree. Raw preorder CSR in the flat input buffer:
+// labels at raw, child_off at raw + n, child_idx at raw + 2n + 1.
+struct DTree {
+    int32_t n;
+    int32_t raw;
+    int32_t nbase;  // prefix sum of n over trees (node pools)
+    int32_t t;      // tree index
+    int64_t S[2];   // keyroot subtree-size sums: right-path, left-path
+};
+
+// One depth level of one oriented tree.
+struct DDepth {
+    int32_t krd_lo, krd_hi;       // keyroots of this depth (pool indices, preorder)
+    int32_t run_lo, run_hi;       // row runs
+    int32_t chunk_lo, nnarrow, nwide;  // chunks: narrow ones first, then wide ones
+    int32_t maxrows, maxw_n, maxw_w;   // largest run and chunk widths (cost estimates)
+    int32_t pad0, pad1;
+};
+
+// One tree in one orientation (index 2 * tree + o; o = 1 mirrored).
+struct DOTree {
+    int32_t n, D, maxka, maxw_wide;
+    int32_t node_base;   // rowinfo/krd/cumw/runs/chunks pool base (capacity n each)
+    int32_t depth_base;  // DDepth pool base (capacity n + 1)
+    int64_t S;
+};
+
+struct DPair {
+    int32_t ta, tb;      // input trees
+    int32_t o;           // orientation: 0 right path, 1 left path (mirrored)
+    int32_t L;           // levels (0 for a pair with an empty tree)
+    int32_t lvl_base;    // first level entry
+    int32_t trivial;     // distance of a pair with an empty tree, else -1
+    int64_t dt_off;
+    int64_t cells;
+};
+
+struct DLevel {
+    int32_t pair, level;
+    int32_t nwide, nnarrow;
+    int32_t ntasks, need;  // tasks at this level; tasks of the pair at lower levels
+    int32_t task_off, unit_off;
+    int64_t key;           // queue position key (smaller first), see k_pair_rank
+};
+
+struct PlanPools {
+    const int32_t *raw;   // input trees
+    const DTree *trees;
+    int32_t ntrees;
+    // per input tree node scratch (original numbering)
+    int32_t *size, *depth, *parent;
+    // per oriented tree node pools (capacity 2 * sum n)
+    int2 *node;           // rowinfo: label, orl | flags
+    int32_t *krd, *cumw;  // keyroots by depth, their column-list position within the depth
+    XRun *runs;
+    XChunk *chunks;
+    int32_t *opar, *okd, *oka;  // orientation scratch
+    DDepth *depths;       // capacity 2 * (sum n + ntrees)
+    DOTree *otrees;
+    int32_t run_rows, narrow_width;
+};
+
+XT_HD inline int32_t mirror_id(int32_t v, int32_t n, const int32_t *size, const int32_t *depth) {
+    return n - 1 - (v - depth[v] + size[v] - 1);
+}
+
+// Sizes, depths, parents and both keyroot-size sums of input tree t.
+XT_HD inline void tree_basic(const PlanPools &P, int t, DTree *trees_out) {
+    DTree T = P.trees[t];
+    const int n = T.n;
+    const int32_t *off = P.raw + T.raw + n;
+    const int32_t *idx = P.raw + T.raw + 2 * n + 1;
+    int32_t *size = P.size + T.nbase, *depth = P.depth + T.nbase, *par = P.parent + T.nbase;
+    T.S[0] = T.S[1] = 0;
+    if (n > 0) {
+        par[0] = -1;
+        depth[0] = 0;
+        for (int v = 0; v < n; v++)
+            for (int32_t e = off[v]; e < off[v + 1]; e++) {
+                par[idx[e]] = v;
+                depth[idx[e]] = depth[v] + 1;
+            }
+        for (int v = n - 1; v >= 0; v--) {
+            int32_t s = 1;
+            for (int32_t e = off[v]; e < off[v + 1]; e++) s += size[idx[e]];
+            size[v] = s;
+        }
+        int64_t sr = size[0], sl = size[0];
+        for (int v = 0; v < n; v++) {
+            const int32_t lo = off[v], hi = off[v + 1];
+            for (int32_t e = lo; e < hi; e++) {
+                if (e != hi - 1) sr += size[idx[e]];
+                if (e != lo) sl += size[idx[e]];
+            }
+        }
+        T.S[0] = sr;
+        T.S[1] = sl;
+    }
+    trees_out[t] = T;
+}
+
+XT_HD inline double row_cost_est(bool wide, int width) {
+    if (width <= 0) return 0.0;
+    if (!wide) return 64.0 + 16.0 * ((width + 31) / 32);
+    return 280.0 + 16.0 * ((width + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS);
+}
+
+// Builds oriented tree ot = 2 t + o: node records, keyroot depths, keyroots
+// grouped by depth, column-list positions, row runs and column chunks.
+XT_HD inline void orient_tree(const PlanPools &P, int ot) {
+    const int t = ot >> 1, o = ot & 1;
+    const DTree T = P.trees[t];
+    const int n = T.n;
+    DOTree O;
+    O.n = n;
+    O.node_base = 2 * T.nbase + o * n;
+    O.depth_base = 2 * (T.nbase + t) + o * (n + 1);
+    O.D = -1;
+    O.maxka = 0;
+    O.maxw_wide = 0;
+    O.S = T.S[o];
+    if (n == 0) {
+        P.otrees[ot] = O;
+        return;
+    }
+    const int32_t *lab = P.raw + T.raw;
+    const int32_t *off = P.raw + T.raw + n;
+    const int32_t *idx = P.raw + T.raw + 2 * n + 1;
+    const int32_t *size = P.size + T.nbase, *depth = P.depth + T.nbase, *par = P.parent + T.nbase;
+    int2 *node = P.node + O.node_base;
+    int32_t *opar = P.opar + O.node_base, *okd = P.okd + O.node_base, *oka = P.oka + O.node_base;
+    // node records in this orientation
+    for (int v = 0; v < n; v++) {
+        const int32_t u = o ? mirror_id(v, n, size, depth) : v;
+        bool kr = true;
+        if (v > 0) {
+            const int32_t p = par[v];
+            kr = o ? idx[off[p]] != v : idx[off[p + 1] - 1] != v;
+            opar[u] = o ? mirror_id(p, n, size, depth) : p;
+        } else {
+            opar[u] = -1;
+        }
+        node[u].x = lab[v];
+        node[u].y = (int32_t)((uint32_t)(u + size[v] - 1) | (kr ? XTED_ROW_ISKR : 0u));
+    }
+    for (int u = 1; u < n; u++) {
+        const int32_t prev_orl = node[u - 1].y & XTED_ROW_ORL_MASK;
+        if (prev_orl == u - 1) node[u].y = (int32_t)((uint32_t)node[u].y | XTED_ROW_PREVLEAF);
+    }
+    // keyroot depth bottom-up: oka[u] collects the max over u's children of
+    // f(child) = max kdepth of keyroots in the child's subtree (-1 if none)
+    for (int u = 0; u < n; u++) oka[u] = -1;
+    for (int u = n - 1; u >= 0; u--) {
+        const bool kr = (node[u].y & XTED_ROW_ISKR) != 0;
+        const int32_t f = kr ? oka[u] + 1 : oka[u];
+        okd[u] = kr ? f : -1;
+        if (u > 0 && f > oka[opar[u]]) oka[opar[u]] = f;
+    }
+    O.D = okd[0];
+    // keyroots on each root path
+    int32_t maxka = 1;
+    oka[0] = 1;
+    for (int u = 1; u < n; u++) {
+        oka[u] = oka[opar[u]] + ((node[u].y & XTED_ROW_ISKR) ? 1 : 0);
+        if (oka[u] > maxka) maxka = oka[u];
+    }
+    O.maxka = maxka;
+    // keyroots grouped by depth (counting sort, preorder inside a depth)
+    DDepth *dep = P.depths + O.depth_base;
+    const int D = O.D;
+    for (int d = 0; d <= D; d++) {
+        dep[d].krd_lo = 0;
+        dep[d].krd_hi = 0;
+    }
+    for (int u = 0; u < n; u++)
+        if (okd[u] >= 0) dep[okd[u]].krd_hi++;
+    int32_t acc = O.node_base;
+    for (int d = 0; d <= D; d++) {
+        const int32_t c = dep[d].krd_hi;
+        dep[d].krd_lo = acc;
+        dep[d].krd_hi = acc;  // fill cursor
+        acc += c;
+    }
+    for (int u = 0; u < n; u++)
+        if (okd[u] >= 0) P.krd[dep[okd[u]].krd_hi++] = u;
+    // column-list positions, row runs and chunks per depth
+    const int nw = P.narrow_width;
+    const int group_w = nw > 0 ? nw : XTED_NARROW_MAX;
+    const int run_rows = P.run_rows;
+    int32_t run_cur = O.node_base, chunk_cur = O.node_base;
+    for (int d = 0; d <= D; d++) {
+        DDepth &dd = dep[d];
+        int32_t pos = 0;
+        dd.maxrows = 0;
+        // runs
+        dd.run_lo = run_cur;
+        XRun r{-1, -1, 0, d};
+        for (int32_t k = dd.krd_lo; k < dd.krd_hi; k++) {
+            const int32_t u = P.krd[k];
+            const int32_t sz = (node[u].y & XTED_ROW_ORL_MASK) - u + 1;
+            P.cumw[k] = pos;
+            pos += sz;
+            if (r.kr_lo >= 0 && r.rows + sz > run_rows) {
+                if (r.rows > dd.maxrows) dd.maxrows = r.rows;
+                P.runs[run_cur++] = r;
+                r = XRun{-1, -1, 0, d};
+            }
+            if (r.kr_lo < 0) r.kr_lo = k;
+            r.kr_hi = k + 1;
+            r.rows += sz;
+        }
+        if (r.kr_lo >= 0) {
+            if (r.rows > dd.maxrows) dd.maxrows = r.rows;
+            P.runs[run_cur++] = r;
+        }
+        dd.run_hi = run_cur;
+        // chunks: two passes, narrow chunks first
+        dd.chunk_lo = chunk_cur;
+        dd.nnarrow = dd.nwide = 0;
+        dd.maxw_n = dd.maxw_w = 0;
+        for (int pass = 0; pass < 2; pass++) {
+            XChunk c{-1, 0, d, 0};
+            for (int32_t k = dd.krd_lo; k <= dd.krd_hi; k++) {
+                int32_t w = 0;
+                if (k < dd.krd_hi) {
+                    const int32_t u = P.krd[k];
+                    w = (node[u].y & XTED_ROW_ORL_MASK) - u + 1;
+                }
+                const bool flush = c.nseg > 0 && (k == dd.krd_hi || c.width + w > group_w);
+                if (flush) {
+                    const bool wide = c.width > nw;
+                    if (wide == (pass == 1)) {
+                        P.chunks[chunk_cur++] = c;
+                        if (wide) {
+                            dd.nwide++;
+                            if (c.width > dd.maxw_w) dd.maxw_w = c.width;
+                        } else {
+                            dd.nnarrow++;
+                            if (c.width > dd.maxw_n) dd.maxw_n = c.width;
+                        }
+                    }
+                    c = XChunk{-1, 0, d, 0};
+                }
+                if (k == dd.krd_hi) break;
+                if (c.nseg == 0) c.k_lo = k;  // first segment (keyroot pool index)
+                c.width += w;
+                c.nseg += 1;
+            }
+        }
+        if (dd.maxw_w > O.maxw_wide) O.maxw_wide = dd.maxw_w;
+    }
+    P.otrees[ot] = O;
+}
+
+// Orientation, level count and table offset of pair p.
+XT_HD inline void pair_setup(const DTree *trees, const DOTree *ot, const int32_t *pair_trees, int orientation,
+                             int p, DPair *pairs) {
+    DPair q;
+    q.ta = pair_trees[2 * p];
+    q.tb = pair_trees[2 * p + 1];
+    const DTree &A = trees[q.ta], &B = trees[q.tb];
+    q.trivial = -1;
+    q.o = 0;
+    q.L = 0;
+    q.cells = 0;
+    q.dt_off = 0;
+    q.lvl_base = 0;
+    if (A.n == 0 || B.n == 0) {  // X-TED_CPU/TED.cpp:181-186
+        q.trivial = A.n == 0 ? B.n : A.n;
+    } else {
+        const int64_t cr = A.S[0] * B.S[0], cl = A.S[1] * B.S[1];
+        q.o = orientation == XTED_ORIENT_LEFT || (orientation == XTED_ORIENT_AUTO && cl < cr);
+        q.cells = q.o ? cl : cr;
+        q.L = ot[2 * q.ta + q.o].D + ot[2 * q.tb + q.o].D + 1;
+    }
+    pairs[p] = q;
+}
+
+struct LevelCtx {
+    const DOTree *ot;
+    const DDepth *depths;
+    const XRun *runs;
+    const XChunk *chunks;
+    const DPair *pairs;
+    int32_t narrow_width;
+};
+
+// Units and tasks of level entry e (pair, level) and its time estimate.
+XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
+    const DPair &q = C.pairs[E.pair];
+    const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
+    const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
+    const int d = E.level;
+    int64_t wide = 0, narrow = 0;
+    double est = 0.0;
+    const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
+    for (int al = lo; al <= hi; al++) {
+        const DDepth &ra = da[al], &cb = db[d - al];
+        const int64_t nr = ra.run_hi - ra.run_lo;
+        wide += nr * cb.nwide;
+        narrow += nr * cb.nnarrow;
+        double c = row_cost_est(false, cb.maxw_n);
+        const double cw = row_cost_est(true, cb.maxw_w);
+        if (cw > c) c = cw;
+        const double e = ra.maxrows * c;
+        if (e > est) est = e;
+    }
+    E.nwide = (int32_t)wide;
+    E.nnarrow = (int32_t)narrow;
+    E.ntasks = (int32_t)(wide + (narrow + XTED_TASK_UNITS - 1) / XTED_TASK_UNITS);
+    *est_out = est;
+}
+
+// Writes the units and tasks of level entry E (offsets already assigned).
+XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, XTask *tasks) {
+    const DPair &q = C.pairs[E.pair];
+    const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
+    const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
+    const int d = E.level;
+    int32_t u = E.unit_off, t = E.task_off;
+    int32_t bundle = 0, bundle_lo = u;
+    const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
+    for (int al = lo; al <= hi; al++) {
+        const DDepth &ra = da[al], &cb = db[d - al];
+        for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            for (int32_t c = cb.chunk_lo; c < cb.chunk_lo + cb.nnarrow; c++) {
+                if (bundle == 0) bundle_lo = u;
+                units[u++] = XUnit{r, c};
+                if (++bundle == XTED_TASK_UNITS) {
+                    tasks[t++] = XTask{E.pair, E.need, (uint32_t)bundle, bundle_lo};
+                    bundle = 0;
+                }
+            }
+        }
+    }
+    if (bundle > 0) tasks[t++] = XTask{E.pair, E.need, (uint32_t)bundle, bundle_lo};
+    for (int al = lo; al <= hi; al++) {
+        const DDepth &ra = da[al], &cb = db[d - al];
+        for (int32_t r = ra.run_lo; r < ra.run_hi; r++)
+            for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nwide; c++) {
+                units[u] = XUnit{r, c};
+                tasks[t++] = XTask{E.pair, E.need, XTED_TASK_WIDE | 1u, u};
+                u++;
+            }
+    }
+}
+
+}  // namespace xted

@@ -1,0 +1,421 @@
+// prep.cu -- device-side preprocessing and work decomposition of a batch.
+//
+// The reference computes orl, keyroots and keyroot depths on the host, then
+// for every depth level fetches, sizes, sorts and bins tables with host
+// round trips (X-TED_CPU/TED.cpp:163-166, X-TED_GPU/parallel_X_TED.cu:184-224,
+// 304-387). Here the raw trees go up once and everything else is built on the
+// device, one thread per tree / oriented tree / pair / (pair, level):
+//
+//   k_tree_basic   sizes, depths, parents, keyroot-size sums (both decompositions)
+//   k_orient       per orientation: node records, kdepth, keyroots by depth,
+//                  column-list positions, row runs, column chunks
+//   k_pair_setup   decomposition choice, level count
+//   k_level_*      unit/task counts and estimates per (pair, level), critical-
+//                  path priority, then the units and tasks themselves
+//
+// Level entries are ordered by a key (earliest start plus a quarter of the
+// pair's slack, see k_pair_rank) with a radix sort; every entry's
+// dependencies (lower levels of its pair) have strictly smaller keys, so the
+// resulting queue order respects them.
+// Two small device-to-host reads size the buffers (entries; tasks and units).
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "ctx.h"
+#include "plan_core.h"
+
+namespace xted {
+
+namespace {
+
+__global__ void k_tree_basic(PlanPools P, DTree *trees) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < P.ntrees) tree_basic(P, t, trees);
+}
+
+__global__ void k_orient(PlanPools P) {
+    const int ot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ot < 2 * P.ntrees) orient_tree(P, ot);
+}
+
+__global__ void k_pair_setup(const DTree *trees, const DOTree *ot, const int32_t *pair_trees, int orientation,
+                             int npairs, DPair *pairs, int64_t *L, int64_t *cells) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    pair_setup(trees, ot, pair_trees, orientation, p, pairs);
+    L[p] = pairs[p].L;
+    cells[p] = pairs[p].trivial >= 0 ? 0 : (int64_t)trees[pairs[p].ta].n * trees[pairs[p].tb].n;
+}
+
+// Exclusive scan of n int64 values in one block; out[n] = total. Optional
+// permutation: scans v[perm[i]] in the order i and writes out[i].
+__global__ void k_scan64(const int64_t *v, const int32_t *perm, int n, int64_t *out) {
+    __shared__ int64_t part[1024];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int per = (n + nt - 1) / nt;
+    const int lo = tid * per, hi = min(lo + per, n);
+    int64_t s = 0;
+    for (int i = lo; i < hi; i++) s += v[perm ? perm[i] : i];
+    part[tid] = s;
+    __syncthreads();
+    for (int d = 1; d < nt; d <<= 1) {
+        int64_t x = tid >= d ? part[tid - d] : 0;
+        __syncthreads();
+        part[tid] += x;
+        __syncthreads();
+    }
+    int64_t run = part[tid] - s;
+    for (int i = lo; i < hi; i++) {
+        out[i] = run;
+        run += v[perm ? perm[i] : i];
+    }
+    if (tid == nt - 1) out[n] = part[nt - 1];
+}
+
+struct Summary {
+    int64_t entries, dt_elems;
+    int64_t tasks, units;
+    int32_t stack_rows, max_wide;
+    int64_t cells, cells_right;
+    int32_t levels_max, pad;
+    int64_t chain_max;
+};
+
+__global__ void k_pair_offsets(DPair *pairs, const DTree *trees, const DOTree *ot, int npairs, const int64_t *Lscan,
+                               const int64_t *dtscan, Summary *sum) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) {
+        sum->entries = Lscan[npairs];
+        sum->dt_elems = dtscan[npairs];
+    }
+    if (p >= npairs) return;
+    DPair &q = pairs[p];
+    q.lvl_base = (int32_t)Lscan[p];
+    q.dt_off = dtscan[p];
+    if (q.trivial < 0) {
+        const DOTree &A = ot[2 * q.ta + q.o], &B = ot[2 * q.tb + q.o];
+        atomicMax(&sum->stack_rows, A.maxka + 1);
+        atomicMax(&sum->max_wide, B.maxw_wide);
+        atomicMax(&sum->levels_max, q.L);
+        atomicAdd((unsigned long long *)&sum->cells, (unsigned long long)q.cells);
+        atomicAdd((unsigned long long *)&sum->cells_right,
+                  (unsigned long long)(trees[q.ta].S[0] * trees[q.tb].S[0]));
+    }
+}
+
+__global__ void k_level_expand(const DPair *pairs, int npairs, DLevel *lv) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const DPair q = pairs[p];
+    for (int d = 0; d < q.L; d++) {
+        DLevel &E = lv[q.lvl_base + d];
+        E.pair = p;
+        E.level = d;
+    }
+}
+
+__global__ void k_level_count(LevelCtx C, DLevel *lv, int64_t nent, int64_t *units, int64_t *tasks) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    DLevel E = lv[e];
+    double est;
+    level_count(C, E, &est);
+    E.key = (int64_t)(est / 64.0) + 1;  // >= 1: strictly decreasing ranks below
+    lv[e] = E;
+    units[e] = (int64_t)E.nwide + E.nnarrow;
+    tasks[e] = E.ntasks;
+}
+
+// Per pair: est(d) is the estimated time of level d's slowest task. With
+// EST(d) = sum of est over lower levels (earliest start of level d) and
+// C = sum of all est (the pair's chain), a level's queue key is
+//   EST(d) + (Tmax - C) / 4,
+// Tmax the longest chain of the batch: levels are queued about when they can
+// start, and pairs with long chains (little slack) ahead of the others. Keys
+// strictly increase with the level inside a pair, so every task's
+// dependencies are queued before it. need = tasks of the pair at lower levels.
+__global__ void k_pair_rank(const DPair *pairs, int npairs, DLevel *lv, int64_t *chain, Summary *sum) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const DPair q = pairs[p];
+    int64_t acc = 0;
+    int32_t need = 0;
+    for (int d = 0; d < q.L; d++) {
+        DLevel &E = lv[q.lvl_base + d];
+        const int64_t est = E.key;
+        E.key = acc;
+        E.need = need;
+        acc += est;
+        need += E.ntasks;
+    }
+    chain[p] = acc;
+    atomicMax((unsigned long long *)&sum->chain_max, (unsigned long long)acc);
+}
+
+__global__ void k_level_keys(const DLevel *lv, int64_t nent, const int64_t *chain, const Summary *sum,
+                             int64_t *keys, int32_t *ids) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    const DLevel E = lv[e];
+    keys[e] = E.key + (sum->chain_max - chain[E.pair]) / 4;
+    ids[e] = (int32_t)e;
+}
+
+__global__ void k_level_offsets(DLevel *lv, int64_t nent, const int32_t *sorted_ids, const int64_t *task_scan,
+                                const int64_t *unit_scan, Summary *sum) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        sum->tasks = task_scan[nent];
+        sum->units = unit_scan[nent];
+    }
+    if (i >= nent) return;
+    DLevel &E = lv[sorted_ids[i]];
+    E.task_off = (int32_t)task_scan[i];
+    lv[i].unit_off = (int32_t)unit_scan[i];
+}
+
+__global__ void k_level_fill(LevelCtx C, const DLevel *lv, int64_t nent, XUnit *units, XTask *tasks) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nent) level_fill(C, lv[e], units, tasks);
+}
+
+__global__ void k_pair_finalize(const DPair *pairs, const DTree *trees, const DOTree *ot, int npairs, XPair *xp,
+                                int32_t *trivial) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const DPair q = pairs[p];
+    XPair x;
+    x.dt_off = q.dt_off;
+    x.m = trees[q.ta].n;
+    x.n = trees[q.tb].n;
+    x.row_base = ot[2 * q.ta + q.o].node_base;
+    x.col_base = ot[2 * q.tb + q.o].node_base;
+    xp[p] = x;
+    trivial[p] = q.trivial;
+}
+
+inline unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+// Carves a device buffer into aligned sections.
+struct Carver {
+    char *base;
+    size_t off = 0;
+    template <class T>
+    T *take(size_t count) {
+        off = (off + 255) & ~(size_t)255;
+        T *p = (T *)(base + off);
+        off += sizeof(T) * (count > 0 ? count : 1);
+        return p;
+    }
+};
+
+int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs, XKernelParams &K) {
+    cudaStream_t s = c->stream;
+    // ---- host: unique trees, flat raw input, pair list ----
+    c->tree_ids.clear();
+    c->uniq.clear();
+    std::vector<int32_t> &pt = c->pair_trees;
+    pt.resize(2 * (size_t)npairs);
+    int64_t N = 0, R = 0;
+    for (int p = 0; p < npairs; p++) {
+        for (int side = 0; side < 2; side++) {
+            const xted_tree &t = side ? b[p] : a[p];
+            TreeKey key{t.labels, t.child_off, t.child_idx, t.n};
+            auto it = c->tree_ids.find(key);
+            int id;
+            if (it == c->tree_ids.end()) {
+                id = (int)c->uniq.size();
+                c->tree_ids.emplace(key, id);
+                TreeView tv{t.n, t.labels, t.child_off, t.child_idx};
+                int rc = validate_tree(tv);
+                if (rc) return rc;
+                c->uniq.push_back(tv);
+                N += t.n;
+                R += 3 * (int64_t)t.n + 1;
+            } else {
+                id = it->second;
+            }
+            pt[2 * (size_t)p + side] = id;
+        }
+    }
+    const int T = (int)c->uniq.size();
+    if (N > (int64_t)1 << 30) return XTED_ENOMEM;
+    std::vector<DTree> &ht = c->htrees;
+    ht.resize((size_t)T);
+    // staging: raw trees | DTree[T] | pair_trees
+    const size_t raw_bytes = (size_t)R * 4, tr_bytes = sizeof(DTree) * (size_t)T,
+                 pt_bytes = 8 * (size_t)npairs;
+    const size_t stage_bytes = raw_bytes + tr_bytes + pt_bytes + 1024;
+    int rc = ctx_host_reserve(c->stage, stage_bytes);
+    if (rc) return rc;
+    char *h = (char *)c->stage.p;
+    int32_t *hraw = (int32_t *)h;
+    {
+        int64_t rpos = 0, nb = 0;
+        for (int t = 0; t < T; t++) {
+            const TreeView &tv = c->uniq[(size_t)t];
+            DTree &d = ht[(size_t)t];
+            d.n = tv.n;
+            d.raw = (int32_t)rpos;
+            d.nbase = (int32_t)nb;
+            d.t = t;
+            d.S[0] = d.S[1] = 0;
+            const int n = tv.n;
+            if (n > 0) {
+                std::memcpy(hraw + rpos, tv.labels, 4 * (size_t)n);
+                std::memcpy(hraw + rpos + n, tv.off, 4 * ((size_t)n + 1));
+                if (n > 1) std::memcpy(hraw + rpos + 2 * n + 1, tv.idx, 4 * ((size_t)n - 1));
+            } else {
+                hraw[rpos] = 0;  // child_off[0]
+            }
+            rpos += 3 * (int64_t)n + 1;
+            nb += n;
+        }
+    }
+    size_t hoff = (raw_bytes + 255) & ~(size_t)255;
+    std::memcpy(h + hoff, ht.data(), tr_bytes);
+    const size_t hoff_pt = (hoff + tr_bytes + 255) & ~(size_t)255;
+    std::memcpy(h + hoff_pt, pt.data(), pt_bytes);
+    const size_t upload = hoff_pt + pt_bytes;
+
+    // ---- device buffer A: input + per-tree pools (sizes known from N, T, npairs) ----
+    const size_t N2 = 2 * (size_t)std::max<int64_t>(N, 1);
+    size_t need = upload + 4096;
+    need += 3 * sizeof(int32_t) * (size_t)std::max<int64_t>(N, 1);  // size, depth, parent
+    need += N2 * (sizeof(int2) + 2 * sizeof(int32_t) + sizeof(XRun) + sizeof(XChunk) + 3 * sizeof(int32_t));
+    need += sizeof(DDepth) * (N2 + 2 * (size_t)T) + sizeof(DOTree) * 2 * (size_t)T + sizeof(DTree) * (size_t)T;
+    need += (size_t)npairs * (sizeof(DPair) + sizeof(XPair) + 4 + 5 * 8) + 20 * 256 + sizeof(Summary);
+    rc = ctx_dev_reserve(c, c->meta, need);
+    if (rc) return rc;
+    Carver cv{(char *)c->meta.p};
+    char *d_in = cv.take<char>(upload);
+    if (cudaMemcpyAsync(d_in, h, upload, cudaMemcpyHostToDevice, s) != cudaSuccess) return XTED_ECUDA;
+    c->h2d_bytes = (int64_t)upload;
+    PlanPools P;
+    P.raw = (const int32_t *)d_in;
+    DTree *d_trees = (DTree *)(d_in + hoff);
+    P.trees = d_trees;
+    const int32_t *d_pt = (const int32_t *)(d_in + hoff_pt);
+    P.ntrees = T;
+    P.size = cv.take<int32_t>((size_t)N);
+    P.depth = cv.take<int32_t>((size_t)N);
+    P.parent = cv.take<int32_t>((size_t)N);
+    P.node = cv.take<int2>(N2);
+    P.krd = cv.take<int32_t>(N2);
+    P.cumw = cv.take<int32_t>(N2);
+    P.runs = cv.take<XRun>(N2);
+    P.chunks = cv.take<XChunk>(N2);
+    P.opar = cv.take<int32_t>(N2);
+    P.okd = cv.take<int32_t>(N2);
+    P.oka = cv.take<int32_t>(N2);
+    P.depths = cv.take<DDepth>(N2 + 2 * (size_t)T);
+    P.otrees = cv.take<DOTree>(2 * (size_t)T);
+    P.run_rows = c->opts.run_rows;
+    P.narrow_width = c->opts.narrow_width;
+    DPair *d_pairs = cv.take<DPair>((size_t)npairs);
+    XPair *d_xpairs = cv.take<XPair>((size_t)npairs);
+    int32_t *d_trivial = cv.take<int32_t>((size_t)npairs);
+    int64_t *d_L = cv.take<int64_t>((size_t)npairs + 1);
+    int64_t *d_chain = cv.take<int64_t>((size_t)npairs + 1);
+    int64_t *d_cells = cv.take<int64_t>((size_t)npairs + 1);
+    int64_t *d_Ls = cv.take<int64_t>((size_t)npairs + 1);
+    int64_t *d_dts = cv.take<int64_t>((size_t)npairs + 1);
+    Summary *d_sum = cv.take<Summary>(1);
+    if (cv.off > c->meta.cap) return XTED_ENOMEM;
+
+    const int BS = 128;
+    cudaMemsetAsync(d_sum, 0, sizeof(Summary), s);
+    k_tree_basic<<<blocks_for(T, BS), BS, 0, s>>>(P, d_trees);
+    k_orient<<<blocks_for(2 * (int64_t)T, BS), BS, 0, s>>>(P);
+    k_pair_setup<<<blocks_for(npairs, BS), BS, 0, s>>>(d_trees, P.otrees, d_pt, c->opts.orientation, npairs,
+                                                       d_pairs, d_L, d_cells);
+    k_scan64<<<1, 1024, 0, s>>>(d_L, nullptr, npairs, d_Ls);
+    k_scan64<<<1, 1024, 0, s>>>(d_cells, nullptr, npairs, d_dts);
+    k_pair_offsets<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_Ls,
+                                                                      d_dts, d_sum);
+    Summary *hs = (Summary *)c->summary.p;
+    cudaMemcpyAsync(hs, d_sum, sizeof(Summary), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return XTED_ECUDA;
+    }
+    const int64_t nent = hs->entries;
+    // ---- buffer B: level entries, sort keys, scans ----
+    size_t cub_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (const int64_t *)nullptr, (int64_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)nent, 0, 64, s);
+    const size_t E1 = (size_t)nent + 1;
+    size_t needB = sizeof(DLevel) * E1 + (2 * 8 + 2 * 4 + 4 * 8) * E1 + cub_bytes + 16 * 256;
+    rc = ctx_dev_reserve(c, c->levels, needB);
+    if (rc) return rc;
+    Carver cb{(char *)c->levels.p};
+    DLevel *d_lv = cb.take<DLevel>(E1);
+    int64_t *d_keys = cb.take<int64_t>(E1), *d_keys2 = cb.take<int64_t>(E1);
+    int32_t *d_ids = cb.take<int32_t>(E1), *d_ids2 = cb.take<int32_t>(E1);
+    int64_t *d_units = cb.take<int64_t>(E1), *d_tasks = cb.take<int64_t>(E1);
+    int64_t *d_uscan = cb.take<int64_t>(E1), *d_tscan = cb.take<int64_t>(E1);
+    void *d_cub = cb.take<char>(cub_bytes);
+    LevelCtx C;
+    C.ot = P.otrees;
+    C.depths = P.depths;
+    C.runs = P.runs;
+    C.chunks = P.chunks;
+    C.pairs = d_pairs;
+    C.narrow_width = c->opts.narrow_width;
+    if (nent > 0) {
+        k_level_expand<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv);
+        k_level_count<<<blocks_for(nent, BS), BS, 0, s>>>(C, d_lv, nent, d_units, d_tasks);
+        k_pair_rank<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv, d_chain, d_sum);
+        k_level_keys<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_chain, d_sum, d_keys, d_ids);
+        if (cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_keys, d_keys2, d_ids, d_ids2, (int)nent, 0, 64, s) !=
+            cudaSuccess)
+            return XTED_ECUDA;
+        // the sorted ids give each entry's place in the queue
+        k_scan64<<<1, 1024, 0, s>>>(d_tasks, d_ids2, (int)nent, d_tscan);
+        k_scan64<<<1, 1024, 0, s>>>(d_units, nullptr, (int)nent, d_uscan);
+        k_level_offsets<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_ids2, d_tscan, d_uscan, d_sum);
+    }
+    cudaMemcpyAsync(hs, d_sum, sizeof(Summary), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return XTED_ECUDA;
+    }
+    const int64_t ntasks = nent > 0 ? hs->tasks : 0, nunits = nent > 0 ? hs->units : 0;
+    if (ntasks > INT32_MAX / 2 || nunits > INT32_MAX / 2) return XTED_ENOMEM;
+    // ---- buffer C: units and tasks ----
+    rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
+                                         512);
+    if (rc) return rc;
+    Carver cw{(char *)c->work.p};
+    XUnit *d_units_out = cw.take<XUnit>((size_t)nunits);
+    XTask *d_tasks_out = cw.take<XTask>((size_t)ntasks);
+    if (nent > 0) k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out);
+    k_pair_finalize<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_xpairs,
+                                                                       d_trivial);
+    if (cudaGetLastError() != cudaSuccess) return XTED_ECUDA;
+
+    std::memset(&K, 0, sizeof(K));
+    K.rowinfo = P.node;
+    K.krd = P.krd;
+    K.cumw = P.cumw;
+    K.runs = P.runs;
+    K.chunks = P.chunks;
+    K.pairs = d_xpairs;
+    K.units = d_units_out;
+    K.tasks = d_tasks_out;
+    K.ntasks = (int32_t)ntasks;
+    c->d_trivial = d_trivial;
+    c->plan_dt_elems = hs->dt_elems;
+    c->plan_stack_rows = std::max(hs->stack_rows, 1);
+    c->plan_max_wide = hs->max_wide;
+    c->plan_cells = hs->cells;
+    c->plan_cells_right = hs->cells_right;
+    c->plan_levels_max = hs->levels_max;
+    c->plan_units = nunits;
+    return XTED_OK;
+}
+
+}  // namespace xted

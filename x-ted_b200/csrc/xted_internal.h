@@ -18,8 +18,9 @@
 // every table (i0, j0) with i0 in the run and j0 in the chunk, computed row by
 // row (rows descending, a min-plus suffix scan across the chunk's columns).
 // A *task* is what one thread block claims from the device queue: one wide
-// unit (chunk wider than a warp can hold) or up to 8 narrow units (one per
-// warp), all of one pair and one level.
+// unit (chunk wider than a warp can hold) or up to XTED_TASK_UNITS narrow
+// units that the block's warps claim one at a time, all of one pair and one
+// level.
 #pragma once
 
 #include <stdint.h>
@@ -37,13 +38,14 @@
 #define XTED_ROW_ISKR (1u << 29)     // node is a keyroot
 #define XTED_ROW_PREVLEAF (1u << 30) // node i-1 is a leaf
 
-// colinfo.z bit layout: foff = orl(j) + 1 - j in the low 20 bits.
+// Per-column state derived in the kernels (the wide generic path keeps it in
+// scratch as int4: x = node j, y = label(j), z = foff | flags, w = dend):
+// foff = orl(j) + 1 - j (low 20 bits), dend = je - j with je = orl(j0) + 1 for
+// the segment's keyroot j0.
 #define XTED_COL_FOFF_MASK 0x000fffff
 #define XTED_COL_FARCOL (1u << 30)   // column j-1 is a leaf inside the segment: a far column
 
-// colinfo: x = node j (index in B), y = label(j), z = foff | flags, w = dend = je - j
-// (je = orl(j0) + 1 for the segment's keyroot j0).
-// rowinfo: x = label(i), y = orl(i) | flags.
+// Node record (both trees use the same pool): x = label, y = orl | flags.
 
 struct XRun {      // a run of keyroots of one depth of a row tree
     int32_t kr_lo; // index into the keyroot pool (global)
@@ -53,7 +55,7 @@ struct XRun {      // a run of keyroots of one depth of a row tree
 };
 
 struct XChunk {     // a run of whole segments of one depth of a column tree
-    int32_t col_lo; // index into the column pool (global)
+    int32_t k_lo;   // keyroot-pool index of its first segment
     int32_t width;
     int32_t depth;
     int32_t nseg;
@@ -62,8 +64,8 @@ struct XChunk {     // a run of whole segments of one depth of a column tree
 struct XPair {
     int64_t dt_off;   // element offset of this pair's m x n distance table
     int32_t m, n;     // rows (A) and columns (B)
-    int32_t row_base; // index of A's node 0 in the rowinfo pool
-    int32_t pad;
+    int32_t row_base; // index of A's node 0 in the node-record pool
+    int32_t col_base; // index of B's node 0 in the node-record pool
 };
 
 struct XUnit {
@@ -72,6 +74,8 @@ struct XUnit {
 };
 
 #define XTED_TASK_WIDE 0x80000000u
+#define XTED_TASK_UNITS 32   // narrow units per task (claimed by the block's warps dynamically)
+#define XTED_PREFETCH 4      // rows of tree distances in flight per unit (cp.async ring depth)
 
 struct XTask {
     int32_t pair;
@@ -81,9 +85,9 @@ struct XTask {
 };
 
 struct XKernelParams {
-    const int2 *rowinfo;  // per node of every row tree
-    const int4 *colinfo;  // per column position of every column tree
+    const int2 *rowinfo;  // node records of every oriented tree
     const int32_t *krd;   // keyroots grouped by depth (node ids within their tree)
+    const int32_t *cumw;  // position of each keyroot's segment in its depth's column list
     const XRun *runs;
     const XChunk *chunks;
     const XPair *pairs;
