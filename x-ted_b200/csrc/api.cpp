@@ -270,9 +270,9 @@ int xted_destroy(xted_ctx *c) {
     cudaSetDevice(c->opts.device);
     xted::serve_shutdown(c);
     cudaStreamSynchronize(c->stream);
-    for (DevBuf *b : {&c->meta, &c->dt, &c->scratch, &c->counters, &c->trace})
+    for (DevBuf *b : {&c->meta, &c->levels, &c->work, &c->dt, &c->scratch, &c->counters, &c->trace})
         if (b->p) cudaFree(b->p);
-    for (HostBuf *b : {&c->stage, &c->result})
+    for (HostBuf *b : {&c->stage, &c->result, &c->summary})
         if (b->p) cudaFreeHost(b->p);
     for (cudaEvent_t e : {c->ev0, c->ev1, c->evk0, c->evk1})
         if (e) cudaEventDestroy(e);

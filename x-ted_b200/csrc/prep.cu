@@ -336,6 +336,8 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     k_scan64<<<1, 1024, 0, s>>>(d_cells, nullptr, npairs, d_dts);
     k_pair_offsets<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_Ls,
                                                                       d_dts, d_sum);
+    rc = ctx_host_reserve(c->summary, sizeof(Summary));
+    if (rc) return rc;
     Summary *hs = (Summary *)c->summary.p;
     cudaMemcpyAsync(hs, d_sum, sizeof(Summary), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) {
