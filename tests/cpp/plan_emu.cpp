@@ -8,7 +8,7 @@
 // plan's invariants (dependency order, single write of every tree cell, every
 // read cell already written, stack discipline, unit coverage) and the distances
 // against the oracle's restatement of X-TED_CPU.
-//   usage: plan_emu <iterations> <max_nodes> <seed>
+//   usage: plan_emu <iterations> <max_nodes> <seed> [stack window rows, default 8]
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -41,6 +41,7 @@ struct HostPlan {
     std::vector<DOTree> ot;
     std::vector<DPair> pairs;
     std::vector<DLevel> lv;
+    std::vector<XEntry> entries;
     std::vector<XUnit> units;
     std::vector<XTask> tasks;
     int stack_rows = 1;
@@ -122,7 +123,6 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     for (int p = 0; p < np; p++) {
         const DPair &q = H.pairs[(size_t)p];
         int64_t acc = 0;
-        int32_t need = 0;
         for (int d = 0; d < q.L; d++) {
             DLevel &E = H.lv[(size_t)(q.lvl_base + d)];
             E.pair = p;
@@ -131,26 +131,25 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
             level_count(C, E, &est);
             const int64_t e = (int64_t)(est / 64.0) + 1;
             E.key = acc;
-            E.need = need;
             acc += e;
-            need += E.ntasks;
         }
         chain[(size_t)p] = acc;
         chain_max = std::max(chain_max, acc);
     }
-    std::vector<int32_t> order((size_t)ent);
-    std::iota(order.begin(), order.end(), 0);
-    std::vector<int64_t> key((size_t)ent);
-    for (size_t e = 0; e < (size_t)ent; e++) key[e] = H.lv[e].key + (chain_max - chain[(size_t)H.lv[e].pair]) / 4;
-    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return key[(size_t)x] < key[(size_t)y]; });
     int64_t toff = 0, uoff = 0;
-    for (int32_t e : order) {
-        H.lv[(size_t)e].task_off = (int32_t)toff;
-        toff += H.lv[(size_t)e].ntasks;
-    }
-    for (auto &E : H.lv) {
+    H.entries.resize(H.lv.size());
+    for (size_t e = 0; e < H.lv.size(); e++) {
+        DLevel &E = H.lv[e];
+        E.task_off = (int32_t)toff;
         E.unit_off = (int32_t)uoff;
+        E.entry = (int32_t)e;
+        toff += E.ntasks;
         uoff += (int64_t)E.nwide + E.nnarrow;
+        XEntry &X = H.entries[e];
+        X.task_off = E.task_off;
+        X.ntasks = E.ntasks;
+        X.bucket = level_bucket(chain[(size_t)E.pair] - E.key, chain_max);
+        X.next = E.level + 1 < H.pairs[(size_t)E.pair].L ? (int32_t)e + 1 : -1;
     }
     H.units.assign((size_t)uoff, XUnit{-1, -1});
     H.tasks.assign((size_t)toff, XTask{-1, -1, 0, -1});
@@ -158,6 +157,8 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
 }
 
 // One unit, exactly as the kernels compute it (columns derived like load_cols).
+static int g_cache = 8;  // shared-memory window of the far-row stack (the kernels use 8)
+
 static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vector<int32_t> &dtv,
                      int narrow_width, bool wide_task) {
     const DOTree &A = H.ot[2 * (size_t)q.ta + q.o], &B = H.ot[2 * (size_t)q.tb + q.o];
@@ -194,13 +195,18 @@ static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vec
         j++;
     }
     if (seg != ch.nseg || s != ch.k_lo + ch.nseg - 1) FAIL("chunk segment count mismatch");
+    // global stack (written only when units can nest deeper than the window) and the window
+    const bool deep = H.stack_rows > g_cache;
     std::vector<std::vector<int>> stk((size_t)H.stack_rows, std::vector<int>((size_t)W, -777));
+    std::vector<std::vector<int>> cache((size_t)g_cache, std::vector<int>((size_t)W, -777));
     std::vector<int> prev(W), cur(W), loc(W);
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = H.krd[(size_t)kr];
         const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
         for (int c = 0; c < W; c++) prev[c] = dend[c];
-        int sp = 0;
+        int sp = 0, lo = 0;
+        for (auto &row : cache) std::fill(row.begin(), row.end(), -777);
+        for (auto &row : stk) std::fill(row.begin(), row.end(), -777);
         for (int i = imax - 1; i >= i0; i--) {
             const int2 ri = rn[i];
             const int ro = ri.y & XTED_ROW_ORL_MASK;
@@ -220,7 +226,8 @@ static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vec
                     else if (tcol) fv = rowfar;
                     else {
                         if (sp < 1) FAIL("far-row stack underflow");
-                        fv = stk[(size_t)sp - 1][(size_t)(c + foff[c])];
+                        if (sp - 1 < lo) FAIL("stack top outside the shared window");
+                        fv = cache[(size_t)((sp - 1) % g_cache)][(size_t)(c + foff[c])];
                         if (fv == -777) FAIL("far value never pushed");
                     }
                     const int dv = dt[(size_t)i * n + node[c]];
@@ -241,11 +248,24 @@ static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vec
                 }
                 prev[c] = cur[c];
             }
-            if (i != i0 && (ri.y & XTED_ROW_ISKR)) sp--;
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
+                sp--;
+                if (sp > 0 && sp - 1 < lo) {
+                    if (!deep) FAIL("window reload in a shallow unit");
+                    for (int c = 0; c < W; c++)
+                        if (far[c]) cache[(size_t)((sp - 1) % g_cache)][(size_t)c] = stk[(size_t)sp - 1][(size_t)c];
+                    lo = sp - 1;
+                }
+            }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp >= H.stack_rows) FAIL("far-row stack overflow (%d rows)", H.stack_rows);
-                for (int c = 0; c < W; c++) stk[(size_t)sp][(size_t)c] = far[c] ? prev[c] : -777;
+                for (int c = 0; c < W; c++)
+                    if (far[c]) {
+                        cache[(size_t)(sp % g_cache)][(size_t)c] = prev[c];
+                        if (deep) stk[(size_t)sp][(size_t)c] = prev[c];
+                    }
                 sp++;
+                if (sp - lo > g_cache) lo = sp - g_cache;
             }
         }
         if (sp != 0) FAIL("far-row stack not empty at table end (%d)", sp);
@@ -288,6 +308,7 @@ static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int
 
 int main(int argc, char **argv) {
     const int iters = argc > 1 ? std::atoi(argv[1]) : 200;
+    if (argc > 4) g_cache = std::atoi(argv[4]);
     const int maxn = argc > 2 ? std::atoi(argv[2]) : 300;
     std::mt19937_64 g(argc > 3 ? (uint64_t)std::atoll(argv[3]) : 12345);
     int64_t pairs_checked = 0;
@@ -310,20 +331,41 @@ int main(int argc, char **argv) {
         for (auto &q : H.pairs)
             if (q.trivial < 0) dts += (int64_t)H.trees[(size_t)q.ta].n * H.trees[(size_t)q.tb].n;
         std::vector<int32_t> dt((size_t)std::max<int64_t>(dts, 1), -1);
-        std::vector<int> fin((size_t)npairs, 0);
+        // ready queue: level 0 of every pair, then each level once its predecessor is done;
+        // highest bucket first, tasks of an entry in a shuffled order
+        std::vector<std::vector<int32_t>> bucket(XTED_BUCKETS);
+        for (auto &q : H.pairs)
+            if (q.L > 0) bucket[(size_t)H.entries[(size_t)q.lvl_base].bucket].push_back(q.lvl_base);
+        std::vector<size_t> head(XTED_BUCKETS, 0);
+        std::vector<int> level_done((size_t)npairs, -1);
         std::vector<int> unit_seen(H.units.size(), 0);
-        for (const XTask &t : H.tasks) {
-            if (t.pair < 0) FAIL("task slot never filled");
-            if (fin[(size_t)t.pair] < t.need) FAIL("task queued before its dependencies");
-            const int nu = (int)(t.kind_n & 0xffff);
-            const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
-            if (nu < 1 || nu > XTED_TASK_UNITS || (wide && nu != 1)) FAIL("bad unit count %d", nu);
-            for (int k = 0; k < nu; k++) {
-                unit_seen[(size_t)(t.unit_lo + k)]++;
-                run_unit(H, H.pairs[(size_t)t.pair], H.units[(size_t)(t.unit_lo + k)], dt, nw, wide);
+        for (;;) {
+            int e = -1;
+            for (int b = XTED_BUCKETS - 1; b >= 0 && e < 0; b--)
+                if (head[(size_t)b] < bucket[(size_t)b].size()) e = bucket[(size_t)b][head[(size_t)b]++];
+            if (e < 0) break;
+            const XEntry &X = H.entries[(size_t)e];
+            const DLevel &E = H.lv[(size_t)e];
+            if (level_done[(size_t)E.pair] != E.level - 1) FAIL("level published before its predecessor finished");
+            std::vector<int> order((size_t)X.ntasks);
+            std::iota(order.begin(), order.end(), 0);
+            std::shuffle(order.begin(), order.end(), g);
+            for (int k : order) {
+                const XTask &t = H.tasks[(size_t)(X.task_off + k)];
+                if (t.pair != E.pair || t.entry != e) FAIL("task of another entry in the range");
+                const int nu = (int)(t.kind_n & 0xffff);
+                const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
+                if (nu < 1 || nu > XTED_TASK_UNITS || (wide && nu != 1)) FAIL("bad unit count %d", nu);
+                for (int u = 0; u < nu; u++) {
+                    unit_seen[(size_t)(t.unit_lo + u)]++;
+                    run_unit(H, H.pairs[(size_t)t.pair], H.units[(size_t)(t.unit_lo + u)], dt, nw, wide);
+                }
             }
-            fin[(size_t)t.pair]++;
+            level_done[(size_t)E.pair] = E.level;
+            if (X.next >= 0) bucket[(size_t)H.entries[(size_t)X.next].bucket].push_back(X.next);
         }
+        for (int p = 0; p < npairs; p++)
+            if (level_done[(size_t)p] != H.pairs[(size_t)p].L - 1) FAIL("pair %d did not finish its levels", p);
         for (int v : unit_seen)
             if (v != 1) FAIL("unit covered %d times", v);
         for (int p = 0; p < npairs; p++) {

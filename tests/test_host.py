@@ -120,6 +120,7 @@ def test_planner_emulation_matches_oracle(tmp_path):
     subprocess.run(["g++", "-O2", "-std=c++17", "-I/usr/local/cuda/include",
                     os.path.join(REPO, "tests", "cpp", "plan_emu.cpp"), str(obj), "-o", str(exe), "-lpthread"],
                    check=True)
-    r = subprocess.run([str(exe), "150", "250", "99"], capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.startswith("ok")
+    for window in ("8", "2"):  # the kernels' shared stack window, and a tiny one that forces reloads
+        r = subprocess.run([str(exe), "100", "250", "99", window], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert r.stdout.startswith("ok")

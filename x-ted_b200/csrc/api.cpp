@@ -25,6 +25,7 @@
 namespace xted {
 int dp_occupancy(int *blocks_per_sm);
 cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s);
+cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s);
 cudaError_t launch_gather(const XPair *pairs, const int32_t *trivial, const int32_t *dt, int npairs,
                           int32_t *out, cudaStream_t s);
 }  // namespace xted
@@ -103,7 +104,7 @@ int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npa
     per = (int64_t)align_up((size_t)per, 64);
     rc = ctx_dev_reserve(c, c->scratch, (size_t)per * (size_t)c->grid * sizeof(int32_t));
     if (rc) return rc;
-    // counters: [0] queue head, [1] error, [2..5] error info, then finished[npairs], out[npairs]
+    // counters: [1] error, [2..5] error info, then out[npairs]
     rc = ctx_dev_reserve(c, c->counters, (8 + 2 * (size_t)npairs) * sizeof(int32_t));
     if (rc) return rc;
     rc = ctx_host_reserve(c->result, ((size_t)npairs + 8) * sizeof(int32_t));
@@ -113,10 +114,8 @@ int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npa
     K.scratch = (int32_t *)c->scratch.p;
     K.scratch_per_cta = per;
     K.stack_rows = (int32_t)stack_rows;
-    K.task_next = cnt;
     K.error = cnt + 1;
     K.error_info = cnt + 2;
-    K.finished = cnt + 8;
     K.timeout_ns = (uint64_t)(c->opts.wait_timeout_s * 1e9);
     // Optional per-task trace (XTED_TRACE=<file>): timestamps of every task,
     // written as raw uint64 quadruples after each run.
@@ -143,7 +142,14 @@ int ctx_run(xted_ctx *c, int32_t *out) {
     int32_t *hres = (int32_t *)c->result.p;
     const size_t res_bytes = (size_t)npairs * sizeof(int32_t);
     cudaEventRecord(c->ev0, c->stream);
-    if (cudaMemsetAsync(cnt, 0, (8 + (size_t)npairs) * sizeof(int32_t), c->stream) != cudaSuccess)
+    // per-run reset of the error words and the ready queue, then level 0 of every pair
+    const size_t ne = (size_t)K.nentries;
+    if (cudaMemsetAsync(cnt, 0, 8 * sizeof(int32_t), c->stream) != cudaSuccess ||
+        (K.ntasks > 0 &&
+         (cudaMemsetAsync(K.entry_state, 0, 2 * ne * sizeof(int32_t), c->stream) != cudaSuccess ||
+          cudaMemsetAsync(K.rq, 0xff, (size_t)XTED_BUCKETS * ne * sizeof(int32_t), c->stream) != cudaSuccess ||
+          cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_BUCKETS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
+          launch_rq_init(K, c->stream) != cudaSuccess)))
         return XTED_ECUDA;
     cudaEventRecord(c->evk0, c->stream);
     if (K.ntasks > 0) {

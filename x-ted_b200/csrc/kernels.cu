@@ -1,6 +1,6 @@
 // kernels.cu -- the keyroot-table dynamic program on sm_100a.
 //
-// One persistent kernel drains a device queue of tasks (see xted_internal.h).
+// One persistent kernel drains a device ready queue of tasks (see xted_internal.h).
 // A task is one wide unit run by the whole 256-thread block, or up to eight
 // narrow units, one per warp. A unit computes the forest tables of a run of
 // A-keyroots against a chunk of B-segments, row by row from the bottom:
@@ -48,22 +48,6 @@ __device__ __forceinline__ void set_error(const XKernelParams &P, int code, int 
         P.error_info[1] = b;
         P.error_info[2] = c;
     }
-}
-
-// Waits until *p >= target. Bounded by time and by iterations; returns false
-// (and the caller gives up) on timeout or when another block reported an error.
-__device__ bool wait_ge(const XKernelParams &P, const int32_t *p, int target) {
-    if (ld_acquire(p) >= target) return true;
-    const uint64_t t0 = global_ns();
-    unsigned ns = 64;
-    for (long it = 0; it < (1L << 26); it++) {
-        __nanosleep(ns);
-        if (ns < 2048) ns <<= 1;
-        if (ld_acquire(p) >= target) return true;
-        if (*(volatile int32_t *)P.error != 0) return false;
-        if (global_ns() - t0 > P.timeout_ns) break;
-    }
-    return false;
 }
 
 __device__ __forceinline__ int warp_suffix_min(int v, int lane) {
@@ -214,11 +198,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// Far-row stack: the top XTED_STACK_CACHE rows of every unit's stack live in
+// shared memory (a ring indexed by stack position); rows are also written to
+// the global stack only when a unit can nest deeper than that, and a row that
+// falls out of the window is reloaded from there when the stack unwinds.
+#define XTED_STACK_CACHE 8
 #define NARROW_SLOT (XTED_NARROW_MAX + 8)  // ints per ring slot: columns, then the row record
 #define WIDE_SLOT (XTED_WIDE_REG_MAX + 8)
 #define RING_INTS ((XTED_WARPS * XTED_PREFETCH * NARROW_SLOT) > (XTED_PREFETCH * WIDE_SLOT) \
                        ? (XTED_WARPS * XTED_PREFETCH * NARROW_SLOT)                          \
                        : (XTED_PREFETCH * WIDE_SLOT))
+#define CACHE_INTS (XTED_STACK_CACHE * XTED_WIDE_REG_MAX)  // = warps x depth x narrow width
+static_assert(CACHE_INTS == XTED_WARPS * XTED_STACK_CACHE * XTED_NARROW_MAX, "stack cache split");
+#define DP_SMEM_BYTES ((RING_INTS + CACHE_INTS) * 4)
 
 // Issues the copies of row r (this thread's columns; one thread: the record).
 template <int W>
@@ -236,7 +228,7 @@ __device__ __forceinline__ void issue_row(const Cols<W> &C, const int32_t *dt, i
 // ---------------------------------------------------------------------------
 template <int W>
 __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
-                           int32_t *ring) {
+                           int32_t *ring, int32_t *cache) {
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = lane * W;
@@ -260,7 +252,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
         int prev[W];
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k];
-        int sp = 0;
+        int sp = 0, lo = 0;  // stack depth; lowest position held in the shared window
         __syncwarp();  // the ring's previous readers are done
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
@@ -286,7 +278,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = stk + (sp > 0 ? sp - 1 : 0) * stride;
+            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) % XTED_STACK_CACHE) * stride;
             const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             int loc[W];
             const int mine = row_cells<W>(C, prev, cur, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
@@ -301,17 +293,34 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
                 if (trow && C.foff[k] == C.dend[k] && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
             }
             __syncwarp();
-            if (i != i0 && (ri.y & XTED_ROW_ISKR)) sp--;
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
+                sp--;
+                if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
+                    const int32_t *src = stk + (sp - 1) * stride + c0;
+                    int32_t *dst = cache + ((sp - 1) % XTED_STACK_CACHE) * stride + c0;
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if ((C.far >> k) & 1u) dst[k] = src[k];
+                    lo = sp - 1;
+                }
+            }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = stk + sp * stride + c0;
+                    int32_t *dst = cache + (sp % XTED_STACK_CACHE) * stride + c0;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = prev[k];
+                    if (P.stack_rows > XTED_STACK_CACHE) {
+                        int32_t *g = stk + sp * stride + c0;
+#pragma unroll
+                        for (int k = 0; k < W; k++)
+                            if ((C.far >> k) & 1u) g[k] = prev[k];
+                    }
                 } else if (lane == 0) {
                     set_error(P, XTED_ENOMEM, 1, sp, P.stack_rows);
                 }
                 sp++;
+                if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
             }
             __syncwarp();
         }
@@ -330,7 +339,7 @@ struct WideShared {
 
 template <int W>
 __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
-                         int32_t *ring) {
+                         int32_t *ring, int32_t *cache) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
@@ -359,7 +368,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
         int prev[W];
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k];
-        int sp = 0;
+        int sp = 0, lo = 0;  // stack depth; lowest position held in the shared window
         __syncthreads();  // the ring's and S.first's previous readers are done
         if (lane == 0) S.first[warp] = prev[0];
         if (tid == 0) S.first[XTED_WARPS] = 0;
@@ -389,7 +398,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = stk + (int64_t)(sp > 0 ? sp - 1 : 0) * stride;
+            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) % XTED_STACK_CACHE) * XTED_WIDE_REG_MAX;
             int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             if (lane == 31) dnext = S.first[warp + 1];
             int loc[W];
@@ -408,17 +417,34 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
                 if (trow && C.foff[k] == C.dend[k] && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
             }
             if (lane == 0) S.first[warp] = prev[0];
-            if (i != i0 && (ri.y & XTED_ROW_ISKR)) sp--;
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
+                sp--;
+                if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
+                    const int32_t *src = stk + (int64_t)(sp - 1) * stride + c0;
+                    int32_t *dst = cache + ((sp - 1) % XTED_STACK_CACHE) * XTED_WIDE_REG_MAX + c0;
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if ((C.far >> k) & 1u) dst[k] = src[k];
+                    lo = sp - 1;
+                }
+            }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = stk + (int64_t)sp * stride + c0;
+                    int32_t *dst = cache + (sp % XTED_STACK_CACHE) * XTED_WIDE_REG_MAX + c0;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = prev[k];
+                    if (P.stack_rows > XTED_STACK_CACHE) {
+                        int32_t *g = stk + (int64_t)sp * stride + c0;
+#pragma unroll
+                        for (int k = 0; k < W; k++)
+                            if ((C.far >> k) & 1u) g[k] = prev[k];
+                    }
                 } else if (tid == 0) {
                     set_error(P, XTED_ENOMEM, 2, sp, P.stack_rows);
                 }
                 sp++;
+                if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
             }
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
             __syncthreads();          // ... and everyone's, the record and the stack push
@@ -428,12 +454,12 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
 }
 
 __device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
-                                int32_t *ring) {
+                                int32_t *ring, int32_t *cache) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk, ring);
-    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk, ring);
-    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk, ring);
-    else run_narrow<8>(P, pr, u, lane, stk, ring);
+    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk, ring, cache);
+    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk, ring, cache);
+    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk, ring, cache);
+    else run_narrow<8>(P, pr, u, lane, stk, ring, cache);
 }
 
 // ---------------------------------------------------------------------------
@@ -536,39 +562,106 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
 }
 
 __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
-                              WideShared &S, int32_t *ring) {
+                              WideShared &S, int32_t *ring, int32_t *cache) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 256) run_wide<1>(P, pr, u, stk, S, ring);
-    else if (width <= 512) run_wide<2>(P, pr, u, stk, S, ring);
-    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S, ring);
-    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S, ring);
+    if (width <= 256) run_wide<1>(P, pr, u, stk, S, ring, cache);
+    else if (width <= 512) run_wide<2>(P, pr, u, stk, S, ring, cache);
+    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S, ring, cache);
+    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S, ring, cache);
     else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S);
     else if (threadIdx.x == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
 }
 
+// ---------------------------------------------------------------------------
+// Ready queue (see xted_internal.h). Entries are appended to their bucket's
+// list; blocks claim tasks from the oldest unexhausted entry of the highest
+// non-empty bucket. An entry is only published after every task of the
+// previous level of its pair has finished, so claimed tasks never wait.
+// ---------------------------------------------------------------------------
+__device__ void rq_publish(const XKernelParams &P, int e) {
+    while (e >= 0) {
+        const XEntry X = P.entries[e];
+        if (X.ntasks > 0) {
+            const int slot = atomicAdd(&P.rq_ctl[2 * X.bucket + 1], 1);
+            ((volatile int32_t *)P.rq)[(int64_t)X.bucket * P.nentries + slot] = e;
+            return;
+        }
+        e = X.next;  // a level without tasks: go on to the next one
+    }
+}
+
+// Returns a task index (and its entry), or -1 when all tasks are done or on
+// error. Idle polling is bounded by time and by iterations.
+__device__ int claim_task(const XKernelParams &P, int *entry) {
+    volatile int32_t *ctl = P.rq_ctl;
+    volatile int32_t *rq = P.rq;
+    unsigned ns = 32;
+    uint64_t t0 = 0;
+    for (long it = 0; it < (1L << 28); it++) {
+        if (*(volatile int32_t *)P.error != 0) return -1;
+        for (int b = XTED_BUCKETS - 1; b >= 0; b--) {
+            int h = ctl[2 * b];
+            while (h < ctl[2 * b + 1]) {
+                const int e = rq[(int64_t)b * P.nentries + h];
+                if (e < 0) break;  // slot reserved but not yet written
+                const int k = atomicAdd(&P.entry_state[2 * e], 1);
+                const XEntry X = P.entries[e];
+                if (k < X.ntasks) {
+                    __threadfence();  // acquire: the level's inputs are visible from here on
+                    *entry = e;
+                    return X.task_off + k;
+                }
+                atomicCAS((int32_t *)&ctl[2 * b], h, h + 1);  // entry exhausted: move the head on
+                h = ctl[2 * b];
+            }
+        }
+        if (ld_acquire(P.done_total) >= P.ntasks) return -1;
+        const uint64_t now = global_ns();
+        if (t0 == 0) {
+            t0 = now;
+        } else if (now - t0 > P.timeout_ns) {
+            set_error(P, XTED_ETIMEOUT, 0, (int)(now - t0 > 0), 0);
+            return -1;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+    set_error(P, XTED_ETIMEOUT, 1, 0, 0);
+    return -1;
+}
+
+// After a task (all its writes fenced and the block synchronised).
+__device__ void complete_task(const XKernelParams &P, int e) {
+    const XEntry X = P.entries[e];
+    const int done = atomicAdd(&P.entry_state[2 * e + 1], 1) + 1;
+    if (done == X.ntasks) {
+        __threadfence();  // acquire the level's other tasks, release to the next level's claimers
+        rq_publish(P, X.next);
+    }
+    __threadfence();
+    atomicAdd(P.done_total, 1);
+}
+
+__global__ void xted_rq_init_kernel(XKernelParams P) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < P.npairs && P.first[p] >= 0) rq_publish(P, P.first[p]);
+}
+
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
-    __shared__ int s_task, s_next;
+    __shared__ int s_task, s_entry, s_next;
     __shared__ WideShared S;
-    __shared__ __align__(16) int32_t s_ring[RING_INTS];
+    extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache (DP_SMEM_BYTES)
+    int32_t *s_ring = s_dyn;
+    int32_t *s_cache = s_dyn + RING_INTS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int32_t *scratch = P.scratch + (int64_t)blockIdx.x * P.scratch_per_cta;
     for (;;) {
         if (tid == 0) {
-            int t = -1;
-            if (*(volatile int32_t *)P.error == 0) {
-                t = atomicAdd(P.task_next, 1);
-                if (t >= P.ntasks) {
-                    t = -1;
-                } else {
-                    if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
-                    const XTask T = P.tasks[t];
-                    if (!wait_ge(P, &P.finished[T.pair], T.need)) {
-                        set_error(P, XTED_ETIMEOUT, t, T.pair, T.need);
-                        t = -1;
-                    }
-                }
-            }
+            int e = -1;
+            const int t = claim_task(P, &e);
+            if (t >= 0 && P.trace) P.trace[4 * (int64_t)t] = global_ns();
             s_task = t;
+            s_entry = e;
             s_next = 0;
         }
         __syncthreads();
@@ -578,24 +671,25 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         const XPair pr = P.pairs[T.pair];
         if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
         if (T.kind_n & XTED_TASK_WIDE) {
-            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S, s_ring);
+            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S, s_ring, s_cache);
         } else {
             // the block's warps take the task's units one at a time
             const int nu = (int)(T.kind_n & 0xffff);
             int32_t *stk = scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX;
             int32_t *ring = s_ring + warp * (XTED_PREFETCH * NARROW_SLOT);
+            int32_t *cache = s_cache + warp * (XTED_STACK_CACHE * XTED_NARROW_MAX);
             for (;;) {
                 int k = 0;
                 if (lane == 0) k = atomicAdd(&s_next, 1);
                 k = __shfl_sync(FULLMASK, k, 0);
                 if (k >= nu) break;
-                dispatch_narrow(P, pr, P.units[T.unit_lo + k], lane, stk, ring);
+                dispatch_narrow(P, pr, P.units[T.unit_lo + k], lane, stk, ring, cache);
             }
         }
         __threadfence();
         __syncthreads();
         if (tid == 0) {
-            atomicAdd(&P.finished[T.pair], 1);
+            complete_task(P, s_entry);
             if (P.trace) {
                 unsigned sm;
                 asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
@@ -617,15 +711,23 @@ __global__ void xted_gather_kernel(const XPair *pairs, const int32_t *trivial, c
 
 // ---- host-side launch helpers ----
 int dp_occupancy(int *blocks_per_sm) {
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, xted_dp_kernel,
-                                                               XTED_CTA_THREADS, 0);
+    cudaError_t e = cudaFuncSetAttribute(xted_dp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_BYTES);
+    if (e != cudaSuccess) return (int)e;
+    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, xted_dp_kernel, XTED_CTA_THREADS,
+                                                               DP_SMEM_BYTES);
 }
 
 cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
     XKernelParams p = P;
     void *args[] = {&p};
-    return cudaLaunchCooperativeKernel((const void *)xted_dp_kernel, dim3(grid),
-                                       dim3(XTED_CTA_THREADS), args, 0, s);
+    return cudaLaunchCooperativeKernel((const void *)xted_dp_kernel, dim3(grid), dim3(XTED_CTA_THREADS), args,
+                                       DP_SMEM_BYTES, s);
+}
+
+cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s) {
+    if (P.npairs <= 0) return cudaSuccess;
+    xted_rq_init_kernel<<<(P.npairs + 255) / 256, 256, 0, s>>>(P);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_gather(const XPair *pairs, const int32_t *trivial, const int32_t *dt, int npairs,

@@ -64,9 +64,9 @@ struct DPair {
 struct DLevel {
     int32_t pair, level;
     int32_t nwide, nnarrow;
-    int32_t ntasks, need;  // tasks at this level; tasks of the pair at lower levels
+    int32_t ntasks, entry;  // tasks at this level; this entry's index
     int32_t task_off, unit_off;
-    int64_t key;           // queue position key (smaller first), see k_pair_rank
+    int64_t key;            // estimate, then the earliest start of the level (see k_pair_rank)
 };
 
 struct PlanPools {
@@ -337,6 +337,13 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     *est_out = est;
 }
 
+// Ready-queue bucket of a level whose pair has `remaining` estimated time left
+// (this level included) when the longest pair of the batch has `chain_max`.
+XT_HD inline int32_t level_bucket(int64_t remaining, int64_t chain_max) {
+    int64_t b = remaining * XTED_BUCKETS / (chain_max + 1);
+    return (int32_t)(b < 0 ? 0 : (b >= XTED_BUCKETS ? XTED_BUCKETS - 1 : b));
+}
+
 // Writes the units and tasks of level entry E (offsets already assigned).
 XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, XTask *tasks) {
     const DPair &q = C.pairs[E.pair];
@@ -353,19 +360,19 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
                 if (bundle == 0) bundle_lo = u;
                 units[u++] = XUnit{r, c};
                 if (++bundle == XTED_TASK_UNITS) {
-                    tasks[t++] = XTask{E.pair, E.need, (uint32_t)bundle, bundle_lo};
+                    tasks[t++] = XTask{E.pair, E.entry, (uint32_t)bundle, bundle_lo};
                     bundle = 0;
                 }
             }
         }
     }
-    if (bundle > 0) tasks[t++] = XTask{E.pair, E.need, (uint32_t)bundle, bundle_lo};
+    if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, (uint32_t)bundle, bundle_lo};
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++)
             for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nwide; c++) {
                 units[u] = XUnit{r, c};
-                tasks[t++] = XTask{E.pair, E.need, XTED_TASK_WIDE | 1u, u};
+                tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
                 u++;
             }
     }

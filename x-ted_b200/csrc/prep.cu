@@ -10,17 +10,14 @@
 //   k_orient       per orientation: node records, kdepth, keyroots by depth,
 //                  column-list positions, row runs, column chunks
 //   k_pair_setup   decomposition choice, level count
-//   k_level_*      unit/task counts and estimates per (pair, level), critical-
-//                  path priority, then the units and tasks themselves
+//   k_level_*      unit/task counts and estimates per (pair, level), ready-
+//                  queue priority, then the units and tasks themselves
 //
-// Level entries are ordered by a key (earliest start plus a quarter of the
-// pair's slack, see k_pair_rank) with a radix sort; every entry's
-// dependencies (lower levels of its pair) have strictly smaller keys, so the
-// resulting queue order respects them.
+// Each (pair, level) entry gets a ready-queue priority bucket from the pair's
+// remaining estimated critical path; the DP kernel publishes an entry when the
+// previous level of its pair has finished (see xted_internal.h).
 // Two small device-to-host reads size the buffers (entries; tasks and units).
 #include <cuda_runtime.h>
-
-#include <cub/device/device_radix_sort.cuh>
 
 #include "ctx.h"
 #include "plan_core.h"
@@ -127,52 +124,43 @@ __global__ void k_level_count(LevelCtx C, DLevel *lv, int64_t nent, int64_t *uni
     tasks[e] = E.ntasks;
 }
 
-// Per pair: est(d) is the estimated time of level d's slowest task. With
-// EST(d) = sum of est over lower levels (earliest start of level d) and
-// C = sum of all est (the pair's chain), a level's queue key is
-//   EST(d) + (Tmax - C) / 4,
-// Tmax the longest chain of the batch: levels are queued about when they can
-// start, and pairs with long chains (little slack) ahead of the others. Keys
-// strictly increase with the level inside a pair, so every task's
-// dependencies are queued before it. need = tasks of the pair at lower levels.
+// Per pair: est(d) is the estimated time of level d's slowest task; EST(d) =
+// sum of est below d; the pair's chain C = sum of all est. A level's ready-
+// queue bucket grows with the pair's remaining chain C - EST(d) relative to
+// the longest chain of the batch.
 __global__ void k_pair_rank(const DPair *pairs, int npairs, DLevel *lv, int64_t *chain, Summary *sum) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
     const DPair q = pairs[p];
     int64_t acc = 0;
-    int32_t need = 0;
     for (int d = 0; d < q.L; d++) {
         DLevel &E = lv[q.lvl_base + d];
         const int64_t est = E.key;
         E.key = acc;
-        E.need = need;
         acc += est;
-        need += E.ntasks;
     }
     chain[p] = acc;
     atomicMax((unsigned long long *)&sum->chain_max, (unsigned long long)acc);
 }
 
-__global__ void k_level_keys(const DLevel *lv, int64_t nent, const int64_t *chain, const Summary *sum,
-                             int64_t *keys, int32_t *ids) {
+__global__ void k_level_offsets(DLevel *lv, int64_t nent, const int64_t *task_scan, const int64_t *unit_scan,
+                                const int64_t *chain, const DPair *pairs, XEntry *entries, Summary *sum) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nent) return;
-    const DLevel E = lv[e];
-    keys[e] = E.key + (sum->chain_max - chain[E.pair]) / 4;
-    ids[e] = (int32_t)e;
-}
-
-__global__ void k_level_offsets(DLevel *lv, int64_t nent, const int32_t *sorted_ids, const int64_t *task_scan,
-                                const int64_t *unit_scan, Summary *sum) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
+    if (e == 0) {
         sum->tasks = task_scan[nent];
         sum->units = unit_scan[nent];
     }
-    if (i >= nent) return;
-    DLevel &E = lv[sorted_ids[i]];
-    E.task_off = (int32_t)task_scan[i];
-    lv[i].unit_off = (int32_t)unit_scan[i];
+    if (e >= nent) return;
+    DLevel &E = lv[e];
+    E.task_off = (int32_t)task_scan[e];
+    E.unit_off = (int32_t)unit_scan[e];
+    E.entry = (int32_t)e;
+    XEntry X;
+    X.task_off = E.task_off;
+    X.ntasks = E.ntasks;
+    X.bucket = level_bucket(chain[E.pair] - E.key, sum->chain_max);
+    X.next = E.level + 1 < pairs[E.pair].L ? (int32_t)e + 1 : -1;
+    entries[e] = X;
 }
 
 __global__ void k_level_fill(LevelCtx C, const DLevel *lv, int64_t nent, XUnit *units, XTask *tasks) {
@@ -181,10 +169,11 @@ __global__ void k_level_fill(LevelCtx C, const DLevel *lv, int64_t nent, XUnit *
 }
 
 __global__ void k_pair_finalize(const DPair *pairs, const DTree *trees, const DOTree *ot, int npairs, XPair *xp,
-                                int32_t *trivial) {
+                                int32_t *trivial, int32_t *first) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
     const DPair q = pairs[p];
+    first[p] = q.L > 0 ? q.lvl_base : -1;
     XPair x;
     x.dt_off = q.dt_off;
     x.m = trees[q.ta].n;
@@ -345,21 +334,17 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
         return XTED_ECUDA;
     }
     const int64_t nent = hs->entries;
-    // ---- buffer B: level entries, sort keys, scans ----
-    size_t cub_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (const int64_t *)nullptr, (int64_t *)nullptr,
-                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)nent, 0, 64, s);
+    if (nent > INT32_MAX / XTED_BUCKETS) return XTED_ENOMEM;
+    // ---- buffer B: level entries and scans ----
     const size_t E1 = (size_t)nent + 1;
-    size_t needB = sizeof(DLevel) * E1 + (2 * 8 + 2 * 4 + 4 * 8) * E1 + cub_bytes + 16 * 256;
+    size_t needB = sizeof(DLevel) * E1 + sizeof(XEntry) * E1 + 4 * 8 * E1 + 12 * 256;
     rc = ctx_dev_reserve(c, c->levels, needB);
     if (rc) return rc;
     Carver cb{(char *)c->levels.p};
     DLevel *d_lv = cb.take<DLevel>(E1);
-    int64_t *d_keys = cb.take<int64_t>(E1), *d_keys2 = cb.take<int64_t>(E1);
-    int32_t *d_ids = cb.take<int32_t>(E1), *d_ids2 = cb.take<int32_t>(E1);
+    XEntry *d_entries = cb.take<XEntry>(E1);
     int64_t *d_units = cb.take<int64_t>(E1), *d_tasks = cb.take<int64_t>(E1);
     int64_t *d_uscan = cb.take<int64_t>(E1), *d_tscan = cb.take<int64_t>(E1);
-    void *d_cub = cb.take<char>(cub_bytes);
     LevelCtx C;
     C.ot = P.otrees;
     C.depths = P.depths;
@@ -371,14 +356,10 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
         k_level_expand<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv);
         k_level_count<<<blocks_for(nent, BS), BS, 0, s>>>(C, d_lv, nent, d_units, d_tasks);
         k_pair_rank<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv, d_chain, d_sum);
-        k_level_keys<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_chain, d_sum, d_keys, d_ids);
-        if (cub::DeviceRadixSort::SortPairs(d_cub, cub_bytes, d_keys, d_keys2, d_ids, d_ids2, (int)nent, 0, 64, s) !=
-            cudaSuccess)
-            return XTED_ECUDA;
-        // the sorted ids give each entry's place in the queue
-        k_scan64<<<1, 1024, 0, s>>>(d_tasks, d_ids2, (int)nent, d_tscan);
+        k_scan64<<<1, 1024, 0, s>>>(d_tasks, nullptr, (int)nent, d_tscan);
         k_scan64<<<1, 1024, 0, s>>>(d_units, nullptr, (int)nent, d_uscan);
-        k_level_offsets<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_ids2, d_tscan, d_uscan, d_sum);
+        k_level_offsets<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_tscan, d_uscan, d_chain, d_pairs,
+                                                              d_entries, d_sum);
     }
     cudaMemcpyAsync(hs, d_sum, sizeof(Summary), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) {
@@ -387,16 +368,21 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     }
     const int64_t ntasks = nent > 0 ? hs->tasks : 0, nunits = nent > 0 ? hs->units : 0;
     if (ntasks > INT32_MAX / 2 || nunits > INT32_MAX / 2) return XTED_ENOMEM;
-    // ---- buffer C: units and tasks ----
+    // ---- buffer C: units, tasks and the ready queue's state ----
+    const size_t rq_ints = (size_t)XTED_BUCKETS * E1;
     rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
-                                         512);
+                                         4 * (2 * E1 + rq_ints + (size_t)npairs + 2 * XTED_BUCKETS + 8) + 8 * 256);
     if (rc) return rc;
     Carver cw{(char *)c->work.p};
     XUnit *d_units_out = cw.take<XUnit>((size_t)nunits);
     XTask *d_tasks_out = cw.take<XTask>((size_t)ntasks);
+    int32_t *d_first = cw.take<int32_t>((size_t)npairs);
+    int32_t *d_state = cw.take<int32_t>(2 * E1);  // claimed, done per entry
+    int32_t *d_rq = cw.take<int32_t>(rq_ints);
+    int32_t *d_ctl = cw.take<int32_t>(2 * XTED_BUCKETS + 8);  // heads/tails, then the done counter
     if (nent > 0) k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out);
     k_pair_finalize<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_xpairs,
-                                                                       d_trivial);
+                                                                       d_trivial, d_first);
     if (cudaGetLastError() != cudaSuccess) return XTED_ECUDA;
 
     std::memset(&K, 0, sizeof(K));
@@ -408,7 +394,15 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.pairs = d_xpairs;
     K.units = d_units_out;
     K.tasks = d_tasks_out;
+    K.entries = d_entries;
+    K.first = d_first;
     K.ntasks = (int32_t)ntasks;
+    K.nentries = (int32_t)nent;
+    K.npairs = npairs;
+    K.entry_state = d_state;
+    K.rq = d_rq;
+    K.rq_ctl = d_ctl;
+    K.done_total = d_ctl + 2 * XTED_BUCKETS;
     c->d_trivial = d_trivial;
     c->plan_dt_elems = hs->dt_elems;
     c->plan_stack_rows = std::max(hs->stack_rows, 1);

@@ -79,9 +79,24 @@ struct XUnit {
 
 struct XTask {
     int32_t pair;
-    int32_t need;     // tasks of this pair at lower levels that must finish first
+    int32_t entry;    // its (pair, level) entry
     uint32_t kind_n;  // XTED_TASK_WIDE | number of units
     int32_t unit_lo;  // first unit
+};
+
+// Ready queue. Every (pair, level) is an entry whose tasks are contiguous.
+// An entry is published into the ready queue of its priority bucket when the
+// last task of the pair's previous level finishes (level 0 at launch), so a
+// block only ever claims tasks whose tables' inputs are complete; the
+// reference instead runs one host-synchronised level at a time
+// (X-TED_CPU/parallel_computing.cpp:155-182, X-TED_GPU/parallel_X_TED.cu:312-387).
+#define XTED_BUCKETS 16
+
+struct XEntry {
+    int32_t task_off;  // first task
+    int32_t ntasks;
+    int32_t bucket;    // priority: larger = longer remaining critical path of the pair
+    int32_t next;      // entry of the pair's next level, -1 after the last level
 };
 
 struct XKernelParams {
@@ -93,15 +108,20 @@ struct XKernelParams {
     const XPair *pairs;
     const XUnit *units;
     const XTask *tasks;
+    const XEntry *entries;
+    const int32_t *first;  // [npairs] level-0 entry of every pair, -1 for pairs with an empty tree
     int32_t *dt;          // all distance tables
     int32_t *scratch;     // per-block far-row stacks (and wide generic rows)
     int64_t scratch_per_cta; // int32 elements
     int32_t stack_rows;   // stack capacity in rows
     int32_t ntasks;
-    int32_t *task_next;   // queue head
-    int32_t *finished;    // per pair finished-task counters
+    int32_t nentries, npairs;
+    int32_t *entry_state; // [2 * nentries]: tasks claimed, tasks done
+    int32_t *rq;          // [XTED_BUCKETS * nentries]: published entry ids, -1 = slot not yet written
+    int32_t *rq_ctl;      // [2 * XTED_BUCKETS]: head, tail of each bucket
+    int32_t *done_total;  // finished tasks
     int32_t *error;       // 0 = ok; else an XTED error code
     int32_t *error_info;  // [4] diagnostics of the first error
-    uint64_t timeout_ns;  // bound on each dependency wait
+    uint64_t timeout_ns;  // bound on every idle wait
     unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, sm|units|kind
 };
