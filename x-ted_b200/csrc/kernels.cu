@@ -591,28 +591,50 @@ __device__ void rq_publish(const XKernelParams &P, int e) {
 }
 
 // Returns a task index (and its entry), or -1 when all tasks are done or on
-// error. Idle polling is bounded by time and by iterations.
+// error. Blocks probe a bucket's live window [head, tail) starting at a
+// block-dependent position, so they spread over many entries instead of all
+// contending for the head entry, and test an entry with a plain load before
+// claiming from it; whoever sees exhausted entries at the head moves it on.
+// Idle polling is bounded by time and by iterations.
 __device__ int claim_task(const XKernelParams &P, int *entry) {
     volatile int32_t *ctl = P.rq_ctl;
     volatile int32_t *rq = P.rq;
+    volatile int32_t *state = P.entry_state;
     unsigned ns = 32;
     uint64_t t0 = 0;
+    unsigned salt = blockIdx.x * 2654435761u;
     for (long it = 0; it < (1L << 28); it++) {
         if (*(volatile int32_t *)P.error != 0) return -1;
         for (int b = XTED_BUCKETS - 1; b >= 0; b--) {
+            const int32_t *slots = P.rq + (int64_t)b * P.nentries;
             int h = ctl[2 * b];
-            while (h < ctl[2 * b + 1]) {
+            // move the head over exhausted entries
+            for (int guard = 0; guard < 64; guard++) {
+                if (h >= ctl[2 * b + 1]) break;
                 const int e = rq[(int64_t)b * P.nentries + h];
-                if (e < 0) break;  // slot reserved but not yet written
-                const int k = atomicAdd(&P.entry_state[2 * e], 1);
+                if (e < 0 || state[2 * e] < P.entries[e].ntasks) break;
+                atomicCAS((int32_t *)&ctl[2 * b], h, h + 1);
+                h = ctl[2 * b];
+            }
+            const int tl = ctl[2 * b + 1];
+            const int live = tl - h;
+            if (live <= 0) continue;
+            salt = salt * 1664525u + 1013904223u;
+            const int start = (int)(salt % (unsigned)live);
+            const int probes = live < 32 ? live : 32;
+            for (int j = 0; j < probes; j++) {
+                int pos = h + start + j;
+                if (pos >= tl) pos -= live;
+                const int e = ((volatile const int32_t *)slots)[pos];
+                if (e < 0) continue;  // slot reserved but not yet written
                 const XEntry X = P.entries[e];
+                if (state[2 * e] >= X.ntasks) continue;
+                const int k = atomicAdd(&P.entry_state[2 * e], 1);
                 if (k < X.ntasks) {
                     __threadfence();  // acquire: the level's inputs are visible from here on
                     *entry = e;
                     return X.task_off + k;
                 }
-                atomicCAS((int32_t *)&ctl[2 * b], h, h + 1);  // entry exhausted: move the head on
-                h = ctl[2 * b];
             }
         }
         if (ld_acquire(P.done_total) >= P.ntasks) return -1;
@@ -620,7 +642,7 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
         if (t0 == 0) {
             t0 = now;
         } else if (now - t0 > P.timeout_ns) {
-            set_error(P, XTED_ETIMEOUT, 0, (int)(now - t0 > 0), 0);
+            set_error(P, XTED_ETIMEOUT, 0, 0, 0);
             return -1;
         }
         __nanosleep(ns);
@@ -690,11 +712,22 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         __syncthreads();
         if (tid == 0) {
             complete_task(P, s_entry);
-            if (P.trace) {
+            if (P.trace) {  // info: wide(1) | units(7) | sm(8) | widest chunk(16) | cells(32)
                 unsigned sm;
                 asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+                const int nu = (int)(T.kind_n & 0xffff);
+                unsigned long long cells = 0, wmax = 0;
+                for (int k = 0; k < nu; k++) {
+                    const XUnit u = P.units[T.unit_lo + k];
+                    const unsigned long long w = (unsigned)P.chunks[u.chunk].width;
+                    cells += w * (unsigned)P.runs[u.run].rows;
+                    if (w > wmax) wmax = w;
+                }
                 P.trace[4 * (int64_t)t + 2] = global_ns();
-                P.trace[4 * (int64_t)t + 3] = (unsigned long long)sm | ((unsigned long long)T.kind_n << 32);
+                P.trace[4 * (int64_t)t + 3] = ((T.kind_n & XTED_TASK_WIDE) ? 1ull : 0ull) |
+                                              ((unsigned long long)(nu & 127) << 1) |
+                                              ((unsigned long long)(sm & 255) << 8) |
+                                              ((wmax & 0xffff) << 16) | ((cells & 0xffffffffull) << 32);
             }
         }
     }

@@ -19,6 +19,8 @@
 // Two small device-to-host reads size the buffers (entries; tasks and units).
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "ctx.h"
 #include "plan_core.h"
 

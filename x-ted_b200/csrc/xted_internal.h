@@ -123,5 +123,5 @@ struct XKernelParams {
     int32_t *error;       // 0 = ok; else an XTED error code
     int32_t *error_info;  // [4] diagnostics of the first error
     uint64_t timeout_ns;  // bound on every idle wait
-    unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, sm|units|kind
+    unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, info
 };
