@@ -50,12 +50,13 @@ __device__ __forceinline__ void set_error(const XKernelParams &P, int code, int 
     }
 }
 
+// Inclusive suffix minimum over the warp (lane l: min over lanes >= l). A lane
+// whose source is out of range gets its own value back from shfl.down, which
+// leaves the minimum unchanged, so no bounds test is needed.
 __device__ __forceinline__ int warp_suffix_min(int v, int lane) {
+    (void)lane;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        int o = __shfl_down_sync(FULLMASK, v, d);
-        if (lane + d < 32) v = min(v, o);
-    }
+    for (int d = 1; d < 32; d <<= 1) v = min(v, __shfl_down_sync(FULLMASK, v, d));
     return v;
 }
 
@@ -71,7 +72,9 @@ __device__ __forceinline__ int warp_prefix_sum(int v, int lane) {
 // Per-column state of one thread: W consecutive columns of the chunk.
 template <int W>
 struct Cols {
-    int node[W], lab[W], foff[W], dend[W], key[W];
+    int node[W], lab[W], dend[W], key[W];
+    int fb[W];      // je - orl(j) - 1: the far value on the table's right path (0 = tree column)
+    int fidx[W];    // stack-row index of the far column orl(j)+1 (clamped into the row)
     unsigned far;   // bit k: column k is a far column (pushed with stack rows)
     unsigned valid; // bit k: column k exists
 };
@@ -82,7 +85,7 @@ struct Cols {
 // records (label, orl, previous-node-is-leaf flag).
 template <int W>
 __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &pr, const XChunk &ch, int c0,
-                                          Cols<W> &C) {
+                                          Cols<W> &C, int row_max) {
     C.far = 0;
     C.valid = 0;
     const int2 *nodes = P.rowinfo + pr.col_base;
@@ -111,18 +114,21 @@ __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &p
                 j = j0;
             }
             const int2 nd = __ldg(&nodes[j]);
+            const int foff = (nd.y & XTED_ROW_ORL_MASK) + 1 - j;
             C.node[k] = j;
             C.lab[k] = nd.x;
-            C.foff[k] = (nd.y & XTED_ROW_ORL_MASK) + 1 - j;
             C.dend[k] = je - j;
+            C.fb[k] = je - j - foff;
+            C.fidx[k] = min(c + foff, row_max);
             if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) C.far |= 1u << k;
             C.valid |= 1u << k;
             j++;
         } else {
             C.node[k] = 0;
             C.lab[k] = 0;
-            C.foff[k] = 1;
-            C.dend[k] = 2;  // never a segment end, never a tree column
+            C.dend[k] = 2;  // never a segment end
+            C.fb[k] = 1;    // never a tree column
+            C.fidx[k] = min(c, row_max);
         }
     }
 }
@@ -146,33 +152,32 @@ __device__ __forceinline__ void set_keys(Cols<W> &C, int c0, int before) {
 }
 
 // The per-row cell work shared by both executors: builds v = A + key for the
-// thread's columns and their local suffix minima. Returns the thread's minimum.
+// thread's columns and their local suffix minima; returns the thread's
+// minimum. Branch-free: the ring and stack reads for every column are issued
+// first, then each column is a handful of selects and one link of the
+// running-minimum chain.
 template <int W>
-__device__ __forceinline__ int row_cells(const Cols<W> &C, const int (&prev)[W], const int (&cur_dt)[W],
+__device__ __forceinline__ int row_cells(const Cols<W> &C, const int (&prev)[W], const int32_t *slot,
                                          int dnext, bool trow, int rl, int bord, int rowfar,
                                          const int32_t *top, int c0, int (&loc)[W]) {
+    int cur[W], farv[W];
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        cur[k] = slot[c0 + k];
+        farv[k] = top[C.fidx[k]];
+    }
     int run = XTED_INF;
 #pragma unroll
     for (int k = W - 1; k >= 0; k--) {
         const int up = prev[k];
-        int diag = (k == W - 1) ? dnext : prev[k + 1];
         const bool segend = C.dend[k] == 1;
-        if (segend) diag = bord - 1;
-        const bool tcol = C.foff[k] == C.dend[k];
-        int a;
-        if (trow && tcol) {
-            a = diag + (rl != C.lab[k]);
-        } else {
-            int far;
-            if (trow) far = C.dend[k] - C.foff[k];
-            else if (tcol) far = rowfar;
-            else far = ((C.valid >> k) & 1u) ? top[c0 + k + C.foff[k]] : 0;
-            a = cur_dt[k] + far;
-        }
+        const int diag = segend ? bord - 1 : ((k == W - 1) ? dnext : prev[k + 1]);
+        const bool tcol = C.fb[k] == 0;
+        const int farsel = trow ? C.fb[k] : (tcol ? rowfar : farv[k]);
+        const int a = (trow && tcol) ? diag + (rl != C.lab[k] ? 1 : 0) : cur[k] + farsel;
         int A = min(a, up + 1);
-        if (segend) A = min(A, bord + 1);
-        const int v = ((C.valid >> k) & 1u) ? A + C.key[k] : XTED_INF;
-        run = min(run, v);
+        A = segend ? min(A, bord + 1) : A;
+        run = min(run, ((C.valid >> k) & 1u) ? A + C.key[k] : XTED_INF);
         loc[k] = run;
     }
     return run;
@@ -233,7 +238,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = lane * W;
     Cols<W> C;
-    load_cols<W>(P, pr, ch, c0, C);
+    load_cols<W>(P, pr, ch, c0, C, XTED_NARROW_MAX - 1);
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -270,18 +275,15 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             cp_async_wait<PF - 1>();
             __syncwarp();
             const int32_t *slot = ring + (i & (PF - 1)) * NARROW_SLOT;
-            int cur[W];
-#pragma unroll
-            for (int k = 0; k < W; k++) cur[k] = slot[c0 + k];
             const int2 ri = *(const int2 *)(slot + stride);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) % XTED_STACK_CACHE) * stride;
+            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * stride;
             const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             int loc[W];
-            const int mine = row_cells<W>(C, prev, cur, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
+            const int mine = row_cells<W>(C, prev, slot, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
             const int incl = warp_suffix_min(mine, lane);
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
             if (lane == 31) carry = XTED_INF;
@@ -290,14 +292,14 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             for (int k = 0; k < W; k++) {
                 const int d = min(loc[k], carry) - C.key[k];
                 prev[k] = d;
-                if (trow && C.foff[k] == C.dend[k] && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
+                if (trow && C.fb[k] == 0 && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
             }
-            __syncwarp();
+            // every lane has read this row's stack top (its values fed the scan above)
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) % XTED_STACK_CACHE) * stride + c0;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * stride + c0;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = src[k];
@@ -306,7 +308,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp % XTED_STACK_CACHE) * stride + c0;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * stride + c0;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = prev[k];
@@ -347,7 +349,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
     const int stride = ch.width;
     constexpr int PF = XTED_PREFETCH;
     Cols<W> C;
-    load_cols<W>(P, pr, ch, c0, C);
+    load_cols<W>(P, pr, ch, c0, C, XTED_WIDE_REG_MAX - 1);
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -390,19 +392,16 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
                 cp_async_commit();
             }
             const int32_t *slot = ring + (i & (PF - 1)) * WIDE_SLOT;
-            int cur[W];
-#pragma unroll
-            for (int k = 0; k < W; k++) cur[k] = slot[c0 + k];
             const int2 ri = *(const int2 *)(slot + XTED_WIDE_REG_MAX);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) % XTED_STACK_CACHE) * XTED_WIDE_REG_MAX;
+            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * XTED_WIDE_REG_MAX;
             int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             if (lane == 31) dnext = S.first[warp + 1];
             int loc[W];
-            const int mine = row_cells<W>(C, prev, cur, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
+            const int mine = row_cells<W>(C, prev, slot, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
             __syncthreads();
@@ -414,14 +413,14 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             for (int k = 0; k < W; k++) {
                 const int d = min(loc[k], carry) - C.key[k];
                 prev[k] = d;
-                if (trow && C.foff[k] == C.dend[k] && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
+                if (trow && C.fb[k] == 0 && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
             }
             if (lane == 0) S.first[warp] = prev[0];
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (int64_t)(sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) % XTED_STACK_CACHE) * XTED_WIDE_REG_MAX + c0;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * XTED_WIDE_REG_MAX + c0;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = src[k];
@@ -430,7 +429,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp % XTED_STACK_CACHE) * XTED_WIDE_REG_MAX + c0;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * XTED_WIDE_REG_MAX + c0;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = prev[k];
