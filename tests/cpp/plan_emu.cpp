@@ -196,7 +196,7 @@ static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vec
     }
     if (seg != ch.nseg || s != ch.k_lo + ch.nseg - 1) FAIL("chunk segment count mismatch");
     // global stack (written only when units can nest deeper than the window) and the window
-    const bool deep = H.stack_rows > g_cache;
+    const bool deep = run.depth > g_cache;  // the kernels' rule: depth-d tables nest <= d rows
     std::vector<std::vector<int>> stk((size_t)H.stack_rows, std::vector<int>((size_t)W, -777));
     std::vector<std::vector<int>> cache((size_t)g_cache, std::vector<int>((size_t)W, -777));
     std::vector<int> prev(W), cur(W), loc(W);
@@ -265,6 +265,7 @@ static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vec
                         if (deep) stk[(size_t)sp][(size_t)c] = prev[c];
                     }
                 sp++;
+                if (sp > run.depth) FAIL("stack depth %d above the run's keyroot depth %d", sp, run.depth);
                 if (sp - lo > g_cache) lo = sp - g_cache;
             }
         }

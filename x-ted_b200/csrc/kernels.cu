@@ -69,6 +69,12 @@ __device__ __forceinline__ int warp_prefix_sum(int v, int lane) {
     return v;
 }
 
+// Shared rows (ring slots and stack rows) store column c at pad(c) = c + c/32:
+// a thread owning W consecutive columns then reads and writes its k-th column
+// in a different bank from every other lane of its warp (the plain layout put
+// lanes W columns apart, a W-way bank conflict on every access).
+__device__ __forceinline__ int pad(int c) { return c + (c >> 5); }
+
 // Per-column state of one thread: W consecutive columns of the chunk.
 template <int W>
 struct Cols {
@@ -119,7 +125,7 @@ __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &p
             C.lab[k] = nd.x;
             C.dend[k] = je - j;
             C.fb[k] = je - j - foff;
-            C.fidx[k] = min(c + foff, row_max);
+            C.fidx[k] = pad(min(c + foff, row_max));
             if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) C.far |= 1u << k;
             C.valid |= 1u << k;
             j++;
@@ -128,7 +134,7 @@ __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &p
             C.lab[k] = 0;
             C.dend[k] = 2;  // never a segment end
             C.fb[k] = 1;    // never a tree column
-            C.fidx[k] = min(c, row_max);
+            C.fidx[k] = pad(min(c, row_max));
         }
     }
 }
@@ -163,7 +169,7 @@ __device__ __forceinline__ int row_cells(const Cols<W> &C, const int (&prev)[W],
     int cur[W], farv[W];
 #pragma unroll
     for (int k = 0; k < W; k++) {
-        cur[k] = slot[c0 + k];
+        cur[k] = slot[pad(c0 + k)];
         farv[k] = top[C.fidx[k]];
     }
     int run = XTED_INF;
@@ -208,13 +214,15 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // the global stack only when a unit can nest deeper than that, and a row that
 // falls out of the window is reloaded from there when the stack unwinds.
 #define XTED_STACK_CACHE 8
-#define NARROW_SLOT (XTED_NARROW_MAX + 8)  // ints per ring slot: columns, then the row record
-#define WIDE_SLOT (XTED_WIDE_REG_MAX + 8)
+#define NARROW_ROW (XTED_NARROW_MAX + XTED_NARROW_MAX / 32)     // 264 ints
+#define WIDE_ROW (XTED_WIDE_REG_MAX + XTED_WIDE_REG_MAX / 32)   // 2112 ints
+#define NARROW_SLOT (NARROW_ROW + 8)  // ring slot: padded columns, then the row record (8-byte aligned)
+#define WIDE_SLOT (WIDE_ROW + 8)
 #define RING_INTS ((XTED_WARPS * XTED_PREFETCH * NARROW_SLOT) > (XTED_PREFETCH * WIDE_SLOT) \
                        ? (XTED_WARPS * XTED_PREFETCH * NARROW_SLOT)                          \
                        : (XTED_PREFETCH * WIDE_SLOT))
-#define CACHE_INTS (XTED_STACK_CACHE * XTED_WIDE_REG_MAX)  // = warps x depth x narrow width
-static_assert(CACHE_INTS == XTED_WARPS * XTED_STACK_CACHE * XTED_NARROW_MAX, "stack cache split");
+#define CACHE_INTS (XTED_STACK_CACHE * WIDE_ROW)  // = warps x depth x padded narrow row
+static_assert(CACHE_INTS == XTED_WARPS * XTED_STACK_CACHE * NARROW_ROW, "stack cache split");
 #define DP_SMEM_BYTES ((RING_INTS + CACHE_INTS) * 4)
 
 // Issues the copies of row r (this thread's columns; one thread: the record).
@@ -224,7 +232,7 @@ __device__ __forceinline__ void issue_row(const Cols<W> &C, const int32_t *dt, i
     const int32_t *drow = dt + (int64_t)r * n;
 #pragma unroll
     for (int k = 0; k < W; k++)
-        if ((C.valid >> k) & 1u) cp_async4(slot + c0 + k, drow + C.node[k]);
+        if ((C.valid >> k) & 1u) cp_async4(slot + pad(c0 + k), drow + C.node[k]);
     if (rec) cp_async8(slot + rec_at, rows + r);
 }
 
@@ -250,6 +258,9 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     const int2 *rows = P.rowinfo + pr.row_base;
     const int stride = XTED_NARROW_MAX;
     constexpr int PF = XTED_PREFETCH;
+    // a table at keyroot depth d nests at most d stack rows (nested keyroots have
+    // strictly smaller depths), so only deep runs need the global copy of the stack
+    const bool deep = run.depth > XTED_STACK_CACHE;
 
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
@@ -262,25 +273,25 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
-            if (r >= i0) issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, stride, c0, lane == 0);
+            if (r >= i0) issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, c0, lane == 0);
             cp_async_commit();
         }
         for (int i = imax - 1; i >= i0; i--) {
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, stride, c0, lane == 0);
+                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, c0, lane == 0);
                 cp_async_commit();
             }
             cp_async_wait<PF - 1>();
             __syncwarp();
             const int32_t *slot = ring + (i & (PF - 1)) * NARROW_SLOT;
-            const int2 ri = *(const int2 *)(slot + stride);
+            const int2 ri = *(const int2 *)(slot + NARROW_ROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * stride;
+            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
             const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             int loc[W];
             const int mine = row_cells<W>(C, prev, slot, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
@@ -299,20 +310,20 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * stride + c0;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = src[k];
+                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = src[k];
                     lo = sp - 1;
                 }
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * stride + c0;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = prev[k];
-                    if (P.stack_rows > XTED_STACK_CACHE) {
+                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = prev[k];
+                    if (deep) {
                         int32_t *g = stk + sp * stride + c0;
 #pragma unroll
                         for (int k = 0; k < W; k++)
@@ -348,6 +359,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
     const int c0 = tid * W;
     const int stride = ch.width;
     constexpr int PF = XTED_PREFETCH;
+    const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, XTED_WIDE_REG_MAX - 1);
     {
@@ -378,7 +390,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
             if (r >= i0)
-                issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, XTED_WIDE_REG_MAX, c0, tid == 0);
+                issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, c0, tid == 0);
             cp_async_commit();
         }
         cp_async_wait<PF - 2>();
@@ -387,17 +399,17 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, XTED_WIDE_REG_MAX, c0,
+                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, c0,
                                  tid == 0);
                 cp_async_commit();
             }
             const int32_t *slot = ring + (i & (PF - 1)) * WIDE_SLOT;
-            const int2 ri = *(const int2 *)(slot + XTED_WIDE_REG_MAX);
+            const int2 ri = *(const int2 *)(slot + WIDE_ROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * XTED_WIDE_REG_MAX;
+            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
             int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             if (lane == 31) dnext = S.first[warp + 1];
             int loc[W];
@@ -420,20 +432,20 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (int64_t)(sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * XTED_WIDE_REG_MAX + c0;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = src[k];
+                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = src[k];
                     lo = sp - 1;
                 }
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * XTED_WIDE_REG_MAX + c0;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = prev[k];
-                    if (P.stack_rows > XTED_STACK_CACHE) {
+                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = prev[k];
+                    if (deep) {
                         int32_t *g = stk + (int64_t)sp * stride + c0;
 #pragma unroll
                         for (int k = 0; k < W; k++)
@@ -698,7 +710,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
             const int nu = (int)(T.kind_n & 0xffff);
             int32_t *stk = scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX;
             int32_t *ring = s_ring + warp * (XTED_PREFETCH * NARROW_SLOT);
-            int32_t *cache = s_cache + warp * (XTED_STACK_CACHE * XTED_NARROW_MAX);
+            int32_t *cache = s_cache + warp * (XTED_STACK_CACHE * NARROW_ROW);
             for (;;) {
                 int k = 0;
                 if (lane == 0) k = atomicAdd(&s_next, 1);
