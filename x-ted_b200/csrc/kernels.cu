@@ -223,16 +223,25 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
                        : (XTED_PREFETCH * WIDE_SLOT))
 #define CACHE_INTS (XTED_STACK_CACHE * WIDE_ROW)  // = warps x depth x padded narrow row
 static_assert(CACHE_INTS == XTED_WARPS * XTED_STACK_CACHE * NARROW_ROW, "stack cache split");
-#define DP_SMEM_BYTES ((RING_INTS + CACHE_INTS) * 4)
+#define CNODE_INTS XTED_WIDE_REG_MAX  // = warps x narrow width: node ids of the unit's columns
+#define DP_SMEM_BYTES ((RING_INTS + CACHE_INTS + CNODE_INTS) * 4)
 
-// Issues the copies of row r (this thread's columns; one thread: the record).
+// Issues the copies of row r. Copies are coalesced: thread `me` of `nthr`
+// copies columns me, me + nthr, ... (node ids from the unit's shared column
+// table), so consecutive lanes read consecutive tree distances; one thread
+// also copies the row's node record. The thread that computes a column is not
+// the one that copied it, so a row is read only after a barrier that follows
+// every copier's wait.
 template <int W>
-__device__ __forceinline__ void issue_row(const Cols<W> &C, const int32_t *dt, int n, const int2 *rows, int r,
-                                          int32_t *slot, int rec_at, int c0, bool rec) {
+__device__ __forceinline__ void issue_row(const int32_t *cnode, int width, const int32_t *dt, int n,
+                                          const int2 *rows, int r, int32_t *slot, int rec_at, int me, int nthr,
+                                          bool rec) {
     const int32_t *drow = dt + (int64_t)r * n;
 #pragma unroll
-    for (int k = 0; k < W; k++)
-        if ((C.valid >> k) & 1u) cp_async4(slot + pad(c0 + k), drow + C.node[k]);
+    for (int j = 0; j < W; j++) {
+        const int c = me + j * nthr;
+        if (c < width) cp_async4(slot + pad(c), drow + cnode[c]);
+    }
     if (rec) cp_async8(slot + rec_at, rows + r);
 }
 
@@ -241,12 +250,18 @@ __device__ __forceinline__ void issue_row(const Cols<W> &C, const int32_t *dt, i
 // ---------------------------------------------------------------------------
 template <int W>
 __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
-                           int32_t *ring, int32_t *cache) {
+                           int32_t *ring, int32_t *cache, int32_t *cnode) {
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = lane * W;
+    const int width = ch.width;
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, XTED_NARROW_MAX - 1);
+    __syncwarp();  // the previous unit's copies have drained (cp_async_wait<0> at its end)
+#pragma unroll
+    for (int k = 0; k < W; k++)
+        if ((C.valid >> k) & 1u) cnode[c0 + k] = C.node[k];
+    __syncwarp();
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -273,14 +288,17 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
-            if (r >= i0) issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, c0, lane == 0);
+            if (r >= i0)
+                issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, lane,
+                             32, lane == 0);
             cp_async_commit();
         }
         for (int i = imax - 1; i >= i0; i--) {
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, c0, lane == 0);
+                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW,
+                                 lane, 32, lane == 0);
                 cp_async_commit();
             }
             cp_async_wait<PF - 1>();
@@ -352,16 +370,20 @@ struct WideShared {
 
 template <int W>
 __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
-                         int32_t *ring, int32_t *cache) {
+                         int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = tid * W;
     const int stride = ch.width;
+    const int width = ch.width;
     constexpr int PF = XTED_PREFETCH;
     const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, XTED_WIDE_REG_MAX - 1);
+#pragma unroll
+    for (int k = 0; k < W; k++)
+        if ((C.valid >> k) & 1u) cnode[c0 + k] = C.node[k];
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -390,7 +412,8 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
             if (r >= i0)
-                issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, c0, tid == 0);
+                issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, tid,
+                             XTED_CTA_THREADS, tid == 0);
             cp_async_commit();
         }
         cp_async_wait<PF - 2>();
@@ -399,8 +422,8 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(C, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, c0,
-                                 tid == 0);
+                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, tid,
+                                 XTED_CTA_THREADS, tid == 0);
                 cp_async_commit();
             }
             const int32_t *slot = ring + (i & (PF - 1)) * WIDE_SLOT;
@@ -465,12 +488,12 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
 }
 
 __device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
-                                int32_t *ring, int32_t *cache) {
+                                int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk, ring, cache);
-    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk, ring, cache);
-    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk, ring, cache);
-    else run_narrow<8>(P, pr, u, lane, stk, ring, cache);
+    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk, ring, cache, cnode);
+    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk, ring, cache, cnode);
+    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk, ring, cache, cnode);
+    else run_narrow<8>(P, pr, u, lane, stk, ring, cache, cnode);
 }
 
 // ---------------------------------------------------------------------------
@@ -573,12 +596,12 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
 }
 
 __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
-                              WideShared &S, int32_t *ring, int32_t *cache) {
+                              WideShared &S, int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 256) run_wide<1>(P, pr, u, stk, S, ring, cache);
-    else if (width <= 512) run_wide<2>(P, pr, u, stk, S, ring, cache);
-    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S, ring, cache);
-    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S, ring, cache);
+    if (width <= 256) run_wide<1>(P, pr, u, stk, S, ring, cache, cnode);
+    else if (width <= 512) run_wide<2>(P, pr, u, stk, S, ring, cache, cnode);
+    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S, ring, cache, cnode);
+    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S, ring, cache, cnode);
     else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S);
     else if (threadIdx.x == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
 }
@@ -683,9 +706,10 @@ __global__ void xted_rq_init_kernel(XKernelParams P) {
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
     __shared__ int s_task, s_entry, s_next;
     __shared__ WideShared S;
-    extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache (DP_SMEM_BYTES)
+    extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache | column nodes (DP_SMEM_BYTES)
     int32_t *s_ring = s_dyn;
     int32_t *s_cache = s_dyn + RING_INTS;
+    int32_t *s_cnode = s_cache + CACHE_INTS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int32_t *scratch = P.scratch + (int64_t)blockIdx.x * P.scratch_per_cta;
     for (;;) {
@@ -704,19 +728,20 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         const XPair pr = P.pairs[T.pair];
         if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
         if (T.kind_n & XTED_TASK_WIDE) {
-            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S, s_ring, s_cache);
+            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S, s_ring, s_cache, s_cnode);
         } else {
             // the block's warps take the task's units one at a time
             const int nu = (int)(T.kind_n & 0xffff);
             int32_t *stk = scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX;
             int32_t *ring = s_ring + warp * (XTED_PREFETCH * NARROW_SLOT);
             int32_t *cache = s_cache + warp * (XTED_STACK_CACHE * NARROW_ROW);
+            int32_t *cnode = s_cnode + warp * XTED_NARROW_MAX;
             for (;;) {
                 int k = 0;
                 if (lane == 0) k = atomicAdd(&s_next, 1);
                 k = __shfl_sync(FULLMASK, k, 0);
                 if (k >= nu) break;
-                dispatch_narrow(P, pr, P.units[T.unit_lo + k], lane, stk, ring, cache);
+                dispatch_narrow(P, pr, P.units[T.unit_lo + k], lane, stk, ring, cache, cnode);
             }
         }
         __threadfence();
