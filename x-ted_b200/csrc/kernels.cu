@@ -76,12 +76,20 @@ __device__ __forceinline__ int warp_prefix_sum(int v, int lane) {
 __device__ __forceinline__ int pad(int c) { return c + (c >> 5); }
 
 // Per-column state of one thread: W consecutive columns of the chunk.
+// Columns past the chunk's end are inert: key KEY_INVALID lifts their scan
+// values above every real one, and their inputs (zeroed shared memory or old
+// distances, never negative) keep them bounded.
+#define KEY_INVALID 0x20000000
+#define NOSEG 0x40000000
 template <int W>
 struct Cols {
-    int node[W], lab[W], dend[W], key[W];
-    int fb[W];      // je - orl(j) - 1: the far value on the table's right path (0 = tree column)
-    int fidx[W];    // stack-row index of the far column orl(j)+1 (clamped into the row)
+    int node[W], lab[W], key[W];
+    int fb[W];      // je - orl(j) - 1: far value on the table's right path (0: a tree column)
+    int fidx[W];    // padded stack index of the far column orl(j)+1
+    int segor[W];   // 0 at a segment's last column, NOSEG elsewhere (min(A, (bord+1) | segor))
+    int dend[W];    // je - j: the table's bottom border, the first row above
     unsigned far;   // bit k: column k is a far column (pushed with stack rows)
+    unsigned tcol;  // bit k: column k is on its segment's right path
     unsigned valid; // bit k: column k exists
 };
 
@@ -93,6 +101,7 @@ template <int W>
 __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &pr, const XChunk &ch, int c0,
                                           Cols<W> &C, int row_max) {
     C.far = 0;
+    C.tcol = 0;
     C.valid = 0;
     const int2 *nodes = P.rowinfo + pr.col_base;
     int s = ch.k_lo, j = 0, j0 = 0, je = 0;
@@ -126,15 +135,18 @@ __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &p
             C.dend[k] = je - j;
             C.fb[k] = je - j - foff;
             C.fidx[k] = pad(min(c + foff, row_max));
+            C.segor[k] = je - j == 1 ? 0 : NOSEG;
             if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) C.far |= 1u << k;
+            if (je - j == foff) C.tcol |= 1u << k;
             C.valid |= 1u << k;
             j++;
         } else {
             C.node[k] = 0;
             C.lab[k] = 0;
-            C.dend[k] = 2;  // never a segment end
-            C.fb[k] = 1;    // never a tree column
+            C.dend[k] = 2;
+            C.fb[k] = 1;
             C.fidx[k] = pad(min(c, row_max));
+            C.segor[k] = NOSEG;
         }
     }
 }
@@ -143,7 +155,7 @@ template <int W>
 __device__ __forceinline__ int count_ends(const Cols<W> &C) {
     int e = 0;
 #pragma unroll
-    for (int k = 0; k < W; k++) e += ((C.valid >> k) & 1u) && C.dend[k] == 1;
+    for (int k = 0; k < W; k++) e += ((C.valid >> k) & 1u) && C.segor[k] == 0;
     return e;
 }
 
@@ -152,38 +164,55 @@ __device__ __forceinline__ void set_keys(Cols<W> &C, int c0, int before) {
     int seg = before;
 #pragma unroll
     for (int k = 0; k < W; k++) {
-        C.key[k] = (c0 + k) + XTED_KEY_BIG * seg;
-        if (((C.valid >> k) & 1u) && C.dend[k] == 1) seg++;
+        const bool v = (C.valid >> k) & 1u;
+        C.key[k] = v ? (c0 + k) + XTED_KEY_BIG * seg : KEY_INVALID;
+        if (v && C.segor[k] == 0) seg++;
     }
 }
 
-// The per-row cell work shared by both executors: builds v = A + key for the
-// thread's columns and their local suffix minima; returns the thread's
-// minimum. Branch-free: the ring and stack reads for every column are issued
-// first, then each column is a handful of selects and one link of the
-// running-minimum chain.
+// Row step, forest rows (row i off its table's right path: the common case).
+// Every cell is a forest cell: a = Dtree + far value, far from the stack top
+// (or the table's border row for a column on its segment's right path).
+// Returns the thread's suffix minimum; loc[k] = minimum over its columns >= k.
 template <int W>
-__device__ __forceinline__ int row_cells(const Cols<W> &C, const int (&prev)[W], const int32_t *slot,
-                                         int dnext, bool trow, int rl, int bord, int rowfar,
-                                         const int32_t *top, int c0, int (&loc)[W]) {
+__device__ __forceinline__ int row_forest(const Cols<W> &C, const int (&prev)[W], const int32_t *slot,
+                                          const int32_t *top, int bord1, int rowfar, int (&loc)[W]) {
     int cur[W], farv[W];
 #pragma unroll
     for (int k = 0; k < W; k++) {
-        cur[k] = slot[pad(c0 + k)];
+        cur[k] = slot[k];
         farv[k] = top[C.fidx[k]];
     }
     int run = XTED_INF;
 #pragma unroll
     for (int k = W - 1; k >= 0; k--) {
-        const int up = prev[k];
-        const bool segend = C.dend[k] == 1;
-        const int diag = segend ? bord - 1 : ((k == W - 1) ? dnext : prev[k + 1]);
-        const bool tcol = C.fb[k] == 0;
-        const int farsel = trow ? C.fb[k] : (tcol ? rowfar : farv[k]);
-        const int a = (trow && tcol) ? diag + (rl != C.lab[k] ? 1 : 0) : cur[k] + farsel;
-        int A = min(a, up + 1);
-        A = segend ? min(A, bord + 1) : A;
-        run = min(run, ((C.valid >> k) & 1u) ? A + C.key[k] : XTED_INF);
+        const int far = ((C.tcol >> k) & 1u) ? rowfar : farv[k];
+        int A = __viaddmin_s32(prev[k], 1, cur[k] + far);  // min(up + 1, forest term)
+        A = min(A, bord1 | C.segor[k]);                     // a segment's last column meets the border
+        run = __viaddmin_s32(A, C.key[k], run);             // min(A + key, run)
+        loc[k] = run;
+    }
+    return run;
+}
+
+// Row step, tree-path rows (row i on its table's right path): tree cells on
+// the segments' right paths, forest cells elsewhere with the far value of the
+// table's bottom border.
+template <int W>
+__device__ __forceinline__ int row_tree(const Cols<W> &C, const int (&prev)[W], const int32_t *slot, int dnext,
+                                        int rl, int bord, int (&loc)[W]) {
+    int cur[W];
+#pragma unroll
+    for (int k = 0; k < W; k++) cur[k] = slot[k];
+    const int bord1 = bord + 1;
+    int run = XTED_INF;
+#pragma unroll
+    for (int k = W - 1; k >= 0; k--) {
+        const int diag = C.segor[k] == 0 ? bord - 1 : ((k == W - 1) ? dnext : prev[k + 1]);
+        const int a = ((C.tcol >> k) & 1u) ? diag + (rl != C.lab[k] ? 1 : 0) : cur[k] + C.fb[k];
+        int A = __viaddmin_s32(prev[k], 1, a);
+        A = min(A, bord1 | C.segor[k]);
+        run = __viaddmin_s32(A, C.key[k], run);
         loc[k] = run;
     }
     return run;
@@ -272,6 +301,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     int32_t *dt_out = P.dt + pr.dt_off;
     const int2 *rows = P.rowinfo + pr.row_base;
     const int stride = XTED_NARROW_MAX;
+    const int pbase = pad(c0);  // pad(c0 + k) == pbase + k for k < W (W divides 32)
     constexpr int PF = XTED_PREFETCH;
     // a table at keyroot depth d nests at most d stack rows (nested keyroots have
     // strictly smaller depths), so only deep runs need the global copy of the stack
@@ -308,39 +338,44 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
-            const int rowfar = imax - ro - 1;
-            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
-            const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
             int loc[W];
-            const int mine = row_cells<W>(C, prev, slot, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
+            int mine;
+            if (!trow) {
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
+                mine = row_forest<W>(C, prev, slot + pbase, top, bord + 1, imax - ro - 1, loc);
+            } else {
+                const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
+                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, loc);
+            }
             const int incl = warp_suffix_min(mine, lane);
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
             if (lane == 31) carry = XTED_INF;
-            int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
-            for (int k = 0; k < W; k++) {
-                const int d = min(loc[k], carry) - C.key[k];
-                prev[k] = d;
-                if (trow && C.fb[k] == 0 && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
+            for (int k = 0; k < W; k++) prev[k] = min(loc[k], carry) - C.key[k];
+            if (trow) {
+                int32_t *orow = dt_out + (int64_t)i * n;
+#pragma unroll
+                for (int k = 0; k < W; k++)
+                    if ((C.tcol >> k) & 1u) orow[C.node[k]] = prev[k];
             }
             // every lane has read this row's stack top (its values fed the scan above)
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * NARROW_ROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = src[k];
+                        if ((C.far >> k) & 1u) dst[k] = src[k];
                     lo = sp - 1;
                 }
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * NARROW_ROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = prev[k];
+                        if ((C.far >> k) & 1u) dst[k] = prev[k];
                     if (deep) {
                         int32_t *g = stk + sp * stride + c0;
 #pragma unroll
@@ -377,6 +412,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
     const int c0 = tid * W;
     const int stride = ch.width;
     const int width = ch.width;
+    const int pbase = pad(c0);  // pad(c0 + k) == pbase + k for k < W (W divides 32)
     constexpr int PF = XTED_PREFETCH;
     const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
     Cols<W> C;
@@ -431,12 +467,16 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
-            const int rowfar = imax - ro - 1;
-            const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
-            int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
-            if (lane == 31) dnext = S.first[warp + 1];
             int loc[W];
-            const int mine = row_cells<W>(C, prev, slot, dnext, trow, ri.x, bord, rowfar, top, c0, loc);
+            int mine;
+            if (!trow) {
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
+                mine = row_forest<W>(C, prev, slot + pbase, top, bord + 1, imax - ro - 1, loc);
+            } else {
+                int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
+                if (lane == 31) dnext = S.first[warp + 1];
+                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, loc);
+            }
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
             __syncthreads();
@@ -445,29 +485,30 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             for (int w = warp + 1; w < XTED_WARPS; w++) carry = min(carry, S.wtot[w]);
             int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
-            for (int k = 0; k < W; k++) {
-                const int d = min(loc[k], carry) - C.key[k];
-                prev[k] = d;
-                if (trow && C.fb[k] == 0 && ((C.valid >> k) & 1u)) orow[C.node[k]] = d;
+            for (int k = 0; k < W; k++) prev[k] = min(loc[k], carry) - C.key[k];
+            if (trow) {
+#pragma unroll
+                for (int k = 0; k < W; k++)
+                    if ((C.tcol >> k) & 1u) orow[C.node[k]] = prev[k];
             }
             if (lane == 0) S.first[warp] = prev[0];
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (int64_t)(sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * WIDE_ROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = src[k];
+                        if ((C.far >> k) & 1u) dst[k] = src[k];
                     lo = sp - 1;
                 }
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * WIDE_ROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[pad(c0 + k)] = prev[k];
+                        if ((C.far >> k) & 1u) dst[k] = prev[k];
                     if (deep) {
                         int32_t *g = stk + (int64_t)sp * stride + c0;
 #pragma unroll
@@ -711,6 +752,10 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
     int32_t *s_cache = s_dyn + RING_INTS;
     int32_t *s_cnode = s_cache + CACHE_INTS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // columns past a chunk's end read ring and stack cells nobody writes for
+    // that unit: start them at zero so those inert columns stay non-negative
+    for (int x = tid; x < RING_INTS + CACHE_INTS; x += XTED_CTA_THREADS) s_dyn[x] = 0;
+    __syncthreads();
     int32_t *scratch = P.scratch + (int64_t)blockIdx.x * P.scratch_per_cta;
     for (;;) {
         if (tid == 0) {
