@@ -250,6 +250,8 @@ def main():
     ap.add_argument("--plain-stride", type=int, default=16)
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--wait-timeout", type=float, default=20.0,
+                    help="bound of the DP kernel's idle waits, seconds (raise it under a profiler's replay)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
@@ -258,7 +260,7 @@ def main():
 
     import xted
     pairs, cfg = make_workload(args.workload, rank)
-    ctx = xted.Context(device=local)
+    ctx = xted.Context(device=local, wait_timeout_s=args.wait_timeout)
     npairs = len(pairs)
 
     # ---- device-resident throughput (value) ----
@@ -343,7 +345,7 @@ def main():
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
                      "kernel": "xted_dp_kernel", "bytes_per_cell": BYTES_PER_CELL},
         "cpu_baseline": cpu,
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 3 * args.steps,  # ready-queue init, DP, gather per step
         "clocks": clk.summary(),
         "tasks": st["tasks"], "units": st["units"], "grid": st["grid"], "host_plan_ms": round(plan_ms, 2),
     }
