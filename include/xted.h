@@ -39,6 +39,7 @@ extern "C" {
 #define XTED_ENODEV (-5)   /* no usable sm_100 device                     */
 #define XTED_ENOTFOUND (-6) /* unknown serving ticket                     */
 #define XTED_EAGAIN (-7)   /* serving queue full; retry later             */
+#define XTED_ETOOBIG (-8)  /* pair exceeds xted_distance_noalloc's arena   */
 
 /* Largest tree accepted (nodes). Bounds the int32 key arithmetic of the
  * row scan and keeps the per-pair distance table addressable. */
@@ -125,6 +126,25 @@ int xted_validate(const xted_tree *t);
  * n labels, n+1 offsets and n-1 children into caller buffers. */
 int xted_gen_tree(int32_t shape, int32_t n, uint64_t seed, int32_t label_kind, int32_t alphabet,
                   int32_t *labels, int32_t *child_off, int32_t *child_idx);
+
+/* ---- allocation-free single pair ----
+ *
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory when they need a distance: a process whose HBM is already handed to
+ * another allocator's pool, a checker running after an allocation failed, or
+ * a latency-bound caller that cannot take the device-wide synchronisation a
+ * cudaFree implies. The pair is computed in a fixed arena of
+ * XTED_NOALLOC_ARENA_BYTES that is part of the loaded library module; the
+ * call makes no device or pinned-host allocation and needs no context.
+ * Limit: with m and n the tree sizes, the inputs, their metadata
+ * (about 8(m + n) ints), the m x n tree-distance matrix and at least one
+ * (m + 1) x (n + 1) forest table must fit in the arena (a pair of two
+ * 1400-node trees fits); larger pairs return XTED_ETOOBIG. Synchronous. Every
+ * call on a device shares the one arena: calls that overlap on the GPU (two
+ * host threads at once) race, so serialise them. Same results and empty-tree
+ * rules as xted_distance. */
+#define XTED_NOALLOC_ARENA_BYTES (16 << 20)
+int xted_distance_noalloc(const xted_tree *a, const xted_tree *b, int32_t device, int32_t *out);
 
 /* ---- serving: a resident corpus and exact top-k queries ---- */
 

@@ -229,6 +229,7 @@ const char *xted_strerror(int code) {
         case XTED_ENODEV: return "no usable sm_100 CUDA device";
         case XTED_ENOTFOUND: return "unknown ticket";
         case XTED_EAGAIN: return "serving queue full";
+        case XTED_ETOOBIG: return "pair does not fit the fixed arena of xted_distance_noalloc";
         default: return "unknown error";
     }
 }

@@ -22,6 +22,8 @@ XTED_ECUDA = -4
 XTED_ENODEV = -5
 XTED_ENOTFOUND = -6
 XTED_EAGAIN = -7
+XTED_ETOOBIG = -8
+XTED_NOALLOC_ARENA_BYTES = 16 << 20
 XTED_MAX_NODES = 65535
 
 ORIENT_AUTO, ORIENT_RIGHT, ORIENT_LEFT = 0, 1, 2
@@ -89,6 +91,7 @@ def lib():
                                                  P(ctypes.c_uint64)]),
             "xted_query_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _i32p, _i32p, _i32p]),
             "xted_serve_drain": (ctypes.c_int, [ctypes.c_void_p]),
+            "xted_distance_noalloc": (ctypes.c_int, [P(CTree), P(CTree), ctypes.c_int32, _i32p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -136,6 +136,20 @@ def pair_cells(a: Tree, b: Tree, orientation: int = _lib.ORIENT_AUTO) -> Tuple[i
     return int(out[0]), int(out[1]), int(out[2])
 
 
+def distance_noalloc(a: Tree, b: Tree, device: int = 0) -> int:
+    """One pair through xted_distance_noalloc: computed in the library's fixed
+    device arena, with no device allocation and no context. For callers that
+    must not allocate device memory (memory held by another allocator's pool,
+    or after an allocation failed). Calls that overlap on the GPU race on the
+    shared arena; raises XtedError(XTED_ETOOBIG) for pairs that do not fit."""
+    keep: list = []
+    ta, tb = _lib.ctree(a, keep), _lib.ctree(b, keep)
+    out = ctypes.c_int32(0)
+    _lib.check(_lib.lib().xted_distance_noalloc(ctypes.byref(ta), ctypes.byref(tb), int(device),
+                                                ctypes.byref(out)), "xted_distance_noalloc")
+    return int(out.value)
+
+
 def validate(t: Tree) -> bool:
     keep: list = []
     c = _lib.ctree(t, keep)
