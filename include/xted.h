@@ -146,21 +146,45 @@ int xted_gen_tree(int32_t shape, int32_t n, uint64_t seed, int32_t label_kind, i
 #define XTED_NOALLOC_ARENA_BYTES (16 << 20)
 int xted_distance_noalloc(const xted_tree *a, const xted_tree *b, int32_t device, int32_t *out);
 
-/* ---- serving: a resident corpus and exact top-k queries ---- */
+/* ---- serving: a resident corpus and exact top-k queries ----
+ *
+ * No counterpart in the reference (its harness computes one pair). A
+ * corpus stays resident on the device with its keyroot metadata; each query
+ * is planned against every corpus tree and fed into the running persistent
+ * DP launch as soon as one of XTED_SERVE_SLOTS slots and enough device
+ * memory for its distance tables are free (continuous batching: queries
+ * overlap on the device, earlier queries take priority). A worker thread of
+ * the context drives the loop; these calls are thread-safe with respect to
+ * each other. Batch calls on the same context wait while a serving launch
+ * is running. */
+#define XTED_SERVE_SLOTS_MAX 16
+#define XTED_SERVE_MAX_QUERY 8192 /* nodes of one query tree */
 
-/* Uploads a corpus (replacing any previous one) and precomputes its
- * keyroot metadata on the device. */
+/* Uploads a corpus (replacing any previous one, after finishing its queries)
+ * and precomputes its keyroot metadata. */
 int xted_corpus_load(xted_ctx *ctx, const xted_tree *trees, int32_t ntrees);
 
-/* Queues a query for the k nearest corpus trees by TED. Returns at once. */
+/* Queues a query for the k nearest corpus trees by TED. Returns at once;
+ * XTED_EAGAIN when the queue is full, XTED_EINVAL for a malformed tree or
+ * one larger than XTED_SERVE_MAX_QUERY. */
 int xted_query_submit(xted_ctx *ctx, const xted_tree *q, int32_t k, uint64_t *ticket);
 
-/* Advances the serving loop and reports a query. *done = 1 when ids/dists
- * (k entries each, ascending distance, ties by corpus index) are final. */
+/* Reports a query. *done = 1 when ids/dists (k entries each, ascending
+ * distance, ties by lower corpus index; -1 past the corpus size) are final;
+ * the ticket is then released. A failed query returns its error code. */
 int xted_query_poll(xted_ctx *ctx, uint64_t ticket, int32_t *ids, int32_t *dists, int32_t *done);
 
-/* Blocks until every submitted query is finished. */
+/* As xted_query_poll, and on completion the time from submission to
+ * admission (queue_ms) and to completion (total_ms). Either may be NULL. */
+int xted_query_poll_timed(xted_ctx *ctx, uint64_t ticket, int32_t *ids, int32_t *dists, int32_t *done,
+                          double *queue_ms, double *total_ms);
+
+/* Blocks until every submitted query is finished; returns the first device
+ * error seen since the last drain, else 0. */
 int xted_serve_drain(xted_ctx *ctx);
+
+/* out4: persistent launches made, queries served, pairs served, cells. */
+int xted_serve_stats(xted_ctx *ctx, int64_t *out4);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,149 @@
+// emu_unit.h -- TEST INFRASTRUCTURE: one DP unit computed on the CPU exactly
+// as the kernels compute it (columns derived like load_cols, row scan with
+// segment keys, far-row stack with its shared-memory window), with checks of
+// the plan's invariants. Shared by the batch and serving planner emulations.
+#pragma once
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "../../x-ted_b200/csrc/plan_core.h"
+
+#define FAIL(...)                 \
+    do {                          \
+        std::printf(__VA_ARGS__); \
+        std::printf("\n");        \
+        std::exit(1);             \
+    } while (0)
+
+namespace emu {
+
+using namespace xted;
+
+struct Pools {
+    const int2 *node;
+    const int32_t *krd, *cumw;
+    const XRun *runs;
+    const XChunk *chunks;
+    int stack_rows;
+};
+
+inline int g_cache = 8;  // shared-memory window of the far-row stack (the kernels use 8)
+
+// Unit u of pair pr; the pair's m x n tree-distance table is dtv[pr.dt_off ...].
+inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vector<int32_t> &dtv, int narrow_width,
+                     bool wide_task) {
+    int32_t *dt = dtv.data() + pr.dt_off;
+    const XRun run = H.runs[(size_t)u.run];
+    const XChunk ch = H.chunks[(size_t)u.chunk];
+    if (!wide_task && ch.width > narrow_width) FAIL("narrow unit wider than the narrow limit");
+    if (wide_task && ch.width <= narrow_width) FAIL("wide unit narrower than the narrow limit");
+    const int W = ch.width, n = pr.n;
+    const int2 *cn = H.node + pr.col_base;
+    const int2 *rn = H.node + pr.row_base;
+    std::vector<int> node(W), lab(W), foff(W), dend(W), key(W);
+    std::vector<char> far(W);
+    int seg = 0, s = ch.k_lo;
+    int j0 = H.krd[(size_t)s], je = (cn[j0].y & XTED_ROW_ORL_MASK) + 1, j = j0;
+    if (H.cumw[(size_t)s] + W > H.cumw[(size_t)(ch.k_lo + ch.nseg - 1)] +
+                                    ((cn[H.krd[(size_t)(ch.k_lo + ch.nseg - 1)]].y & XTED_ROW_ORL_MASK) + 1 -
+                                     H.krd[(size_t)(ch.k_lo + ch.nseg - 1)]))
+        FAIL("chunk width exceeds its segments");
+    for (int c = 0; c < W; c++) {
+        if (j >= je) {
+            s++;
+            j0 = H.krd[(size_t)s];
+            je = (cn[j0].y & XTED_ROW_ORL_MASK) + 1;
+            j = j0;
+        }
+        node[c] = j;
+        lab[c] = cn[j].x;
+        foff[c] = (cn[j].y & XTED_ROW_ORL_MASK) + 1 - j;
+        dend[c] = je - j;
+        far[c] = j > j0 && (cn[j].y & XTED_ROW_PREVLEAF);
+        key[c] = c + XTED_KEY_BIG * seg;
+        if (dend[c] == 1) seg++;
+        j++;
+    }
+    if (seg != ch.nseg || s != ch.k_lo + ch.nseg - 1) FAIL("chunk segment count mismatch");
+    // global stack (written only when units can nest deeper than the window) and the window
+    const bool deep = run.depth > g_cache;  // the kernels' rule: depth-d tables nest <= d rows
+    std::vector<std::vector<int>> stk((size_t)H.stack_rows, std::vector<int>((size_t)W, -777));
+    std::vector<std::vector<int>> cache((size_t)g_cache, std::vector<int>((size_t)W, -777));
+    std::vector<int> prev(W), cur(W), loc(W);
+    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+        const int i0 = H.krd[(size_t)kr];
+        const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
+        for (int c = 0; c < W; c++) prev[c] = dend[c];
+        int sp = 0, lo = 0;
+        for (auto &row : cache) std::fill(row.begin(), row.end(), -777);
+        for (auto &row : stk) std::fill(row.begin(), row.end(), -777);
+        for (int i = imax - 1; i >= i0; i--) {
+            const int2 ri = rn[i];
+            const int ro = ri.y & XTED_ROW_ORL_MASK;
+            const bool trow = ro == imax - 1;
+            const int bord = imax - i, rowfar = imax - ro - 1;
+            int runmin = XTED_INF;
+            for (int c = W - 1; c >= 0; c--) {
+                const bool se = dend[c] == 1;
+                const int diag = se ? bord - 1 : prev[(size_t)c + 1];
+                const bool tcol = foff[c] == dend[c];
+                int a;
+                if (trow && tcol) {
+                    a = diag + (ri.x != lab[c]);
+                } else {
+                    int fv;
+                    if (trow) fv = dend[c] - foff[c];
+                    else if (tcol) fv = rowfar;
+                    else {
+                        if (sp < 1) FAIL("far-row stack underflow");
+                        if (sp - 1 < lo) FAIL("stack top outside the shared window");
+                        fv = cache[(size_t)((sp - 1) % g_cache)][(size_t)(c + foff[c])];
+                        if (fv == -777) FAIL("far value never pushed");
+                    }
+                    const int dv = dt[(size_t)i * n + node[c]];
+                    if (dv < 0) FAIL("tree distance (%d,%d) read before it was written", i, node[c]);
+                    a = dv + fv;
+                }
+                int Av = std::min(a, prev[c] + 1);
+                if (se) Av = std::min(Av, bord + 1);
+                runmin = std::min(runmin, Av + key[c]);
+                loc[c] = runmin;
+            }
+            for (int c = 0; c < W; c++) {
+                cur[c] = loc[c] - key[c];
+                if (trow && foff[c] == dend[c]) {
+                    int32_t &slot = dt[(size_t)i * n + node[c]];
+                    if (slot >= 0) FAIL("tree distance (%d,%d) written twice", i, node[c]);
+                    slot = cur[c];
+                }
+                prev[c] = cur[c];
+            }
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
+                sp--;
+                if (sp > 0 && sp - 1 < lo) {
+                    if (!deep) FAIL("window reload in a shallow unit");
+                    for (int c = 0; c < W; c++)
+                        if (far[c]) cache[(size_t)((sp - 1) % g_cache)][(size_t)c] = stk[(size_t)sp - 1][(size_t)c];
+                    lo = sp - 1;
+                }
+            }
+            if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
+                if (sp >= H.stack_rows) FAIL("far-row stack overflow (%d rows)", H.stack_rows);
+                for (int c = 0; c < W; c++)
+                    if (far[c]) {
+                        cache[(size_t)(sp % g_cache)][(size_t)c] = prev[c];
+                        if (deep) stk[(size_t)sp][(size_t)c] = prev[c];
+                    }
+                sp++;
+                if (sp > run.depth) FAIL("stack depth %d above the run's keyroot depth %d", sp, run.depth);
+                if (sp - lo > g_cache) lo = sp - g_cache;
+            }
+        }
+        if (sp != 0) FAIL("far-row stack not empty at table end (%d)", sp);
+    }
+}
+
+}  // namespace emu

@@ -18,17 +18,11 @@
 
 #include "../../include/xted.h"
 #include "../../x-ted_b200/csrc/plan_core.h"
+#include "emu_unit.h"
 
 extern "C" int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx, int n,
                            const int32_t *lb, const int32_t *boff, const int32_t *bidx);
 using namespace xted;
-
-#define FAIL(...)                 \
-    do {                          \
-        std::printf(__VA_ARGS__); \
-        std::printf("\n");        \
-        std::exit(1);             \
-    } while (0)
 
 struct HostPlan {
     std::vector<int32_t> raw, pair_trees;
@@ -156,123 +150,6 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     for (auto &E : H.lv) level_fill(C, E, H.units.data(), H.tasks.data());
 }
 
-// One unit, exactly as the kernels compute it (columns derived like load_cols).
-static int g_cache = 8;  // shared-memory window of the far-row stack (the kernels use 8)
-
-static void run_unit(const HostPlan &H, const DPair &q, const XUnit &u, std::vector<int32_t> &dtv,
-                     int narrow_width, bool wide_task) {
-    const DOTree &A = H.ot[2 * (size_t)q.ta + q.o], &B = H.ot[2 * (size_t)q.tb + q.o];
-    int32_t *dt = dtv.data() + q.dt_off;
-    const XRun run = H.runs[(size_t)u.run];
-    const XChunk ch = H.chunks[(size_t)u.chunk];
-    if (!wide_task && ch.width > narrow_width) FAIL("narrow unit wider than the narrow limit");
-    if (wide_task && ch.width <= narrow_width) FAIL("wide unit narrower than the narrow limit");
-    const int W = ch.width, n = B.n;
-    const int2 *cn = H.node.data() + B.node_base;
-    const int2 *rn = H.node.data() + A.node_base;
-    std::vector<int> node(W), lab(W), foff(W), dend(W), key(W);
-    std::vector<char> far(W);
-    int seg = 0, s = ch.k_lo;
-    int j0 = H.krd[(size_t)s], je = (cn[j0].y & XTED_ROW_ORL_MASK) + 1, j = j0;
-    if (H.cumw[(size_t)s] + W > H.cumw[(size_t)(ch.k_lo + ch.nseg - 1)] +
-                                    ((cn[H.krd[(size_t)(ch.k_lo + ch.nseg - 1)]].y & XTED_ROW_ORL_MASK) + 1 -
-                                     H.krd[(size_t)(ch.k_lo + ch.nseg - 1)]))
-        FAIL("chunk width exceeds its segments");
-    for (int c = 0; c < W; c++) {
-        if (j >= je) {
-            s++;
-            j0 = H.krd[(size_t)s];
-            je = (cn[j0].y & XTED_ROW_ORL_MASK) + 1;
-            j = j0;
-        }
-        node[c] = j;
-        lab[c] = cn[j].x;
-        foff[c] = (cn[j].y & XTED_ROW_ORL_MASK) + 1 - j;
-        dend[c] = je - j;
-        far[c] = j > j0 && (cn[j].y & XTED_ROW_PREVLEAF);
-        key[c] = c + XTED_KEY_BIG * seg;
-        if (dend[c] == 1) seg++;
-        j++;
-    }
-    if (seg != ch.nseg || s != ch.k_lo + ch.nseg - 1) FAIL("chunk segment count mismatch");
-    // global stack (written only when units can nest deeper than the window) and the window
-    const bool deep = run.depth > g_cache;  // the kernels' rule: depth-d tables nest <= d rows
-    std::vector<std::vector<int>> stk((size_t)H.stack_rows, std::vector<int>((size_t)W, -777));
-    std::vector<std::vector<int>> cache((size_t)g_cache, std::vector<int>((size_t)W, -777));
-    std::vector<int> prev(W), cur(W), loc(W);
-    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
-        const int i0 = H.krd[(size_t)kr];
-        const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
-        for (int c = 0; c < W; c++) prev[c] = dend[c];
-        int sp = 0, lo = 0;
-        for (auto &row : cache) std::fill(row.begin(), row.end(), -777);
-        for (auto &row : stk) std::fill(row.begin(), row.end(), -777);
-        for (int i = imax - 1; i >= i0; i--) {
-            const int2 ri = rn[i];
-            const int ro = ri.y & XTED_ROW_ORL_MASK;
-            const bool trow = ro == imax - 1;
-            const int bord = imax - i, rowfar = imax - ro - 1;
-            int runmin = XTED_INF;
-            for (int c = W - 1; c >= 0; c--) {
-                const bool se = dend[c] == 1;
-                const int diag = se ? bord - 1 : prev[(size_t)c + 1];
-                const bool tcol = foff[c] == dend[c];
-                int a;
-                if (trow && tcol) {
-                    a = diag + (ri.x != lab[c]);
-                } else {
-                    int fv;
-                    if (trow) fv = dend[c] - foff[c];
-                    else if (tcol) fv = rowfar;
-                    else {
-                        if (sp < 1) FAIL("far-row stack underflow");
-                        if (sp - 1 < lo) FAIL("stack top outside the shared window");
-                        fv = cache[(size_t)((sp - 1) % g_cache)][(size_t)(c + foff[c])];
-                        if (fv == -777) FAIL("far value never pushed");
-                    }
-                    const int dv = dt[(size_t)i * n + node[c]];
-                    if (dv < 0) FAIL("tree distance (%d,%d) read before it was written", i, node[c]);
-                    a = dv + fv;
-                }
-                int Av = std::min(a, prev[c] + 1);
-                if (se) Av = std::min(Av, bord + 1);
-                runmin = std::min(runmin, Av + key[c]);
-                loc[c] = runmin;
-            }
-            for (int c = 0; c < W; c++) {
-                cur[c] = loc[c] - key[c];
-                if (trow && foff[c] == dend[c]) {
-                    int32_t &slot = dt[(size_t)i * n + node[c]];
-                    if (slot >= 0) FAIL("tree distance (%d,%d) written twice", i, node[c]);
-                    slot = cur[c];
-                }
-                prev[c] = cur[c];
-            }
-            if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
-                sp--;
-                if (sp > 0 && sp - 1 < lo) {
-                    if (!deep) FAIL("window reload in a shallow unit");
-                    for (int c = 0; c < W; c++)
-                        if (far[c]) cache[(size_t)((sp - 1) % g_cache)][(size_t)c] = stk[(size_t)sp - 1][(size_t)c];
-                    lo = sp - 1;
-                }
-            }
-            if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
-                if (sp >= H.stack_rows) FAIL("far-row stack overflow (%d rows)", H.stack_rows);
-                for (int c = 0; c < W; c++)
-                    if (far[c]) {
-                        cache[(size_t)(sp % g_cache)][(size_t)c] = prev[c];
-                        if (deep) stk[(size_t)sp][(size_t)c] = prev[c];
-                    }
-                sp++;
-                if (sp > run.depth) FAIL("stack depth %d above the run's keyroot depth %d", sp, run.depth);
-                if (sp - lo > g_cache) lo = sp - g_cache;
-            }
-        }
-        if (sp != 0) FAIL("far-row stack not empty at table end (%d)", sp);
-    }
-}
-
 static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int32_t> &lab,
                 std::vector<int32_t> &off, std::vector<int32_t> &idx) {
     lab.clear();
@@ -309,7 +186,7 @@ static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int
 
 int main(int argc, char **argv) {
     const int iters = argc > 1 ? std::atoi(argv[1]) : 200;
-    if (argc > 4) g_cache = std::atoi(argv[4]);
+    if (argc > 4) emu::g_cache = std::atoi(argv[4]);
     const int maxn = argc > 2 ? std::atoi(argv[2]) : 300;
     std::mt19937_64 g(argc > 3 ? (uint64_t)std::atoll(argv[3]) : 12345);
     int64_t pairs_checked = 0;
@@ -357,9 +234,18 @@ int main(int argc, char **argv) {
                 const int nu = (int)(t.kind_n & 0xffff);
                 const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
                 if (nu < 1 || nu > XTED_TASK_UNITS || (wide && nu != 1)) FAIL("bad unit count %d", nu);
+                const DPair &q = H.pairs[(size_t)t.pair];
+                XPair x;
+                x.dt_off = q.dt_off;
+                x.m = H.trees[(size_t)q.ta].n;
+                x.n = H.trees[(size_t)q.tb].n;
+                x.row_base = H.ot[2 * (size_t)q.ta + q.o].node_base;
+                x.col_base = H.ot[2 * (size_t)q.tb + q.o].node_base;
+                const emu::Pools EP{H.node.data(), H.krd.data(), H.cumw.data(), H.runs.data(), H.chunks.data(),
+                                    H.stack_rows};
                 for (int u = 0; u < nu; u++) {
                     unit_seen[(size_t)(t.unit_lo + u)]++;
-                    run_unit(H, H.pairs[(size_t)t.pair], H.units[(size_t)(t.unit_lo + u)], dt, nw, wide);
+                    emu::run_unit(EP, x, H.units[(size_t)(t.unit_lo + u)], dt, nw, wide);
                 }
             }
             level_done[(size_t)E.pair] = E.level;

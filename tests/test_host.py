@@ -124,3 +124,20 @@ def test_planner_emulation_matches_oracle(tmp_path):
         r = subprocess.run([str(exe), "100", "250", "99", window], capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout + r.stderr
         assert r.stdout.startswith("ok")
+
+
+def test_serving_planner_emulation_matches_oracle(tmp_path):
+    """Runs the serving planner (serve_plan.h: corpus pools, per-slot query
+    plans, offset fix-ups) and an interleaved execution of several queries'
+    pairs with the kernels' row math (tests/cpp/serve_emu.cpp), checking
+    every index against its pool and every distance against the oracle."""
+    obj = tmp_path / "xo.o"
+    exe = tmp_path / "serve_emu"
+    subprocess.run(["gcc", "-O2", "-c", os.path.join(REPO, "oracle", "xted_oracle.c"), "-o", str(obj)], check=True)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I/usr/local/cuda/include",
+                    os.path.join(REPO, "tests", "cpp", "serve_emu.cpp"), str(obj), "-o", str(exe), "-lpthread"],
+                   check=True)
+    for seed in ("7", "8", "9"):
+        r = subprocess.run([str(exe), "12", "150", seed], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert r.stdout.startswith("ok")

@@ -147,7 +147,8 @@ int ctx_run(xted_ctx *c, int32_t *out) {
     if (cudaMemsetAsync(cnt, 0, 8 * sizeof(int32_t), c->stream) != cudaSuccess ||
         (K.ntasks > 0 &&
          (cudaMemsetAsync(K.entry_state, 0, 2 * ne * sizeof(int32_t), c->stream) != cudaSuccess ||
-          cudaMemsetAsync(K.rq, 0xff, (size_t)XTED_BUCKETS * ne * sizeof(int32_t), c->stream) != cudaSuccess ||
+          cudaMemsetAsync(K.rq, 0xff, ((size_t)XTED_BUCKETS << K.rq_log2) * sizeof(unsigned long long),
+                          c->stream) != cudaSuccess ||
           cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_BUCKETS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
           launch_rq_init(K, c->stream) != cudaSuccess)))
         return XTED_ECUDA;

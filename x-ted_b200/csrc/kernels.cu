@@ -653,55 +653,81 @@ __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUn
 // non-empty bucket. An entry is only published after every task of the
 // previous level of its pair has finished, so claimed tasks never wait.
 // ---------------------------------------------------------------------------
-__device__ void rq_publish(const XKernelParams &P, int e) {
+// Publishes entry e (or, past levels without tasks, the first later level
+// that has some) into its bucket's ring. Returns false when the pair has no
+// level left, i.e. the pair is finished.
+__device__ bool rq_publish(const XKernelParams &P, int e) {
     while (e >= 0) {
         const XEntry X = P.entries[e];
         if (X.ntasks > 0) {
-            const int slot = atomicAdd(&P.rq_ctl[2 * X.bucket + 1], 1);
-            ((volatile int32_t *)P.rq)[(int64_t)X.bucket * P.nentries + slot] = e;
-            return;
+            const unsigned pos = (unsigned)atomicAdd(&P.rq_ctl[2 * X.bucket + 1], 1);
+            const unsigned head = *(volatile unsigned *)&P.rq_ctl[2 * X.bucket];
+            if (pos - head >= (1u << P.rq_log2)) {  // ring full: never overwrite a live slot
+                set_error(P, XTED_ENOMEM, 5, X.bucket, (int)pos);
+                return true;
+            }
+            const unsigned long long v = ((unsigned long long)pos << 32) | (unsigned)e;
+            ((volatile unsigned long long *)P.rq)[((int64_t)X.bucket << P.rq_log2) + (pos & ((1u << P.rq_log2) - 1))] = v;
+            return true;
         }
         e = X.next;  // a level without tasks: go on to the next one
     }
+    return false;
 }
 
-// Returns a task index (and its entry), or -1 when all tasks are done or on
-// error. Blocks probe a bucket's live window [head, tail) starting at a
+// Entry held by ring position pos of bucket b, or -1 if that position is not
+// written yet.
+__device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned pos) {
+    const unsigned long long v =
+        ((volatile const unsigned long long *)P.rq)[((int64_t)b << P.rq_log2) + (pos & ((1u << P.rq_log2) - 1))];
+    return (unsigned)(v >> 32) == pos ? (int)(unsigned)v : -1;
+}
+
+#define CLAIM_EXIT (-1)
+#define CLAIM_RECORD (-2)
+
+// Returns a task index (and its entry), CLAIM_EXIT when the launch is over
+// (all tasks done, an error, or in a serving session the stop word or an
+// idle spell), or CLAIM_RECORD with *entry = a mailbox record this block
+// claimed and must publish. Buckets are probed from the most urgent: bucket
+// 15 down in a batch, the oldest query's bucket onwards in a serving session.
+// Blocks probe a bucket's live window [head, tail) starting at a
 // block-dependent position, so they spread over many entries instead of all
 // contending for the head entry, and test an entry with a plain load before
 // claiming from it; whoever sees exhausted entries at the head moves it on.
 // Idle polling is bounded by time and by iterations.
 __device__ int claim_task(const XKernelParams &P, int *entry) {
     volatile int32_t *ctl = P.rq_ctl;
-    volatile int32_t *rq = P.rq;
     volatile int32_t *state = P.entry_state;
+    volatile int32_t *mbox = P.mbox;
     unsigned ns = 32;
     uint64_t t0 = 0;
     unsigned salt = blockIdx.x * 2654435761u;
     for (long it = 0; it < (1L << 28); it++) {
-        if (*(volatile int32_t *)P.error != 0) return -1;
-        for (int b = XTED_BUCKETS - 1; b >= 0; b--) {
-            const int32_t *slots = P.rq + (int64_t)b * P.nentries;
-            int h = ctl[2 * b];
+        if (*(volatile int32_t *)P.error != 0) return CLAIM_EXIT;
+        const int top = P.serve ? mbox[XTED_MBOX_TOP] : XTED_BUCKETS - 1;
+        for (int i = 0; i < XTED_BUCKETS; i++) {
+            const int b = (top - i) & (XTED_BUCKETS - 1);
+            unsigned h = (unsigned)ctl[2 * b];
             // move the head over exhausted entries
             for (int guard = 0; guard < 64; guard++) {
-                if (h >= ctl[2 * b + 1]) break;
-                const int e = rq[(int64_t)b * P.nentries + h];
+                if ((int)((unsigned)ctl[2 * b + 1] - h) <= 0) break;
+                const int e = rq_entry(P, b, h);
                 if (e < 0 || state[2 * e] < P.entries[e].ntasks) break;
-                atomicCAS((int32_t *)&ctl[2 * b], h, h + 1);
-                h = ctl[2 * b];
+                atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));
+                h = (unsigned)ctl[2 * b];
             }
-            const int tl = ctl[2 * b + 1];
-            const int live = tl - h;
+            const unsigned tl = (unsigned)ctl[2 * b + 1];
+            const int live = (int)(tl - h);
             if (live <= 0) continue;
             salt = salt * 1664525u + 1013904223u;
             const int start = (int)(salt % (unsigned)live);
             const int probes = live < 32 ? live : 32;
             for (int j = 0; j < probes; j++) {
-                int pos = h + start + j;
-                if (pos >= tl) pos -= live;
-                const int e = ((volatile const int32_t *)slots)[pos];
-                if (e < 0) continue;  // slot reserved but not yet written
+                int off = start + j;
+                if (off >= live) off -= live;
+                const int e = rq_entry(P, b, h + (unsigned)off);
+                if (e < 0) continue;  // position reserved but not yet written
                 const XEntry X = P.entries[e];
                 if (state[2 * e] >= X.ntasks) continue;
                 const int k = atomicAdd(&P.entry_state[2 * e], 1);
@@ -712,31 +738,79 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
                 }
             }
         }
-        if (ld_acquire(P.done_total) >= P.ntasks) return -1;
+        if (P.serve) {
+            int cons = mbox[XTED_MBOX_CONSUMED];
+            while (cons < mbox[XTED_MBOX_POSTED]) {
+                if (atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons + 1) == cons) {
+                    __threadfence();  // acquire: the record and its query's plan are visible from here on
+                    *entry = cons;
+                    return CLAIM_RECORD;
+                }
+                cons = mbox[XTED_MBOX_CONSUMED];
+            }
+            if (mbox[XTED_MBOX_STOP] != 0) return CLAIM_EXIT;
+        } else if (ld_acquire(P.done_total) >= P.ntasks) {
+            return CLAIM_EXIT;
+        }
         const uint64_t now = global_ns();
         if (t0 == 0) {
             t0 = now;
+        } else if (P.serve) {
+            if (now - t0 > P.idle_exit_ns) return CLAIM_EXIT;  // idle: the host relaunches on new work
         } else if (now - t0 > P.timeout_ns) {
             set_error(P, XTED_ETIMEOUT, 0, 0, 0);
-            return -1;
+            return CLAIM_EXIT;
         }
         __nanosleep(ns);
         if (ns < 1024) ns <<= 1;
     }
     set_error(P, XTED_ETIMEOUT, 1, 0, 0);
-    return -1;
+    return CLAIM_EXIT;
+}
+
+// A serving pair is finished: its distance goes to the host-visible result
+// array, and the last pair of a query raises the slot's flag to the query's
+// generation (the host polls it).
+__device__ void finish_served_pair(const XKernelParams &P, int pair) {
+    const int d = __ldcg(P.dt + __ldcg(&P.pairs[pair].dt_off));
+    ((volatile int32_t *)P.results)[pair] = d;
+    __threadfence_system();
+    const int s = pair / P.serve_pairs;
+    const int n = atomicAdd(&P.slot_done[s], 1) + 1;
+    if (n == __ldcg(&P.slot_need[s])) {
+        P.slot_done[s] = 0;
+        __threadfence_system();
+        ((volatile int32_t *)P.flags)[s] = __ldcg(&P.slot_gen[s]);
+    }
 }
 
 // After a task (all its writes fenced and the block synchronised).
-__device__ void complete_task(const XKernelParams &P, int e) {
+__device__ void complete_task(const XKernelParams &P, int e, int pair) {
     const XEntry X = P.entries[e];
     const int done = atomicAdd(&P.entry_state[2 * e + 1], 1) + 1;
     if (done == X.ntasks) {
         __threadfence();  // acquire the level's other tasks, release to the next level's claimers
-        rq_publish(P, X.next);
+        if (!rq_publish(P, X.next) && P.serve) finish_served_pair(P, pair);
     }
     __threadfence();
     atomicAdd(P.done_total, 1);
+}
+
+// A block publishes level 0 of every pair of mailbox record r.
+__device__ void publish_record(const XKernelParams &P, int r, int *s_rec) {
+    if (threadIdx.x == 0) {
+        const volatile int32_t *rec = P.mbox + XTED_MBOX_REC + 4 * (r & (XTED_SERVE_RECS - 1));
+        s_rec[0] = rec[1];
+        s_rec[1] = rec[2];
+    }
+    __syncthreads();
+    const int lo = s_rec[0], n = s_rec[1];
+    __threadfence();
+    for (int p = lo + (int)threadIdx.x; p < lo + n; p += XTED_CTA_THREADS) {
+        const int e = __ldcg(&P.first[p]);
+        if (e >= 0) rq_publish(P, e);
+    }
+    __syncthreads();
 }
 
 __global__ void xted_rq_init_kernel(XKernelParams P) {
@@ -745,7 +819,7 @@ __global__ void xted_rq_init_kernel(XKernelParams P) {
 }
 
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
-    __shared__ int s_task, s_entry, s_next;
+    __shared__ int s_task, s_entry, s_next, s_rec[2];
     __shared__ WideShared S;
     extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache | column nodes (DP_SMEM_BYTES)
     int32_t *s_ring = s_dyn;
@@ -768,6 +842,10 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         }
         __syncthreads();
         const int t = s_task;
+        if (t == CLAIM_RECORD) {
+            publish_record(P, s_entry, s_rec);
+            continue;
+        }
         if (t < 0) break;
         const XTask T = P.tasks[t];
         const XPair pr = P.pairs[T.pair];
@@ -792,7 +870,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         __threadfence();
         __syncthreads();
         if (tid == 0) {
-            complete_task(P, s_entry);
+            complete_task(P, s_entry, T.pair);
             if (P.trace) {  // info: wide(1) | units(7) | sm(8) | widest chunk(16) | cells(32)
                 unsigned sm;
                 asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));

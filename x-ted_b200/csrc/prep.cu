@@ -371,16 +371,19 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     const int64_t ntasks = nent > 0 ? hs->tasks : 0, nunits = nent > 0 ? hs->units : 0;
     if (ntasks > INT32_MAX / 2 || nunits > INT32_MAX / 2) return XTED_ENOMEM;
     // ---- buffer C: units, tasks and the ready queue's state ----
-    const size_t rq_ints = (size_t)XTED_BUCKETS * E1;
+    int rq_log2 = 0;
+    while (((int64_t)1 << rq_log2) < (int64_t)E1) rq_log2++;
+    const size_t rq_slots = (size_t)XTED_BUCKETS << rq_log2;
     rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
-                                         4 * (2 * E1 + rq_ints + (size_t)npairs + 2 * XTED_BUCKETS + 8) + 8 * 256);
+                                         8 * rq_slots + 4 * (2 * E1 + (size_t)npairs + 2 * XTED_BUCKETS + 8) +
+                                         8 * 256);
     if (rc) return rc;
     Carver cw{(char *)c->work.p};
     XUnit *d_units_out = cw.take<XUnit>((size_t)nunits);
     XTask *d_tasks_out = cw.take<XTask>((size_t)ntasks);
     int32_t *d_first = cw.take<int32_t>((size_t)npairs);
     int32_t *d_state = cw.take<int32_t>(2 * E1);  // claimed, done per entry
-    int32_t *d_rq = cw.take<int32_t>(rq_ints);
+    unsigned long long *d_rq = cw.take<unsigned long long>(rq_slots);
     int32_t *d_ctl = cw.take<int32_t>(2 * XTED_BUCKETS + 8);  // heads/tails, then the done counter
     if (nent > 0) k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out);
     k_pair_finalize<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_xpairs,
@@ -403,6 +406,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.npairs = npairs;
     K.entry_state = d_state;
     K.rq = d_rq;
+    K.rq_log2 = rq_log2;
     K.rq_ctl = d_ctl;
     K.done_total = d_ctl + 2 * XTED_BUCKETS;
     c->d_trivial = d_trivial;

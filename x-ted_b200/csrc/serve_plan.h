@@ -1,0 +1,240 @@
+// serve_plan.h -- host-side planning of serving queries against a resident
+// corpus (no CUDA runtime calls; the CPU emulation test includes it too).
+//
+// Pool layout: the corpus trees first (planned once, both orientations),
+// then one fixed region per query slot sized for XTED_SERVE_MAX_QUERY nodes.
+// A query is planned into its slot's region with the batch planner's own
+// functions (plan_core.h): every (corpus tree, query) pair, the corpus tree
+// as the row tree, so the far-row stack depth of every pair is bounded by a
+// corpus property known at load time.
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/xted.h"
+#include "plan_core.h"
+
+namespace xted {
+
+struct ServePools {
+    int T = 0, S = 0, Qmax = 0;
+    int64_t N = 0, R = 0;  // corpus nodes and raw ints
+    std::vector<int32_t> raw;
+    std::vector<DTree> trees;  // T corpus trees, then S slot trees
+    std::vector<int32_t> size, depth, parent, krd, cumw, opar, okd, oka;
+    std::vector<int2> node;
+    std::vector<XRun> runs;
+    std::vector<XChunk> chunks;
+    std::vector<DDepth> depths;
+    std::vector<DOTree> otrees;
+    PlanPools P{};
+    int32_t stack_rows = 1;  // far-row stack rows any pair needs (corpus rows)
+};
+
+// A planned query. Offsets are relative (pairs from 0, entries, units and
+// tasks from 0, tables from 0) until serve_fixup moves them to the slot's
+// device ranges.
+struct QPlan {
+    std::vector<XPair> pairs;     // [T]
+    std::vector<int32_t> first;   // [T] level-0 entry, -1 for an empty-tree pair
+    std::vector<int32_t> trivial; // [T] distance of an empty-tree pair, else -1
+    std::vector<XEntry> entries;
+    std::vector<XUnit> units;
+    std::vector<XTask> tasks;
+    int64_t dt_elems = 0, cells = 0;
+    int32_t need = 0;             // pairs the device computes
+};
+
+// Lays out the pools and plans the corpus. The trees must be valid.
+inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, int Qmax, int run_rows,
+                              int narrow_width) {
+    s.T = T;
+    s.S = S;
+    s.Qmax = Qmax;
+    int64_t N = 0, R = 0;
+    for (int t = 0; t < T; t++) {
+        N += tr[t].n;
+        R += 3 * (int64_t)tr[t].n + 1;
+    }
+    s.N = N;
+    s.R = R;
+    const int64_t Nall = N + (int64_t)S * Qmax;
+    s.raw.assign((size_t)(R + (int64_t)S * (3 * Qmax + 1)), 0);
+    s.trees.resize((size_t)(T + S));
+    int64_t rpos = 0, nb = 0;
+    for (int t = 0; t < T; t++) {
+        DTree &d = s.trees[(size_t)t];
+        const int n = tr[t].n;
+        d.n = n;
+        d.raw = (int32_t)rpos;
+        d.nbase = (int32_t)nb;
+        d.t = t;
+        d.S[0] = d.S[1] = 0;
+        if (n > 0) {
+            std::memcpy(&s.raw[(size_t)rpos], tr[t].labels, 4 * (size_t)n);
+            std::memcpy(&s.raw[(size_t)rpos + n], tr[t].child_off, 4 * ((size_t)n + 1));
+            if (n > 1) std::memcpy(&s.raw[(size_t)rpos + 2 * n + 1], tr[t].child_idx, 4 * ((size_t)n - 1));
+        }
+        rpos += 3 * (int64_t)n + 1;
+        nb += n;
+    }
+    for (int i = 0; i < S; i++) {
+        DTree &d = s.trees[(size_t)(T + i)];
+        d.n = 0;
+        d.raw = (int32_t)(R + (int64_t)i * (3 * Qmax + 1));
+        d.nbase = (int32_t)(N + (int64_t)i * Qmax);
+        d.t = T + i;
+        d.S[0] = d.S[1] = 0;
+    }
+    const size_t n1 = (size_t)std::max<int64_t>(Nall, 1), n2 = 2 * n1;
+    s.size.assign(n1, 0);
+    s.depth.assign(n1, 0);
+    s.parent.assign(n1, 0);
+    s.node.assign(n2, int2{0, 0});
+    s.krd.assign(n2, 0);
+    s.cumw.assign(n2, 0);
+    s.opar.assign(n2, 0);
+    s.okd.assign(n2, 0);
+    s.oka.assign(n2, 0);
+    s.runs.assign(n2, XRun{0, 0, 0, 0});
+    s.chunks.assign(n2, XChunk{0, 0, 0, 0});
+    s.depths.assign(2 * (n1 + (size_t)(T + S)), DDepth{});
+    s.otrees.assign(2 * (size_t)(T + S), DOTree{});
+    PlanPools &P = s.P;
+    P.raw = s.raw.data();
+    P.trees = s.trees.data();
+    P.ntrees = T + S;
+    P.size = s.size.data();
+    P.depth = s.depth.data();
+    P.parent = s.parent.data();
+    P.node = s.node.data();
+    P.krd = s.krd.data();
+    P.cumw = s.cumw.data();
+    P.runs = s.runs.data();
+    P.chunks = s.chunks.data();
+    P.opar = s.opar.data();
+    P.okd = s.okd.data();
+    P.oka = s.oka.data();
+    P.depths = s.depths.data();
+    P.otrees = s.otrees.data();
+    P.run_rows = run_rows;
+    P.narrow_width = narrow_width;
+    s.stack_rows = 1;
+    for (int t = 0; t < T; t++) {
+        tree_basic(P, t, s.trees.data());
+        orient_tree(P, 2 * t);
+        orient_tree(P, 2 * t + 1);
+        for (int o = 0; o < 2; o++) s.stack_rows = std::max(s.stack_rows, s.otrees[2 * (size_t)t + o].maxka + 1);
+    }
+}
+
+// Plans query (lab, off, idx, n <= Qmax, valid) in slot `slot`: the tree into
+// the slot's region, then every (corpus tree, query) pair as the batch
+// planner does (k_pair_setup ... k_level_fill in prep.cu).
+inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const int32_t *off, const int32_t *idx,
+                             int n, int orientation, int narrow_width, QPlan &out) {
+    const int T = s.T, tq = T + slot;
+    DTree &Q = s.trees[(size_t)tq];
+    Q.n = n;
+    int32_t *r = s.raw.data() + Q.raw;
+    if (n > 0) {
+        std::memcpy(r, lab, 4 * (size_t)n);
+        std::memcpy(r + n, off, 4 * ((size_t)n + 1));
+        if (n > 1) std::memcpy(r + 2 * n + 1, idx, 4 * ((size_t)n - 1));
+    } else {
+        r[0] = 0;
+    }
+    tree_basic(s.P, tq, s.trees.data());
+    orient_tree(s.P, 2 * tq);
+    orient_tree(s.P, 2 * tq + 1);
+
+    out = QPlan{};
+    std::vector<DPair> dp((size_t)T);
+    out.pairs.resize((size_t)T);
+    out.first.assign((size_t)T, -1);
+    out.trivial.assign((size_t)T, -1);
+    std::vector<DLevel> lv;
+    int64_t dt = 0;
+    for (int t = 0; t < T; t++) {
+        const int32_t pt[2] = {t, tq};
+        pair_setup(s.trees.data(), s.otrees.data(), pt, orientation, 0, &dp[(size_t)t]);
+        DPair &d = dp[(size_t)t];
+        XPair &x = out.pairs[(size_t)t];
+        std::memset(&x, 0, sizeof(x));
+        if (d.trivial >= 0) {
+            out.trivial[(size_t)t] = d.trivial;
+            continue;
+        }
+        x.dt_off = dt;
+        x.m = s.trees[(size_t)t].n;
+        x.n = n;
+        x.row_base = s.otrees[2 * (size_t)t + d.o].node_base;
+        x.col_base = s.otrees[2 * (size_t)tq + d.o].node_base;
+        dt += (int64_t)x.m * x.n;
+        d.lvl_base = (int32_t)lv.size();
+        out.first[(size_t)t] = d.lvl_base;
+        for (int l = 0; l < d.L; l++) {
+            DLevel E{};
+            E.pair = t;
+            E.level = l;
+            lv.push_back(E);
+        }
+        out.cells += d.cells;
+        out.need++;
+    }
+    out.dt_elems = dt;
+    LevelCtx C;
+    C.ot = s.otrees.data();
+    C.depths = s.depths.data();
+    C.runs = s.runs.data();
+    C.chunks = s.chunks.data();
+    C.pairs = dp.data();
+    C.narrow_width = narrow_width;
+    int64_t nu = 0, nt = 0;
+    for (size_t e = 0; e < lv.size(); e++) {
+        double est;
+        level_count(C, lv[e], &est);
+        lv[e].unit_off = (int32_t)nu;
+        lv[e].task_off = (int32_t)nt;
+        lv[e].entry = (int32_t)e;
+        nu += (int64_t)lv[e].nwide + lv[e].nnarrow;
+        nt += lv[e].ntasks;
+    }
+    out.units.resize((size_t)nu);
+    out.tasks.resize((size_t)nt);
+    out.entries.resize(lv.size());
+    for (size_t e = 0; e < lv.size(); e++) {
+        const DLevel &E = lv[e];
+        level_fill(C, E, out.units.data(), out.tasks.data());
+        XEntry &X = out.entries[e];
+        X.task_off = E.task_off;
+        X.ntasks = E.ntasks;
+        X.bucket = 0;
+        X.next = E.level + 1 < dp[(size_t)E.pair].L ? (int32_t)e + 1 : -1;
+    }
+}
+
+// Moves a plan to its device ranges: pairs of slot `slot` start at slot * T,
+// tables at dt_off, units at u_off, tasks at t_off, entries at e_off; every
+// entry goes to ready-queue bucket `bucket`.
+inline void serve_fixup(QPlan &p, int slot, int T, int64_t dt_off, int64_t u_off, int64_t t_off, int64_t e_off,
+                        int32_t bucket) {
+    const int32_t pair_base = (int32_t)((int64_t)slot * T);
+    for (XPair &x : p.pairs) x.dt_off += dt_off;
+    for (int32_t &f : p.first)
+        if (f >= 0) f += (int32_t)e_off;
+    for (XEntry &X : p.entries) {
+        X.task_off += (int32_t)t_off;
+        X.bucket = bucket;
+        if (X.next >= 0) X.next += (int32_t)e_off;
+    }
+    for (XTask &t : p.tasks) {
+        t.pair += pair_base;
+        t.entry += (int32_t)e_off;
+        t.unit_lo += (int32_t)u_off;
+    }
+}
+
+}  // namespace xted

@@ -117,11 +117,36 @@ struct XKernelParams {
     int32_t ntasks;
     int32_t nentries, npairs;
     int32_t *entry_state; // [2 * nentries]: tasks claimed, tasks done
-    int32_t *rq;          // [XTED_BUCKETS * nentries]: published entry ids, -1 = slot not yet written
-    int32_t *rq_ctl;      // [2 * XTED_BUCKETS]: head, tail of each bucket
+    // Bucket b's ring is rq[b << rq_log2 ...]; queue position pos lives in
+    // slot pos & (2^rq_log2 - 1) as (pos << 32 | entry), so a reader knows a
+    // slot holds position pos and not an older or not-yet-written one.
+    unsigned long long *rq;
+    int32_t rq_log2;
+    int32_t *rq_ctl;      // [2 * XTED_BUCKETS]: head, tail of each bucket (unsigned positions)
     int32_t *done_total;  // finished tasks
     int32_t *error;       // 0 = ok; else an XTED error code
     int32_t *error_info;  // [4] diagnostics of the first error
     uint64_t timeout_ns;  // bound on every idle wait
     unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, info
+    // ---- serving session (serve = 1); a batch launch leaves these zero ----
+    int32_t serve;
+    int32_t serve_pairs;    // pairs per query slot (the corpus size)
+    uint64_t idle_exit_ns;  // a block with no work for this long leaves the launch
+    int32_t *mbox;          // XTED_MBOX_* words and records, device memory
+    int32_t *slot_done;     // [XTED_SERVE_SLOTS] pairs finished in the slot's current query
+    const int32_t *slot_need, *slot_gen;  // pairs to finish, generation to report
+    int32_t *results;       // [slots * serve_pairs] distances, mapped host memory
+    int32_t *flags;         // [XTED_SERVE_SLOTS] generation of the last finished query, mapped host memory
 };
+
+// Serving mailbox in device memory. The host writes records and then the
+// posted count with stream-ordered copies; blocks claim records in order and
+// publish level 0 of the record's pairs into the running launch's ready queue.
+#define XTED_SERVE_SLOTS 16
+#define XTED_SERVE_RECS 64
+#define XTED_MBOX_POSTED 0    // records posted (host)
+#define XTED_MBOX_STOP 1      // nonzero: blocks leave when idle (host)
+#define XTED_MBOX_CONSUMED 2  // records claimed (device)
+#define XTED_MBOX_TOP 3       // bucket of the oldest query in flight (host)
+#define XTED_MBOX_REC 4       // records: 4 ints each {slot, pair_lo, npairs, 0}
+#define XTED_MBOX_INTS (XTED_MBOX_REC + 4 * XTED_SERVE_RECS)

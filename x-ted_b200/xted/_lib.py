@@ -25,6 +25,7 @@ XTED_EAGAIN = -7
 XTED_ETOOBIG = -8
 XTED_NOALLOC_ARENA_BYTES = 16 << 20
 XTED_MAX_NODES = 65535
+XTED_SERVE_MAX_QUERY = 8192
 
 ORIENT_AUTO, ORIENT_RIGHT, ORIENT_LEFT = 0, 1, 2
 
@@ -92,6 +93,9 @@ def lib():
             "xted_query_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _i32p, _i32p, _i32p]),
             "xted_serve_drain": (ctypes.c_int, [ctypes.c_void_p]),
             "xted_distance_noalloc": (ctypes.c_int, [P(CTree), P(CTree), ctypes.c_int32, _i32p]),
+            "xted_query_poll_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _i32p, _i32p, _i32p,
+                                                     P(ctypes.c_double), P(ctypes.c_double)]),
+            "xted_serve_stats": (ctypes.c_int, [ctypes.c_void_p, _i64p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -120,6 +120,65 @@ class Context:
         _lib.check(_lib.lib().xted_last_stats(self._h, ctypes.byref(s)))
         return s.as_dict()
 
+    # ---- serving: a resident corpus and exact top-k queries ----
+
+    def corpus_load(self, corpus: Sequence[Tree]) -> None:
+        """Makes `corpus` the resident corpus (ids are list positions)."""
+        keep: list = []
+        arr = (_lib.CTree * max(len(corpus), 1))()
+        for i, t in enumerate(corpus):
+            arr[i] = _lib.ctree(t, keep)
+        _lib.check(_lib.lib().xted_corpus_load(self._h, arr, len(corpus)), "xted_corpus_load")
+
+    def query_submit(self, q: Tree, k: int = 10) -> int:
+        """Queues a top-k query; returns its ticket at once."""
+        keep: list = []
+        cq = _lib.ctree(q, keep)
+        t = ctypes.c_uint64(0)
+        _lib.check(_lib.lib().xted_query_submit(self._h, ctypes.byref(cq), int(k), ctypes.byref(t)),
+                   "xted_query_submit")
+        self._k = getattr(self, "_k", {})
+        self._k[t.value] = int(k)
+        return int(t.value)
+
+    def query_poll(self, ticket: int):
+        """None while running; else (ids, dists, queue_ms, total_ms)."""
+        k = self._k.get(ticket, 1)
+        ids = np.zeros(k, np.int32)
+        dists = np.zeros(k, np.int32)
+        done = ctypes.c_int32(0)
+        qm, tm = ctypes.c_double(0), ctypes.c_double(0)
+        rc = _lib.lib().xted_query_poll_timed(self._h, ctypes.c_uint64(ticket), ids.ctypes.data_as(_lib._i32p),
+                                              dists.ctypes.data_as(_lib._i32p), ctypes.byref(done),
+                                              ctypes.byref(qm), ctypes.byref(tm))
+        if rc != 0:
+            self._k.pop(ticket, None)
+            _lib.check(rc, "xted_query_poll")
+        if not done.value:
+            return None
+        self._k.pop(ticket, None)
+        return ids, dists, qm.value, tm.value
+
+    def query_wait(self, ticket: int, poll_s: float = 0.0002, timeout_s: float = 600.0):
+        """Polls until the query is done; returns (ids, dists, queue_ms, total_ms)."""
+        import time
+        t_end = time.monotonic() + timeout_s
+        while True:
+            r = self.query_poll(ticket)
+            if r is not None:
+                return r
+            if time.monotonic() > t_end:
+                raise TimeoutError(f"query {ticket} not done after {timeout_s} s")
+            time.sleep(poll_s)
+
+    def serve_drain(self) -> None:
+        _lib.check(_lib.lib().xted_serve_drain(self._h), "xted_serve_drain")
+
+    def serve_stats(self) -> dict:
+        out = np.zeros(4, np.int64)
+        _lib.check(_lib.lib().xted_serve_stats(self._h, out.ctypes.data_as(_lib._i64p)), "xted_serve_stats")
+        return {"launches": int(out[0]), "queries": int(out[1]), "pairs": int(out[2]), "cells": int(out[3])}
+
 
 def default_context() -> Context:
     global _CTX
