@@ -215,6 +215,99 @@ def cpu_reference(pairs, budget_s: float, stride: int):
                                  f"{ncpu} threads per pair"}
 
 
+def serve_bench(ctx, budget_s: float = 30.0, seed: int = 6):
+    """Serving: a corpus of 1,000 resident trees (sizes uniform 100-1,000, mixed
+    shapes, Zipf(1.1) labels over 1,000 ids) and an open-loop Poisson stream of
+    query trees (same distribution), each asking for the exact top-10. First a
+    burst of queries measures the saturation rate; then Poisson arrivals at
+    fractions of it give p50/p99 latency (submission to completion, measured by
+    the library) and the achieved queries/s."""
+    import random
+    import numpy as np
+    from xted import gen
+    corpus = gen.corpus(1000, seed=5)
+    pool = gen.corpus(64, seed=seed)
+    ctx.corpus_load(corpus)
+    for q in pool[:2]:
+        ctx.query_wait(ctx.query_submit(q, 10))
+    st0 = ctx.serve_stats()
+    # saturation: a burst keeps every slot busy
+    burst = 32
+    t0 = time.perf_counter()
+    tickets = [ctx.query_submit(pool[i % len(pool)], 10) for i in range(burst)]
+    for t in tickets:
+        ctx.query_wait(t)
+    sat_s = time.perf_counter() - t0
+    st1 = ctx.serve_stats()
+    qps_sat = burst / sat_s
+    gcups_sat = (st1["cells"] - st0["cells"]) / sat_s / 1e9
+    rng = random.Random(seed)
+    sweep = []
+    per_rate_s = max(2.0, (budget_s - sat_s) / 3)
+    for frac in (0.5, 0.8, 0.95):
+        rate = frac * qps_sat
+        nq = max(8, int(rate * per_rate_s))
+        arrivals, t = [], 0.0
+        for _ in range(nq):
+            t += rng.expovariate(rate)
+            arrivals.append(t)
+        pending, lat = {}, []
+        start = time.perf_counter()
+        i = 0
+        last_done = start
+        while i < nq or pending:
+            now = time.perf_counter() - start
+            while i < nq and arrivals[i] <= now:
+                pending[ctx.query_submit(pool[rng.randrange(len(pool))], 10)] = True
+                i += 1
+            for tk in list(pending):
+                r = ctx.query_poll(tk)
+                if r is not None:
+                    lat.append(r[3])
+                    del pending[tk]
+                    last_done = time.perf_counter()
+            time.sleep(0.0002)
+        span = last_done - start
+        lat.sort()
+        sweep.append({"offered_qps": round(rate, 2), "achieved_qps": round(nq / span, 2), "queries": nq,
+                      "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                      "p99_ms": round(float(np.percentile(lat, 99)), 2)})
+    sustained = sweep[-1]
+    for r in sweep:
+        if r["achieved_qps"] >= 0.9 * r["offered_qps"]:
+            sustained = r
+    return {"workload": "corpus 1000 trees U[100,1000] mixed shapes, Zipf(1.1)/1000 labels; Poisson queries "
+                        "U[100,1000], exact top-10", "saturation_qps": round(qps_sat, 2),
+            "saturation_gcups": round(gcups_sat, 1), "sustained_qps": sustained["achieved_qps"],
+            "p50_ms": sustained["p50_ms"], "p99_ms": sustained["p99_ms"], "sweep": sweep,
+            "launches": ctx.serve_stats()["launches"]}
+
+
+def serve_cpu_baseline(budget_s: float, seed: int = 6):
+    """Reference X-TED_CPU for one serving query on a sample of the corpus
+    (all host cores per pair, pairs in sequence), extrapolated to the whole
+    corpus: queries/s."""
+    import oracle
+    from xted import gen
+    corpus = gen.corpus(1000, seed=5)
+    q = gen.corpus(64, seed=seed)[0]
+    ncpu = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    done, t0 = 0, time.perf_counter()
+    for t in corpus[::8]:
+        if kind == "reference":
+            oracle.ref_distance(q, t, num_threads=ncpu)
+        else:
+            oracle.distance(q, t)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(done / dt / len(corpus), 5), "unit": "queries/s", "cores": ncpu if kind == "reference" else 1,
+            "kind": kind, "sample": f"query 0 against every 8th corpus tree, first {done} pairs "
+                                    f"({dt:.1f} s), scaled to 1,000 corpus trees"}
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -250,6 +343,8 @@ def main():
     ap.add_argument("--plain-stride", type=int, default=16)
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
+    ap.add_argument("--serve-budget", type=float, default=20.0, help="seconds for the serving sweep")
     ap.add_argument("--wait-timeout", type=float, default=20.0,
                     help="bound of the DP kernel's idle waits, seconds (raise it under a profiler's replay)")
     args = ap.parse_args()
@@ -325,6 +420,13 @@ def main():
         cpu = {"value": round(v, 3), "unit": "pairs/s", "cores": info["cores"], "kind": info["kind"],
                "sample": info["sample"]}
 
+    # ---- serving (1 GPU) ----
+    serve = None
+    if world == 1 and not args.no_serve:
+        serve = serve_bench(ctx, args.serve_budget)
+        if not args.no_cpu_baseline:
+            serve["cpu_baseline"] = serve_cpu_baseline(min(args.ref_budget, 10.0))
+
     if rank != 0:
         return
     peak, peak_src = _peaks()
@@ -345,6 +447,7 @@ def main():
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
                      "kernel": "xted_dp_kernel", "bytes_per_cell": BYTES_PER_CELL},
         "cpu_baseline": cpu,
+        "serve": serve,
         "gpu_launches": 3 * args.steps,  # ready-queue init, DP, gather per step
         "clocks": clk.summary(),
         "tasks": st["tasks"], "units": st["units"], "grid": st["grid"], "host_plan_ms": round(plan_ms, 2),
