@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "../../include/xted.h"
@@ -186,6 +187,21 @@ int ctx_run(xted_ctx *c, int32_t *out) {
             if (FILE *f = std::fopen(std::getenv("XTED_TRACE"), "wb")) {
                 std::fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
                 std::fclose(f);
+            }
+            // the plan beside it: tasks (pair, entry, kind, first unit) and entries
+            std::vector<XTask> tk((size_t)K.ntasks);
+            std::vector<XEntry> en((size_t)K.nentries);
+            const std::string base = std::getenv("XTED_TRACE");
+            if (cudaMemcpy(tk.data(), K.tasks, tk.size() * sizeof(XTask), cudaMemcpyDeviceToHost) == cudaSuccess &&
+                cudaMemcpy(en.data(), K.entries, en.size() * sizeof(XEntry), cudaMemcpyDeviceToHost) == cudaSuccess) {
+                if (FILE *f = std::fopen((base + ".tasks").c_str(), "wb")) {
+                    std::fwrite(tk.data(), sizeof(XTask), tk.size(), f);
+                    std::fclose(f);
+                }
+                if (FILE *f = std::fopen((base + ".entries").c_str(), "wb")) {
+                    std::fwrite(en.data(), sizeof(XEntry), en.size(), f);
+                    std::fclose(f);
+                }
             }
         }
     }

@@ -691,51 +691,36 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 // idle spell), or CLAIM_RECORD with *entry = a mailbox record this block
 // claimed and must publish. Buckets are probed from the most urgent: bucket
 // 15 down in a batch, the oldest query's bucket onwards in a serving session.
-// Blocks probe a bucket's live window [head, tail) starting at a
-// block-dependent position, so they spread over many entries instead of all
-// contending for the head entry, and test an entry with a plain load before
-// claiming from it; whoever sees exhausted entries at the head moves it on.
-// Idle polling is bounded by time and by iterations.
+// Within a bucket entries are served first in, first out: a block claims the
+// next task of the entry at the bucket's head, and whoever finds that entry
+// exhausted moves the head on. Idle polling is bounded by time and by
+// iterations.
 __device__ int claim_task(const XKernelParams &P, int *entry) {
     volatile int32_t *ctl = P.rq_ctl;
     volatile int32_t *state = P.entry_state;
     volatile int32_t *mbox = P.mbox;
     unsigned ns = 32;
     uint64_t t0 = 0;
-    unsigned salt = blockIdx.x * 2654435761u;
     for (long it = 0; it < (1L << 28); it++) {
         if (*(volatile int32_t *)P.error != 0) return CLAIM_EXIT;
         const int top = P.serve ? mbox[XTED_MBOX_TOP] : XTED_BUCKETS - 1;
         for (int i = 0; i < XTED_BUCKETS; i++) {
             const int b = (top - i) & (XTED_BUCKETS - 1);
-            unsigned h = (unsigned)ctl[2 * b];
-            // move the head over exhausted entries
-            for (int guard = 0; guard < 64; guard++) {
-                if ((int)((unsigned)ctl[2 * b + 1] - h) <= 0) break;
+            for (int guard = 0; guard < 256; guard++) {
+                const unsigned h = (unsigned)ctl[2 * b];
+                if ((int)((unsigned)ctl[2 * b + 1] - h) <= 0) break;  // empty
                 const int e = rq_entry(P, b, h);
-                if (e < 0 || state[2 * e] < P.entries[e].ntasks) break;
-                atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));
-                h = (unsigned)ctl[2 * b];
-            }
-            const unsigned tl = (unsigned)ctl[2 * b + 1];
-            const int live = (int)(tl - h);
-            if (live <= 0) continue;
-            salt = salt * 1664525u + 1013904223u;
-            const int start = (int)(salt % (unsigned)live);
-            const int probes = live < 32 ? live : 32;
-            for (int j = 0; j < probes; j++) {
-                int off = start + j;
-                if (off >= live) off -= live;
-                const int e = rq_entry(P, b, h + (unsigned)off);
-                if (e < 0) continue;  // position reserved but not yet written
+                if (e < 0) break;  // the head position is reserved but not yet written
                 const XEntry X = P.entries[e];
-                if (state[2 * e] >= X.ntasks) continue;
-                const int k = atomicAdd(&P.entry_state[2 * e], 1);
-                if (k < X.ntasks) {
-                    __threadfence();  // acquire: the level's inputs are visible from here on
-                    *entry = e;
-                    return X.task_off + k;
+                if (state[2 * e] < X.ntasks) {
+                    const int k = atomicAdd(&P.entry_state[2 * e], 1);
+                    if (k < X.ntasks) {
+                        __threadfence();  // acquire: the level's inputs are visible from here on
+                        *entry = e;
+                        return X.task_off + k;
+                    }
                 }
+                atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));  // exhausted: next entry
             }
         }
         if (P.serve) {

@@ -125,10 +125,24 @@ XT_HD inline void tree_basic(const PlanPools &P, int t, DTree *trees_out) {
     trees_out[t] = T;
 }
 
+// Cycles one row of a unit takes under full load (fitted to per-task traces
+// of the mixed batch): a warp's narrow row, a block's wide row.
 XT_HD inline double row_cost_est(bool wide, int width) {
     if (width <= 0) return 0.0;
-    if (!wide) return 64.0 + 16.0 * ((width + 31) / 32);
-    return 280.0 + 16.0 * ((width + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS);
+    if (!wide) return 2800.0 + 6.0 * width;
+    return 1300.0 + 0.7 * width;
+}
+
+// Narrow units of one level are bundled into tasks of this many units (the
+// block's 8 warps claim them one at a time): small bundles when the level has
+// few units, so its units spread over several blocks and the level (often on
+// a pair's critical path) finishes sooner; up to XTED_TASK_UNITS when there
+// are plenty, to keep per-task overhead low.
+XT_HD inline int32_t level_bundle(int64_t nnarrow) {
+    int64_t b = (nnarrow + 15) / 16;
+    if (b < XTED_WARPS) b = XTED_WARPS;
+    if (b > XTED_TASK_UNITS) b = XTED_TASK_UNITS;
+    return (int32_t)b;
 }
 
 // Builds oriented tree ot = 2 t + o: node records, keyroot depths, keyroots
@@ -318,30 +332,48 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
     int64_t wide = 0, narrow = 0;
-    double est = 0.0;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         const int64_t nr = ra.run_hi - ra.run_lo;
         wide += nr * cb.nwide;
         narrow += nr * cb.nnarrow;
-        double c = row_cost_est(false, cb.maxw_n);
-        const double cw = row_cost_est(true, cb.maxw_w);
-        if (cw > c) c = cw;
-        const double e = ra.maxrows * c;
+    }
+    const int32_t bundle = level_bundle(narrow);
+    const int rounds = (bundle + XTED_WARPS - 1) / XTED_WARPS;  // units a warp runs in one task
+    // the level's longest task: its largest run against its widest chunk
+    double est = 0.0;
+    for (int al = lo; al <= hi; al++) {
+        const DDepth &ra = da[al], &cb = db[d - al];
+        double e = 0.0;
+        if (cb.nnarrow > 0) e = rounds * ra.maxrows * row_cost_est(false, cb.maxw_n);
+        if (cb.nwide > 0) {
+            const double ew = ra.maxrows * row_cost_est(true, cb.maxw_w);
+            if (ew > e) e = ew;
+        }
         if (e > est) est = e;
     }
     E.nwide = (int32_t)wide;
     E.nnarrow = (int32_t)narrow;
-    E.ntasks = (int32_t)(wide + (narrow + XTED_TASK_UNITS - 1) / XTED_TASK_UNITS);
+    E.ntasks = (int32_t)(wide + (narrow + bundle - 1) / bundle);
     *est_out = est;
 }
 
 // Ready-queue bucket of a level whose pair has `remaining` estimated time left
 // (this level included) when the longest pair of the batch has `chain_max`.
+// Half-octave scale: bucket 15 holds the levels within a factor sqrt(2) of
+// the longest chain, each bucket below another factor sqrt(2) less, so pairs
+// with mid-length chains keep priority over the many short ones instead of
+// sharing the lowest bucket with them.
 XT_HD inline int32_t level_bucket(int64_t remaining, int64_t chain_max) {
-    int64_t b = remaining * XTED_BUCKETS / (chain_max + 1);
-    return (int32_t)(b < 0 ? 0 : (b >= XTED_BUCKETS ? XTED_BUCKETS - 1 : b));
+    double x = remaining > 0 ? (double)remaining : 1.0;
+    const double lim = (double)chain_max;
+    int32_t b = XTED_BUCKETS - 1;
+    while (b > 0 && x * 1.4142135623730951 < lim) {
+        x *= 1.4142135623730951;
+        b--;
+    }
+    return b;
 }
 
 // Writes the units and tasks of level entry E (offsets already assigned).
@@ -351,6 +383,7 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
     int32_t u = E.unit_off, t = E.task_off;
+    const int32_t per_task = level_bundle(E.nnarrow);
     int32_t bundle = 0, bundle_lo = u;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
     for (int al = lo; al <= hi; al++) {
@@ -359,7 +392,7 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
             for (int32_t c = cb.chunk_lo; c < cb.chunk_lo + cb.nnarrow; c++) {
                 if (bundle == 0) bundle_lo = u;
                 units[u++] = XUnit{r, c};
-                if (++bundle == XTED_TASK_UNITS) {
+                if (++bundle == per_task) {
                     tasks[t++] = XTask{E.pair, E.entry, (uint32_t)bundle, bundle_lo};
                     bundle = 0;
                 }
