@@ -132,6 +132,10 @@ def make_workload(name: str, rank: int):
         return gen.mixed_batch(256, seed=4 + 1000 * rank), {
             "workload": "256 mixed pairs (same distribution as the 4096-pair batch; profiling size)",
             "npairs": 256, "seed": 4 + 1000 * rank}
+    if name == "batched1024":
+        return gen.mixed_batch(1024, seed=4 + 1000 * rank), {
+            "workload": "1024 mixed pairs (same distribution as the 4096-pair batch; profiling size)",
+            "npairs": 1024, "seed": 4 + 1000 * rank}
     if name == "single100":
         return [gen.single_pair_100()], {"workload": "one pair, 100 vs 100 random recursive, 26 labels"}
     if name == "single1000":

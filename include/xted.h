@@ -66,7 +66,10 @@ typedef struct xted_opts {
                                0 runs every chunk on a whole thread block   */
     int32_t run_rows;       /* target rows per row run (>= 1)               */
     int32_t ctas_per_sm;    /* persistent blocks per SM (0 = occupancy max) */
-    int32_t reserved;
+    int32_t wide_rows;      /* > 0: a narrow chunk's unit whose row run is
+                               longer than this runs on the whole block
+                               (shortens critical paths, costs throughput);
+                               <= 0: never (default)                        */
     double wait_timeout_s;  /* bound on every device-side wait              */
     int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
 } xted_opts;

@@ -44,7 +44,7 @@ struct HostPlan {
 static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<std::vector<int32_t>> &O,
                  const std::vector<std::vector<int32_t>> &I, const std::vector<int> &nn,
                  const std::vector<int32_t> &pair_trees, int orientation, int narrow_width, int run_rows,
-                 HostPlan &H) {
+                 int wide_rows, HostPlan &H) {
     const int T = (int)nn.size();
     int64_t N = 0;
     H.trees.resize((size_t)T);
@@ -111,7 +111,8 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
         }
     }
     H.lv.resize((size_t)ent);
-    LevelCtx C{H.ot.data(), H.depths.data(), H.runs.data(), H.chunks.data(), H.pairs.data(), narrow_width};
+    LevelCtx C{H.ot.data(), H.depths.data(), H.runs.data(), H.chunks.data(), H.pairs.data(), narrow_width,
+               wide_rows};
     std::vector<int64_t> chain((size_t)np, 0);
     int64_t chain_max = 0;
     for (int p = 0; p < np; p++) {
@@ -203,8 +204,10 @@ int main(int argc, char **argv) {
         std::vector<int32_t> pt;
         for (int p = 0; p < 2 * npairs; p++) pt.push_back((int32_t)(g() % (uint64_t)ntrees));
         const int orient = it % 3, nw = nws[it % 4], rr = 1 + (int)(g() % 100);
+        const int wrs[4] = {256, -1, 4, 40};
+        const int wr = wrs[(it / 4) % 4];
         HostPlan H;
-        plan(L, O, I, nn, pt, orient, nw, rr, H);
+        plan(L, O, I, nn, pt, orient, nw, rr, wr, H);
         int64_t dts = 0;
         for (auto &q : H.pairs)
             if (q.trivial < 0) dts += (int64_t)H.trees[(size_t)q.ta].n * H.trees[(size_t)q.tb].n;

@@ -104,7 +104,8 @@ int main(int argc, char **argv) {
             const int n = (g() % 8 == 0) ? 0 : 1 + (int)(g() % (uint64_t)Qmax);
             qs[(size_t)q] = gen(n, g, 1 + (int)(g() % 5), (int)(g() % 4));
             const HTree &h = qs[(size_t)q];
-            serve_plan_query(H, q, h.lab.data(), h.off.data(), h.idx.data(), h.n, orient, narrow, plans[(size_t)q]);
+            serve_plan_query(H, q, h.lab.data(), h.off.data(), h.idx.data(), h.n, orient, narrow,
+                             (r % 2) ? 5 : 256, plans[(size_t)q]);
             QPlan &p = plans[(size_t)q];
             u_at += (int64_t)(g() % 1000);
             t_at += (int64_t)(g() % 1000);

@@ -1,7 +1,10 @@
 // plan.h -- host-side checks of caller trees (planning itself runs on the device, prep.cu).
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "xted_internal.h"
@@ -23,6 +26,35 @@ void keyroot_sums(const TreeView &t, int64_t S[2]);
 
 // Validates a preorder CSR tree. Returns 0 or XTED_EINVAL.
 int validate_tree(const TreeView &t);
+
+// Runs f(lo, hi) over [0, n) split across host threads, at least `grain`
+// items per thread (inline when that leaves one thread, or when threads
+// cannot be started).
+template <class F>
+void parallel_for(int64_t n, int64_t grain, F &&f) {
+    unsigned hw = std::thread::hardware_concurrency();
+    const int64_t nt = std::min<int64_t>(std::max(1u, std::min(hw, 32u)), (n + grain - 1) / std::max<int64_t>(grain, 1));
+    if (nt <= 1) {
+        f((int64_t)0, n);
+        return;
+    }
+    const int64_t per = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    int64_t done_inline = 0;
+    for (int64_t k = 1; k < nt; k++) {
+        const int64_t lo = k * per, hi = std::min(n, lo + per);
+        if (lo >= hi) break;
+        try {
+            th.emplace_back(f, lo, hi);
+        } catch (const std::system_error &) {
+            done_inline = lo;  // run the rest here
+            break;
+        }
+    }
+    f((int64_t)0, std::min(n, per));
+    if (done_inline > 0) f(done_inline, n);
+    for (std::thread &t : th) t.join();
+}
 
 // Identity of a caller's tree (its pointers and size): the same tree passed in
 // several pairs is preprocessed once.

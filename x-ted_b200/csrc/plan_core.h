@@ -323,7 +323,14 @@ struct LevelCtx {
     const XChunk *chunks;
     const DPair *pairs;
     int32_t narrow_width;
+    int32_t wide_rows;  // narrow-chunk units of runs longer than this are wide tasks (< 0: none)
 };
+
+// A unit of a narrow chunk whose run is long (one big keyroot) would keep a
+// whole block waiting on one warp; it runs on the whole block instead.
+XT_HD inline bool big_run(const LevelCtx &C, int32_t run) {
+    return C.wide_rows >= 0 && C.runs[run].rows > C.wide_rows;
+}
 
 // Units and tasks of level entry e (pair, level) and its time estimate.
 XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
@@ -333,11 +340,20 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     const int d = E.level;
     int64_t wide = 0, narrow = 0;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
+    int32_t small_max[64];  // longest non-big run per depth (the first 64 depths; more use maxrows)
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         const int64_t nr = ra.run_hi - ra.run_lo;
-        wide += nr * cb.nwide;
-        narrow += nr * cb.nnarrow;
+        int64_t nbig = 0;
+        int32_t sm = 0;
+        if (cb.nnarrow > 0)
+            for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+                if (big_run(C, r)) nbig++;
+                else if (C.runs[r].rows > sm) sm = C.runs[r].rows;
+            }
+        if (al - lo < 64) small_max[al - lo] = sm;
+        wide += nr * cb.nwide + nbig * cb.nnarrow;
+        narrow += (nr - nbig) * cb.nnarrow;
     }
     const int32_t bundle = level_bundle(narrow);
     const int rounds = (bundle + XTED_WARPS - 1) / XTED_WARPS;  // units a warp runs in one task
@@ -346,7 +362,14 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         double e = 0.0;
-        if (cb.nnarrow > 0) e = rounds * ra.maxrows * row_cost_est(false, cb.maxw_n);
+        if (cb.nnarrow > 0) {
+            const int32_t sm = al - lo < 64 ? small_max[al - lo] : ra.maxrows;
+            e = rounds * sm * row_cost_est(false, cb.maxw_n);
+            if (C.wide_rows >= 0 && ra.maxrows > C.wide_rows) {
+                const double eb = ra.maxrows * row_cost_est(true, cb.maxw_n);
+                if (eb > e) e = eb;
+            }
+        }
         if (cb.nwide > 0) {
             const double ew = ra.maxrows * row_cost_est(true, cb.maxw_w);
             if (ew > e) e = ew;
@@ -389,6 +412,7 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            if (big_run(C, r)) continue;
             for (int32_t c = cb.chunk_lo; c < cb.chunk_lo + cb.nnarrow; c++) {
                 if (bundle == 0) bundle_lo = u;
                 units[u++] = XUnit{r, c};
@@ -402,12 +426,15 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
     if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, (uint32_t)bundle, bundle_lo};
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
-        for (int32_t r = ra.run_lo; r < ra.run_hi; r++)
-            for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nwide; c++) {
+        for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            const bool big = big_run(C, r);
+            const int32_t c_lo = big ? cb.chunk_lo : cb.chunk_lo + cb.nnarrow;
+            for (int32_t c = c_lo; c < cb.chunk_lo + cb.nnarrow + cb.nwide; c++) {
                 units[u] = XUnit{r, c};
                 tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
                 u++;
             }
+        }
     }
 }
 

@@ -220,10 +220,8 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
             if (it == c->tree_ids.end()) {
                 id = (int)c->uniq.size();
                 c->tree_ids.emplace(key, id);
-                TreeView tv{t.n, t.labels, t.child_off, t.child_idx};
-                int rc = validate_tree(tv);
-                if (rc) return rc;
-                c->uniq.push_back(tv);
+                if (t.n < 0 || t.n > XTED_MAX_NODES) return XTED_EINVAL;
+                c->uniq.push_back(TreeView{t.n, t.labels, t.child_off, t.child_idx});
                 N += t.n;
                 R += 3 * (int64_t)t.n + 1;
             } else {
@@ -234,6 +232,14 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     }
     const int T = (int)c->uniq.size();
     if (N > (int64_t)1 << 30) return XTED_ENOMEM;
+    {   // every unique tree is checked before anything reads it (host threads for big batches)
+        std::vector<int> bad((size_t)std::max(T, 1), 0);
+        parallel_for(T, 512, [&](int64_t lo, int64_t hi) {
+            for (int64_t t = lo; t < hi; t++) bad[(size_t)t] = validate_tree(c->uniq[(size_t)t]);
+        });
+        for (int t = 0; t < T; t++)
+            if (bad[(size_t)t]) return bad[(size_t)t];
+    }
     std::vector<DTree> &ht = c->htrees;
     ht.resize((size_t)T);
     // staging: raw trees | DTree[T] | pair_trees
@@ -254,17 +260,23 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
             d.nbase = (int32_t)nb;
             d.t = t;
             d.S[0] = d.S[1] = 0;
-            const int n = tv.n;
-            if (n > 0) {
-                std::memcpy(hraw + rpos, tv.labels, 4 * (size_t)n);
-                std::memcpy(hraw + rpos + n, tv.off, 4 * ((size_t)n + 1));
-                if (n > 1) std::memcpy(hraw + rpos + 2 * n + 1, tv.idx, 4 * ((size_t)n - 1));
-            } else {
-                hraw[rpos] = 0;  // child_off[0]
-            }
-            rpos += 3 * (int64_t)n + 1;
-            nb += n;
+            rpos += 3 * (int64_t)tv.n + 1;
+            nb += tv.n;
         }
+        parallel_for(T, 512, [&](int64_t lo, int64_t hi) {
+            for (int64_t t = lo; t < hi; t++) {
+                const TreeView &tv = c->uniq[(size_t)t];
+                int32_t *dst = hraw + ht[(size_t)t].raw;
+                const int n = tv.n;
+                if (n > 0) {
+                    std::memcpy(dst, tv.labels, 4 * (size_t)n);
+                    std::memcpy(dst + n, tv.off, 4 * ((size_t)n + 1));
+                    if (n > 1) std::memcpy(dst + 2 * n + 1, tv.idx, 4 * ((size_t)n - 1));
+                } else {
+                    dst[0] = 0;  // child_off[0]
+                }
+            }
+        });
     }
     size_t hoff = (raw_bytes + 255) & ~(size_t)255;
     std::memcpy(h + hoff, ht.data(), tr_bytes);
@@ -354,6 +366,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     C.chunks = P.chunks;
     C.pairs = d_pairs;
     C.narrow_width = c->opts.narrow_width;
+    C.wide_rows = c->opts.wide_rows > 0 ? c->opts.wide_rows : -1;
     if (nent > 0) {
         k_level_expand<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv);
         k_level_count<<<blocks_for(nent, BS), BS, 0, s>>>(C, d_lv, nent, d_units, d_tasks);

@@ -381,8 +381,10 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
             s->next_seq++;
             Query qcopy = q;  // plan outside the lock
             lk.unlock();
+            const int wr = s->c->opts.wide_rows;
             serve_plan_query(s->pools, slot, qcopy.lab.data(), qcopy.off.data(), qcopy.idx.data(), qcopy.n,
-                             s->c->opts.orientation, s->c->opts.narrow_width, sl.plan);
+                             s->c->opts.orientation, s->c->opts.narrow_width, wr > 0 ? wr : -1,
+                             sl.plan);
             lk.lock();
             if (s->stop || !sl.busy || sl.ticket != ticket) break;  // shut down meanwhile
             sl.planned = true;

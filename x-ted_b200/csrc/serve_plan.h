@@ -134,7 +134,7 @@ inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, 
 // the slot's region, then every (corpus tree, query) pair as the batch
 // planner does (k_pair_setup ... k_level_fill in prep.cu).
 inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const int32_t *off, const int32_t *idx,
-                             int n, int orientation, int narrow_width, QPlan &out) {
+                             int n, int orientation, int narrow_width, int wide_rows, QPlan &out) {
     const int T = s.T, tq = T + slot;
     DTree &Q = s.trees[(size_t)tq];
     Q.n = n;
@@ -192,6 +192,7 @@ inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const 
     C.chunks = s.chunks.data();
     C.pairs = dp.data();
     C.narrow_width = narrow_width;
+    C.wide_rows = wide_rows;
     int64_t nu = 0, nt = 0;
     for (size_t e = 0; e < lv.size(); e++) {
         double est;

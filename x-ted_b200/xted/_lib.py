@@ -40,7 +40,7 @@ class CTree(ctypes.Structure):
 class COpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("orientation", ctypes.c_int32),
                 ("narrow_width", ctypes.c_int32), ("run_rows", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("wide_rows", ctypes.c_int32),
                 ("wait_timeout_s", ctypes.c_double), ("mem_limit", ctypes.c_int64)]
 
 
@@ -108,6 +108,45 @@ def lib():
 def check(code: int, what: str = "") -> None:
     if code != XTED_OK:
         raise XtedError(code, what)
+
+
+# numpy view of an xted_tree array: building the C array in one vectorised
+# assignment costs about a microsecond per tree, where filling ctypes
+# structures one by one costs tens.
+TREE_DTYPE = np.dtype([("labels", np.uintp), ("child_off", np.uintp), ("child_idx", np.uintp),
+                       ("n", np.int32), ("_pad", np.int32)])
+assert TREE_DTYPE.itemsize == ctypes.sizeof(CTree)
+
+
+def tree_record(t) -> tuple:
+    """(labels, child_off, child_idx pointers, n) of a Tree, cached on the tree
+    object together with the contiguous int32 arrays the pointers refer to."""
+    cv = getattr(t, "_xted_cv", None)
+    if cv is not None and cv[0] is t.labels and cv[1] is t.off and cv[2] is t.idx:
+        return cv[4]
+    lab = np.ascontiguousarray(t.labels, dtype=np.int32)
+    off = np.ascontiguousarray(t.off, dtype=np.int32)
+    idx = np.ascontiguousarray(t.idx, dtype=np.int32)
+    hold = (lab if lab.size else np.zeros(1, np.int32), off if off.size else np.zeros(1, np.int32),
+            idx if idx.size else np.zeros(1, np.int32))
+    rec = (hold[0].ctypes.data, hold[1].ctypes.data, hold[2].ctypes.data, int(len(t.labels)), 0)
+    try:
+        t._xted_cv = (t.labels, t.off, t.idx, hold, rec)
+    except AttributeError:  # objects that take no attributes: no caching
+        pass
+    return rec
+
+
+def tree_array(trees_) -> np.ndarray:
+    """Contiguous xted_tree array of `trees_` (each tree keeps its buffers alive)."""
+    arr = np.empty(max(len(trees_), 1), TREE_DTYPE)
+    if len(trees_):
+        arr[:len(trees_)] = [tree_record(t) for t in trees_]
+    return arr
+
+
+def tree_ptr(arr: np.ndarray):
+    return arr.ctypes.data_as(ctypes.POINTER(CTree))
 
 
 def ctree(t, keep: list) -> CTree:

@@ -28,7 +28,8 @@ _CTX: Optional["Context"] = None
 class Context:
     def __init__(self, device: int = 0, orientation: int = _lib.ORIENT_AUTO,
                  narrow_width: Optional[int] = None, run_rows: Optional[int] = None,
-                 ctas_per_sm: int = 0, wait_timeout_s: float = 20.0, mem_limit: int = 0):
+                 ctas_per_sm: int = 0, wait_timeout_s: float = 20.0, mem_limit: int = 0,
+                 wide_rows: int = 0):
         L = _lib.lib()
         o = _lib.COpts()
         L.xted_opts_default(ctypes.byref(o))
@@ -39,6 +40,7 @@ class Context:
         if run_rows is not None:
             o.run_rows = run_rows
         o.ctas_per_sm = ctas_per_sm
+        o.wide_rows = wide_rows
         o.wait_timeout_s = wait_timeout_s
         o.mem_limit = mem_limit
         self.opts = o
@@ -77,24 +79,10 @@ class Context:
 
     @staticmethod
     def _views(pairs):
-        """C tree arrays for a pair list; a tree object shared by several pairs
-        is passed once, so the library preprocesses it once."""
-        keep: list = []
-        n = len(pairs)
-        A = (_lib.CTree * max(n, 1))()
-        B = (_lib.CTree * max(n, 1))()
-        cache = {}
-
-        def view(t):
-            k = id(t)
-            if k not in cache:
-                cache[k] = _lib.ctree(t, keep)
-            return cache[k]
-
-        for p, (a, b) in enumerate(pairs):
-            A[p] = view(a)
-            B[p] = view(b)
-        return A, B, keep
+        """C tree arrays for a pair list (numpy-backed xted_tree arrays)."""
+        A = _lib.tree_array([a for a, _ in pairs])
+        B = _lib.tree_array([b for _, b in pairs])
+        return _lib.tree_ptr(A), _lib.tree_ptr(B), (A, B)
 
     def distance_batch(self, pairs: Sequence[Tuple[Tree, Tree]]) -> np.ndarray:
         n = len(pairs)
