@@ -143,9 +143,13 @@ int xted_gen_tree(int32_t shape, int32_t n, uint64_t seed, int32_t label_kind, i
  * (about 8(m + n) ints), the m x n tree-distance matrix and at least one
  * (m + 1) x (n + 1) forest table must fit in the arena (a pair of two
  * 1400-node trees fits); larger pairs return XTED_ETOOBIG. Synchronous. Every
- * call on a device shares the one arena: calls that overlap on the GPU (two
- * host threads at once) race, so serialise them. Same results and empty-tree
- * rules as xted_distance. */
+ * call on a device shares the one arena, which keeps the last call's
+ * contents (each call clears its status words and overwrites everything else
+ * it reads): calls that overlap on the GPU (two host threads at once) race,
+ * so serialise them. The first call on a device does the set-up: it checks
+ * the device and looks up the arena's device address with that device
+ * current; make that first call before any stream capture. Same results and
+ * empty-tree rules as xted_distance. */
 #define XTED_NOALLOC_ARENA_BYTES (16 << 20)
 int xted_distance_noalloc(const xted_tree *a, const xted_tree *b, int32_t device, int32_t *out);
 

@@ -9,10 +9,14 @@
 // part of the loaded module: no cudaMalloc, no cudaFree, no pinned host
 // buffer, no host heap.
 //
-// The arena is shared by every call in the process on a device. The entry
-// point is synchronous, so calls made one after another from one host thread
-// are safe; calls that overlap on the GPU (two host threads at once) race on
-// the arena and must be serialised by the caller.
+// The arena is shared by every call in the process on a device and keeps the
+// last call's contents; a call clears only its status words and writes every
+// other cell before reading it. The entry point is synchronous, so calls made
+// one after another from one host thread are safe; calls that overlap on the
+// GPU (two host threads at once) race on the arena and must be serialised by
+// the caller. The first call on a device checks the device and looks up the
+// arena's device address (the array's name is only a stand-in in host code),
+// so that first call belongs before any stream capture.
 //
 // Algorithm: the same right-path keyroot decomposition as the batched path
 // (orl(v) = v + size(v) - 1 in preorder; keyroots = root and every child that
