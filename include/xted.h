@@ -70,6 +70,11 @@ typedef struct xted_opts {
                                longer than this runs on the whole block
                                (shortens critical paths, costs throughput);
                                <= 0: never (default)                        */
+    int32_t half_width;     /* chunks wider than narrow_width up to this
+                               width (at most 1024) run on half a block, two
+                               at a time; 0 = 512 (fastest on the mixed
+                               batch), < 0: none                            */
+    int32_t reserved;
     double wait_timeout_s;  /* bound on every device-side wait              */
     int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
 } xted_opts;

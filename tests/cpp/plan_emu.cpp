@@ -44,7 +44,7 @@ struct HostPlan {
 static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<std::vector<int32_t>> &O,
                  const std::vector<std::vector<int32_t>> &I, const std::vector<int> &nn,
                  const std::vector<int32_t> &pair_trees, int orientation, int narrow_width, int run_rows,
-                 int wide_rows, HostPlan &H) {
+                 int wide_rows, int half_width, HostPlan &H) {
     const int T = (int)nn.size();
     int64_t N = 0;
     H.trees.resize((size_t)T);
@@ -94,6 +94,7 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     P.otrees = H.ot.data();
     P.run_rows = run_rows;
     P.narrow_width = narrow_width;
+    P.half_width = half_width;
     for (int t = 0; t < T; t++) tree_basic(P, t, H.trees.data());
     for (int o = 0; o < 2 * T; o++) orient_tree(P, o);
     const int np = (int)pair_trees.size() / 2;
@@ -139,7 +140,7 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
         E.unit_off = (int32_t)uoff;
         E.entry = (int32_t)e;
         toff += E.ntasks;
-        uoff += (int64_t)E.nwide + E.nnarrow;
+        uoff += (int64_t)E.nwide + E.nnarrow + E.nhalf;
         XEntry &X = H.entries[e];
         X.task_off = E.task_off;
         X.ntasks = E.ntasks;
@@ -206,8 +207,10 @@ int main(int argc, char **argv) {
         const int orient = it % 3, nw = nws[it % 4], rr = 1 + (int)(g() % 100);
         const int wrs[4] = {256, -1, 4, 40};
         const int wr = wrs[(it / 4) % 4];
+        const int hws[3] = {XTED_HALF_MAX, -1, 100};
+        const int hw = hws[(it / 16) % 3];
         HostPlan H;
-        plan(L, O, I, nn, pt, orient, nw, rr, wr, H);
+        plan(L, O, I, nn, pt, orient, nw, rr, wr, hw, H);
         int64_t dts = 0;
         for (auto &q : H.pairs)
             if (q.trivial < 0) dts += (int64_t)H.trees[(size_t)q.ta].n * H.trees[(size_t)q.tb].n;
@@ -235,8 +238,14 @@ int main(int argc, char **argv) {
                 const XTask &t = H.tasks[(size_t)(X.task_off + k)];
                 if (t.pair != E.pair || t.entry != e) FAIL("task of another entry in the range");
                 const int nu = (int)(t.kind_n & 0xffff);
-                const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
-                if (nu < 1 || nu > XTED_TASK_UNITS || (wide && nu != 1)) FAIL("bad unit count %d", nu);
+                const bool full = (t.kind_n & XTED_TASK_WIDE) != 0, half = (t.kind_n & XTED_TASK_HALF) != 0;
+                const bool wide = full || half;
+                if (nu < 1 || nu > XTED_TASK_UNITS || (full && nu != 1) || (half && nu > 8)) FAIL("bad unit count %d", nu);
+                for (int u = 0; u < nu; u++) {
+                    const int w = H.chunks[(size_t)H.units[(size_t)(t.unit_lo + u)].chunk].width;
+                    if (half && (w <= nw || w > XTED_HALF_MAX || w > hw)) FAIL("half unit of width %d", w);
+                    if (full && w <= XTED_HALF_MAX && w > nw && hw >= w) FAIL("whole-block unit of width %d", w);
+                }
                 const DPair &q = H.pairs[(size_t)t.pair];
                 XPair x;
                 x.dt_off = q.dt_off;

@@ -87,7 +87,7 @@ int main(int argc, char **argv) {
         const int narrow = r % 3 == 0 ? XTED_NARROW_MAX : (r % 3 == 1 ? 7 : 0);
         const int run_rows = 1 + (int)(g() % 80), orient = r % 3;
         ServePools H;
-        serve_pools_build(H, ct.data(), T, S, Qmax, run_rows, narrow);
+        serve_pools_build(H, ct.data(), T, S, Qmax, run_rows, narrow, (r % 4 == 3) ? -1 : XTED_HALF_MAX);
         // device-style pools; plans land at scattered offsets
         const int64_t UC = 1 << 22, TC = 1 << 21, EC = 1 << 18;
         std::vector<XPair> pairs((size_t)S * T);
@@ -177,8 +177,9 @@ int main(int argc, char **argv) {
                     FAIL("pair node ranges outside the pools");
                 if (x.dt_off < 0 || x.dt_off + (int64_t)x.m * x.n > dt_at) FAIL("pair table outside the pool");
                 const int nu = (int)(t.kind_n & 0xffff);
-                const bool wide = (t.kind_n & XTED_TASK_WIDE) != 0;
-                if (nu < 1 || nu > XTED_TASK_UNITS || (wide && nu != 1)) FAIL("bad unit count %d", nu);
+                const bool full = (t.kind_n & XTED_TASK_WIDE) != 0, half = (t.kind_n & XTED_TASK_HALF) != 0;
+                const bool wide = full || half;
+                if (nu < 1 || nu > XTED_TASK_UNITS || (full && nu != 1) || (half && nu > 8)) FAIL("bad unit count %d", nu);
                 for (int u = 0; u < nu; u++) {
                     if (t.unit_lo + u >= UC) FAIL("unit index out of range");
                     const XUnit &U = units[(size_t)(t.unit_lo + u)];

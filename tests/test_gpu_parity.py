@@ -71,17 +71,20 @@ def test_golden_synthetic(ctx, golden_synthetic):
 
 
 @pytest.mark.parametrize("orientation", [xted.ORIENT_RIGHT, xted.ORIENT_LEFT, xted.ORIENT_AUTO])
-@pytest.mark.parametrize("narrow_width,run_rows", [(0, 1), (7, 3), (32, 64), (256, 17), (256, 64)])
-def test_forced_granularities(orientation, narrow_width, run_rows):
-    """Every executor (warp-narrow of each width class, block-wide) and every
-    decomposition, forced, on the same random pairs."""
-    rng = random.Random(1000 * orientation + narrow_width + run_rows)
+@pytest.mark.parametrize("narrow_width,run_rows,half_width", [(0, 1, -1), (0, 5, 0), (7, 3, 100), (32, 64, 0),
+                                                              (256, 17, -1), (256, 64, 0)])
+def test_forced_granularities(orientation, narrow_width, run_rows, half_width):
+    """Every executor (warp-narrow of each width class, half-block, block-wide)
+    and every decomposition, forced, on the same random pairs."""
+    rng = random.Random(1000 * orientation + narrow_width + run_rows + half_width)
     pairs = []
     for _ in range(24):
         pairs.append((_rand_tree(rng, rng.choice([0, 1, 2, 5, 30, 90, 200, 420]), rng.randint(1, 6), rng.randrange(3)),
-                      _rand_tree(rng, rng.choice([1, 3, 8, 50, 130, 300, 700]), rng.randint(1, 6), rng.randrange(3))))
+                      _rand_tree(rng, rng.choice([1, 3, 8, 50, 130, 300, 700, 1100]), rng.randint(1, 6),
+                                 rng.randrange(3))))
     want = [oracle.distance(a, b) for a, b in pairs]
-    with xted.Context(orientation=orientation, narrow_width=narrow_width, run_rows=run_rows) as c:
+    with xted.Context(orientation=orientation, narrow_width=narrow_width, run_rows=run_rows,
+                      half_width=half_width) as c:
         got = c.distance_batch(pairs)
     assert list(got) == want
 

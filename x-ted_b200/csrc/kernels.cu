@@ -395,7 +395,10 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
 }
 
 // ---------------------------------------------------------------------------
-// Wide unit: the whole block, chunk width <= 256*W.
+// Group unit: G warps (a half block, G = 4, or the whole block, G = 8), chunk
+// width <= 32*G*W. The group's threads hold W consecutive columns each; a row
+// is a suffix scan within each warp, then across the group's warps through
+// shared memory, with the group's own named barrier.
 // ---------------------------------------------------------------------------
 struct WideShared {
     int wtot[XTED_WARPS];       // per-warp suffix minima of the current row
@@ -403,20 +406,34 @@ struct WideShared {
     int ends[XTED_WARPS];
 };
 
-template <int W>
-__device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
-                         int32_t *ring, int32_t *cache, int32_t *cnode) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+template <int G>
+__device__ __forceinline__ void group_sync(int gid) {
+    if (G == XTED_WARPS) {
+        __syncthreads();
+    } else {
+        // immediate barrier ids: the kernel then reserves only barriers 0-2
+        if (gid == 0) asm volatile("bar.sync 1, %0;" ::"n"(32 * G) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(32 * G) : "memory");
+    }
+}
+
+template <int W, int G>
+__device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
+                          int32_t *ring, int32_t *cache, int32_t *cnode, int gtid, int gid) {
+    constexpr int GROW = 256 * G + 8 * G;  // padded row of 256*G columns
+    constexpr int GSLOT = GROW + 8;        // ring slot: the row, then its record
+    const int lane = gtid & 31, warp = gtid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
-    const int c0 = tid * W;
+    const int c0 = gtid * W;
     const int stride = ch.width;
     const int width = ch.width;
     const int pbase = pad(c0);  // pad(c0 + k) == pbase + k for k < W (W divides 32)
     constexpr int PF = XTED_PREFETCH;
     const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
     Cols<W> C;
-    load_cols<W>(P, pr, ch, c0, C, XTED_WIDE_REG_MAX - 1);
+    load_cols<W>(P, pr, ch, c0, C, 256 * G - 1);
+    group_sync<G>(gid);  // the group's previous unit is done with cnode and S
 #pragma unroll
     for (int k = 0; k < W; k++)
         if ((C.valid >> k) & 1u) cnode[c0 + k] = C.node[k];
@@ -424,7 +441,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
         if (lane == 31) S.ends[warp] = incl;
-        __syncthreads();
+        group_sync<G>(gid);
         int before = incl - e;
         for (int w = 0; w < warp; w++) before += S.ends[w];
         set_keys<W>(C, c0, before);
@@ -441,36 +458,36 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k];
         int sp = 0, lo = 0;  // stack depth; lowest position held in the shared window
-        __syncthreads();  // the ring's and S.first's previous readers are done
+        group_sync<G>(gid);  // the ring's and S.first's previous readers are done
         if (lane == 0) S.first[warp] = prev[0];
-        if (tid == 0) S.first[XTED_WARPS] = 0;
+        if (gtid == 0) S.first[G] = 0;
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
             if (r >= i0)
-                issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, tid,
-                             XTED_CTA_THREADS, tid == 0);
+                issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                             gtid == 0);
             cp_async_commit();
         }
         cp_async_wait<PF - 2>();
-        __syncthreads();
+        group_sync<G>(gid);
         for (int i = imax - 1; i >= i0; i--) {
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * WIDE_SLOT, WIDE_ROW, tid,
-                                 XTED_CTA_THREADS, tid == 0);
+                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                                 gtid == 0);
                 cp_async_commit();
             }
-            const int32_t *slot = ring + (i & (PF - 1)) * WIDE_SLOT;
-            const int2 ri = *(const int2 *)(slot + WIDE_ROW);
+            const int32_t *slot = ring + (i & (PF - 1)) * GSLOT;
+            const int2 ri = *(const int2 *)(slot + GROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             int loc[W];
             int mine;
             if (!trow) {
-                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * WIDE_ROW;
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
                 mine = row_forest<W>(C, prev, slot + pbase, top, bord + 1, imax - ro - 1, loc);
             } else {
                 int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
@@ -479,10 +496,10 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             }
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
-            __syncthreads();
+            group_sync<G>(gid);
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
             if (lane == 31) carry = XTED_INF;
-            for (int w = warp + 1; w < XTED_WARPS; w++) carry = min(carry, S.wtot[w]);
+            for (int w = warp + 1; w < G; w++) carry = min(carry, S.wtot[w]);
             int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
             for (int k = 0; k < W; k++) prev[k] = min(loc[k], carry) - C.key[k];
@@ -496,7 +513,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (int64_t)(sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * WIDE_ROW + pbase;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * GROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = src[k];
@@ -505,7 +522,7 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < P.stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * WIDE_ROW + pbase;
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * GROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = prev[k];
@@ -515,14 +532,14 @@ __device__ void run_wide(const XKernelParams &P, const XPair &pr, const XUnit &u
                         for (int k = 0; k < W; k++)
                             if ((C.far >> k) & 1u) g[k] = prev[k];
                     }
-                } else if (tid == 0) {
+                } else if (gtid == 0) {
                     set_error(P, XTED_ENOMEM, 2, sp, P.stack_rows);
                 }
                 sp++;
                 if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
             }
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
-            __syncthreads();          // ... and everyone's, the record and the stack push
+            group_sync<G>(gid);       // ... and everyone's, the record and the stack push
         }
     }
     cp_async_wait<0>();
@@ -639,12 +656,24 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
 __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
                               WideShared &S, int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 256) run_wide<1>(P, pr, u, stk, S, ring, cache, cnode);
-    else if (width <= 512) run_wide<2>(P, pr, u, stk, S, ring, cache, cnode);
-    else if (width <= 1024) run_wide<4>(P, pr, u, stk, S, ring, cache, cnode);
-    else if (width <= XTED_WIDE_REG_MAX) run_wide<8>(P, pr, u, stk, S, ring, cache, cnode);
+    const int tid = threadIdx.x;
+    if (width <= 256) run_group<1, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (width <= 512) run_group<2, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (width <= 1024) run_group<4, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (width <= XTED_WIDE_REG_MAX) run_group<8, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
     else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S);
-    else if (threadIdx.x == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
+    else if (tid == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
+}
+
+// Half-block unit: group gid (warps 4*gid .. 4*gid+3), chunk width <= XTED_HALF_MAX.
+__device__ void dispatch_half(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
+                              int32_t *ring, int32_t *cache, int32_t *cnode, int gtid, int gid) {
+    const int width = P.chunks[u.chunk].width;
+    if (width <= 128) run_group<1, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (width <= 256) run_group<2, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (width <= 512) run_group<4, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (width <= XTED_HALF_MAX) run_group<8, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (gtid == 0) set_error(P, XTED_EINVAL, 6, width, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -804,8 +833,8 @@ __global__ void xted_rq_init_kernel(XKernelParams P) {
 }
 
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
-    __shared__ int s_task, s_entry, s_next, s_rec[2];
-    __shared__ WideShared S;
+    __shared__ int s_task, s_entry, s_next, s_rec[2], s_k[2];
+    __shared__ WideShared S[2];
     extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache | column nodes (DP_SMEM_BYTES)
     int32_t *s_ring = s_dyn;
     int32_t *s_cache = s_dyn + RING_INTS;
@@ -836,7 +865,23 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         const XPair pr = P.pairs[T.pair];
         if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
         if (T.kind_n & XTED_TASK_WIDE) {
-            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S, s_ring, s_cache, s_cnode);
+            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S[0], s_ring, s_cache, s_cnode);
+        } else if (T.kind_n & XTED_TASK_HALF) {
+            // the block's two halves take the task's units one at a time
+            const int nu = (int)(T.kind_n & 0xffff);
+            const int gid = warp >> 2, gtid = tid & 127;
+            int32_t *stk = scratch + (int64_t)gid * P.stack_rows * XTED_HALF_MAX;
+            int32_t *ring = s_ring + gid * (4 * XTED_PREFETCH * NARROW_SLOT);
+            int32_t *cache = s_cache + gid * (4 * XTED_STACK_CACHE * NARROW_ROW);
+            int32_t *cnode = s_cnode + gid * (4 * XTED_NARROW_MAX);
+            for (;;) {
+                if (gtid == 0) s_k[gid] = atomicAdd(&s_next, 1);
+                group_sync<4>(gid);
+                const int k = s_k[gid];
+                group_sync<4>(gid);  // every thread of the half has read s_k before its next claim
+                if (k >= nu) break;
+                dispatch_half(P, pr, P.units[T.unit_lo + k], stk, S[gid], ring, cache, cnode, gtid, gid);
+            }
         } else {
             // the block's warps take the task's units one at a time
             const int nu = (int)(T.kind_n & 0xffff);
@@ -868,7 +913,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
                     if (w > wmax) wmax = w;
                 }
                 P.trace[4 * (int64_t)t + 2] = global_ns();
-                P.trace[4 * (int64_t)t + 3] = ((T.kind_n & XTED_TASK_WIDE) ? 1ull : 0ull) |
+                P.trace[4 * (int64_t)t + 3] = ((T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) ? 1ull : 0ull) |
                                               ((unsigned long long)(nu & 127) << 1) |
                                               ((unsigned long long)(sm & 255) << 8) |
                                               ((wmax & 0xffff) << 16) | ((cells & 0xffffffffull) << 32);

@@ -38,9 +38,9 @@ struct DTree {
 struct DDepth {
     int32_t krd_lo, krd_hi;       // keyroots of this depth (pool indices, preorder)
     int32_t run_lo, run_hi;       // row runs
-    int32_t chunk_lo, nnarrow, nwide;  // chunks: narrow ones first, then wide ones
+    int32_t chunk_lo, nnarrow, nwide;  // chunks: narrow, then half-block, then whole-block ones
     int32_t maxrows, maxw_n, maxw_w;   // largest run and chunk widths (cost estimates)
-    int32_t pad0, pad1;
+    int32_t nhalf, maxw_h;
 };
 
 // One tree in one orientation (index 2 * tree + o; o = 1 mirrored).
@@ -63,7 +63,7 @@ struct DPair {
 
 struct DLevel {
     int32_t pair, level;
-    int32_t nwide, nnarrow;
+    int32_t nwide, nnarrow, nhalf;
     int32_t ntasks, entry;  // tasks at this level; this entry's index
     int32_t task_off, unit_off;
     int64_t key;            // estimate, then the earliest start of the level (see k_pair_rank)
@@ -84,6 +84,7 @@ struct PlanPools {
     DDepth *depths;       // capacity 2 * (sum n + ntrees)
     DOTree *otrees;
     int32_t run_rows, narrow_width;
+    int32_t half_width;   // chunks wider than narrow_width up to this run on half a block
 };
 
 XT_HD inline int32_t mirror_id(int32_t v, int32_t n, const int32_t *size, const int32_t *depth) {
@@ -131,6 +132,16 @@ XT_HD inline double row_cost_est(bool wide, int width) {
     if (width <= 0) return 0.0;
     if (!wide) return 2800.0 + 6.0 * width;
     return 1300.0 + 0.7 * width;
+}
+XT_HD inline double row_cost_half(int width) { return width <= 0 ? 0.0 : 1600.0 + 1.4 * width; }
+
+// Half-block units of one level are bundled into tasks of this many units
+// (the block's two halves claim them one at a time).
+XT_HD inline int32_t level_bundle_half(int64_t nhalf) {
+    int64_t b = (nhalf + 15) / 16;
+    if (b < 2) b = 2;
+    if (b > 8) b = 8;
+    return (int32_t)b;
 }
 
 // Narrow units of one level are bundled into tasks of this many units (the
@@ -226,6 +237,7 @@ XT_HD inline void orient_tree(const PlanPools &P, int ot) {
     // column-list positions, row runs and chunks per depth
     const int nw = P.narrow_width;
     const int group_w = nw > 0 ? nw : XTED_NARROW_MAX;
+    const int half_w = P.half_width > nw ? (P.half_width < XTED_HALF_MAX ? P.half_width : XTED_HALF_MAX) : nw;
     const int run_rows = P.run_rows;
     int32_t run_cur = O.node_base, chunk_cur = O.node_base;
     for (int d = 0; d <= D; d++) {
@@ -254,11 +266,11 @@ XT_HD inline void orient_tree(const PlanPools &P, int ot) {
             P.runs[run_cur++] = r;
         }
         dd.run_hi = run_cur;
-        // chunks: two passes, narrow chunks first
+        // chunks: three passes, narrow chunks first, then half-block ones, then whole-block ones
         dd.chunk_lo = chunk_cur;
-        dd.nnarrow = dd.nwide = 0;
-        dd.maxw_n = dd.maxw_w = 0;
-        for (int pass = 0; pass < 2; pass++) {
+        dd.nnarrow = dd.nwide = dd.nhalf = 0;
+        dd.maxw_n = dd.maxw_w = dd.maxw_h = 0;
+        for (int pass = 0; pass < 3; pass++) {
             XChunk c{-1, 0, d, 0};
             for (int32_t k = dd.krd_lo; k <= dd.krd_hi; k++) {
                 int32_t w = 0;
@@ -268,12 +280,15 @@ XT_HD inline void orient_tree(const PlanPools &P, int ot) {
                 }
                 const bool flush = c.nseg > 0 && (k == dd.krd_hi || c.width + w > group_w);
                 if (flush) {
-                    const bool wide = c.width > nw;
-                    if (wide == (pass == 1)) {
+                    const int kind = c.width <= nw ? 0 : (c.width <= half_w ? 1 : 2);
+                    if (kind == pass) {
                         P.chunks[chunk_cur++] = c;
-                        if (wide) {
+                        if (kind == 2) {
                             dd.nwide++;
                             if (c.width > dd.maxw_w) dd.maxw_w = c.width;
+                        } else if (kind == 1) {
+                            dd.nhalf++;
+                            if (c.width > dd.maxw_h) dd.maxw_h = c.width;
                         } else {
                             dd.nnarrow++;
                             if (c.width > dd.maxw_n) dd.maxw_n = c.width;
@@ -287,6 +302,7 @@ XT_HD inline void orient_tree(const PlanPools &P, int ot) {
                 c.nseg += 1;
             }
         }
+        if (dd.maxw_h > O.maxw_wide) O.maxw_wide = dd.maxw_h;
         if (dd.maxw_w > O.maxw_wide) O.maxw_wide = dd.maxw_w;
     }
     P.otrees[ot] = O;
@@ -338,7 +354,7 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
-    int64_t wide = 0, narrow = 0;
+    int64_t wide = 0, narrow = 0, half = 0;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
     int32_t small_max[64];  // longest non-big run per depth (the first 64 depths; more use maxrows)
     for (int al = lo; al <= hi; al++) {
@@ -353,10 +369,13 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
             }
         if (al - lo < 64) small_max[al - lo] = sm;
         wide += nr * cb.nwide + nbig * cb.nnarrow;
+        half += nr * cb.nhalf;
         narrow += (nr - nbig) * cb.nnarrow;
     }
     const int32_t bundle = level_bundle(narrow);
     const int rounds = (bundle + XTED_WARPS - 1) / XTED_WARPS;  // units a warp runs in one task
+    const int32_t bundle_h = level_bundle_half(half);
+    const int rounds_h = (bundle_h + 1) / 2;                     // units a half block runs in one task
     // the level's longest task: its largest run against its widest chunk
     double est = 0.0;
     for (int al = lo; al <= hi; al++) {
@@ -370,6 +389,10 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
                 if (eb > e) e = eb;
             }
         }
+        if (cb.nhalf > 0) {
+            const double eh = rounds_h * ra.maxrows * row_cost_half(cb.maxw_h);
+            if (eh > e) e = eh;
+        }
         if (cb.nwide > 0) {
             const double ew = ra.maxrows * row_cost_est(true, cb.maxw_w);
             if (ew > e) e = ew;
@@ -378,7 +401,8 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     }
     E.nwide = (int32_t)wide;
     E.nnarrow = (int32_t)narrow;
-    E.ntasks = (int32_t)(wide + (narrow + bundle - 1) / bundle);
+    E.nhalf = (int32_t)half;
+    E.ntasks = (int32_t)(wide + (narrow + bundle - 1) / bundle + (half + bundle_h - 1) / bundle_h);
     *est_out = est;
 }
 
@@ -424,12 +448,33 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
         }
     }
     if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, (uint32_t)bundle, bundle_lo};
+    const int32_t per_half = level_bundle_half(E.nhalf);
+    bundle = 0;
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
-            const bool big = big_run(C, r);
-            const int32_t c_lo = big ? cb.chunk_lo : cb.chunk_lo + cb.nnarrow;
-            for (int32_t c = c_lo; c < cb.chunk_lo + cb.nnarrow + cb.nwide; c++) {
+            for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nhalf; c++) {
+                if (bundle == 0) bundle_lo = u;
+                units[u++] = XUnit{r, c};
+                if (++bundle == per_half) {
+                    tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_HALF | (uint32_t)bundle, bundle_lo};
+                    bundle = 0;
+                }
+            }
+        }
+    }
+    if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_HALF | (uint32_t)bundle, bundle_lo};
+    for (int al = lo; al <= hi; al++) {
+        const DDepth &ra = da[al], &cb = db[d - al];
+        const int32_t cw_lo = cb.chunk_lo + cb.nnarrow + cb.nhalf, cw_hi = cw_lo + cb.nwide;
+        for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            if (big_run(C, r))
+                for (int32_t c = cb.chunk_lo; c < cb.chunk_lo + cb.nnarrow; c++) {
+                    units[u] = XUnit{r, c};
+                    tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
+                    u++;
+                }
+            for (int32_t c = cw_lo; c < cw_hi; c++) {
                 units[u] = XUnit{r, c};
                 tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
                 u++;

@@ -122,7 +122,7 @@ __global__ void k_level_count(LevelCtx C, DLevel *lv, int64_t nent, int64_t *uni
     level_count(C, E, &est);
     E.key = (int64_t)(est / 64.0) + 1;  // >= 1: strictly decreasing ranks below
     lv[e] = E;
-    units[e] = (int64_t)E.nwide + E.nnarrow;
+    units[e] = (int64_t)E.nwide + E.nnarrow + E.nhalf;
     tasks[e] = E.ntasks;
 }
 
@@ -318,6 +318,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     P.otrees = cv.take<DOTree>(2 * (size_t)T);
     P.run_rows = c->opts.run_rows;
     P.narrow_width = c->opts.narrow_width;
+    P.half_width = c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width;
     DPair *d_pairs = cv.take<DPair>((size_t)npairs);
     XPair *d_xpairs = cv.take<XPair>((size_t)npairs);
     int32_t *d_trivial = cv.take<int32_t>((size_t)npairs);

@@ -501,7 +501,8 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     const int64_t Nall = N + (int64_t)S * Qm;
     if (2 * Nall + 2 * (int64_t)(T + S) >= INT32_MAX / 2 || (int64_t)S * T >= INT32_MAX / 2) return XTED_ENOMEM;
     s->Nc_nonempty = nonempty;
-    serve_pools_build(s->pools, tr, T, S, Qm, c->opts.run_rows, c->opts.narrow_width);
+    serve_pools_build(s->pools, tr, T, S, Qm, c->opts.run_rows, c->opts.narrow_width,
+                      c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width);
     const ServePools &H = s->pools;
     const size_t n2 = H.node.size();
     // device memory

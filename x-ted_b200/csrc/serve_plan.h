@@ -49,7 +49,7 @@ struct QPlan {
 
 // Lays out the pools and plans the corpus. The trees must be valid.
 inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, int Qmax, int run_rows,
-                              int narrow_width) {
+                              int narrow_width, int half_width) {
     s.T = T;
     s.S = S;
     s.Qmax = Qmax;
@@ -121,6 +121,7 @@ inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, 
     P.otrees = s.otrees.data();
     P.run_rows = run_rows;
     P.narrow_width = narrow_width;
+    P.half_width = half_width;
     s.stack_rows = 1;
     for (int t = 0; t < T; t++) {
         tree_basic(P, t, s.trees.data());
@@ -200,7 +201,7 @@ inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const 
         lv[e].unit_off = (int32_t)nu;
         lv[e].task_off = (int32_t)nt;
         lv[e].entry = (int32_t)e;
-        nu += (int64_t)lv[e].nwide + lv[e].nnarrow;
+        nu += (int64_t)lv[e].nwide + lv[e].nnarrow + lv[e].nhalf;
         nt += lv[e].ntasks;
     }
     out.units.resize((size_t)nu);

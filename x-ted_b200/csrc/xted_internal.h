@@ -73,7 +73,10 @@ struct XUnit {
     int32_t chunk; // global chunk index (column tree)
 };
 
-#define XTED_TASK_WIDE 0x80000000u
+#define XTED_TASK_WIDE 0x80000000u  // one unit run by the whole block
+#define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
+#define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
+#define XTED_HALF_DEFAULT 512       // default limit: wider chunks run faster on the whole block
 #define XTED_TASK_UNITS 32   // narrow units per task (claimed by the block's warps dynamically)
 #define XTED_PREFETCH 4      // rows of tree distances in flight per unit (cp.async ring depth)
 
