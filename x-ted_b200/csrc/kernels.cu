@@ -724,14 +724,34 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 // next task of the entry at the bucket's head, and whoever finds that entry
 // exhausted moves the head on. Idle polling is bounded by time and by
 // iterations.
+// Serving: rq_ctl words after the done counter.
+#define CTL_IDLE (2 * XTED_BUCKETS + 1)     // blocks currently idle (or gone)
+#define CTL_LEAVING (2 * XTED_BUCKETS + 2)  // nonzero once blocks have started to leave
+
 __device__ int claim_task(const XKernelParams &P, int *entry) {
     volatile int32_t *ctl = P.rq_ctl;
     volatile int32_t *state = P.entry_state;
     volatile int32_t *mbox = P.mbox;
     unsigned ns = 32;
     uint64_t t0 = 0;
+    bool idle_counted = false;  // serving: this block is counted in CTL_IDLE
     for (long it = 0; it < (1L << 28); it++) {
         if (*(volatile int32_t *)P.error != 0) return CLAIM_EXIT;
+        if (P.serve) {
+            // admit posted queries first: their level-0 entries go to the new
+            // query's own (least urgent) bucket, and a busy launch would
+            // otherwise only look at the mailbox once it ran out of work
+            int cons = mbox[XTED_MBOX_CONSUMED];
+            while (cons < mbox[XTED_MBOX_POSTED]) {
+                if (atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons + 1) == cons) {
+                    __threadfence();  // acquire: the record and its query's plan are visible from here on
+                    if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
+                    *entry = cons;
+                    return CLAIM_RECORD;
+                }
+                cons = mbox[XTED_MBOX_CONSUMED];
+            }
+        }
         const int top = P.serve ? mbox[XTED_MBOX_TOP] : XTED_BUCKETS - 1;
         for (int i = 0; i < XTED_BUCKETS; i++) {
             const int b = (top - i) & (XTED_BUCKETS - 1);
@@ -745,6 +765,7 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
                     const int k = atomicAdd(&P.entry_state[2 * e], 1);
                     if (k < X.ntasks) {
                         __threadfence();  // acquire: the level's inputs are visible from here on
+                        if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
                         *entry = e;
                         return X.task_off + k;
                     }
@@ -753,16 +774,15 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
             }
         }
         if (P.serve) {
-            int cons = mbox[XTED_MBOX_CONSUMED];
-            while (cons < mbox[XTED_MBOX_POSTED]) {
-                if (atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons + 1) == cons) {
-                    __threadfence();  // acquire: the record and its query's plan are visible from here on
-                    *entry = cons;
-                    return CLAIM_RECORD;
-                }
-                cons = mbox[XTED_MBOX_CONSUMED];
+            // A block leaves a serving launch only once every block has been
+            // idle (then the others follow as soon as they are idle too), so
+            // the launch never runs on a few blocks while work arrives; the
+            // host relaunches when the last one is gone and work is posted.
+            if (!idle_counted) {
+                atomicAdd(&P.rq_ctl[CTL_IDLE], 1);
+                idle_counted = true;
             }
-            if (mbox[XTED_MBOX_STOP] != 0) return CLAIM_EXIT;
+            if (mbox[XTED_MBOX_STOP] != 0 || ctl[CTL_LEAVING] != 0) return CLAIM_EXIT;
         } else if (ld_acquire(P.done_total) >= P.ntasks) {
             return CLAIM_EXIT;
         }
@@ -770,7 +790,10 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
         if (t0 == 0) {
             t0 = now;
         } else if (P.serve) {
-            if (now - t0 > P.idle_exit_ns) return CLAIM_EXIT;  // idle: the host relaunches on new work
+            if (now - t0 > P.idle_exit_ns && ctl[CTL_IDLE] >= (int)gridDim.x) {
+                atomicExch(&P.rq_ctl[CTL_LEAVING], 1);
+                return CLAIM_EXIT;  // idle everywhere: the host relaunches on new work
+            }
         } else if (now - t0 > P.timeout_ns) {
             set_error(P, XTED_ETIMEOUT, 0, 0, 0);
             return CLAIM_EXIT;
@@ -785,7 +808,7 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
 // A serving pair is finished: its distance goes to the host-visible result
 // array, and the last pair of a query raises the slot's flag to the query's
 // generation (the host polls it).
-__device__ void finish_served_pair(const XKernelParams &P, int pair) {
+__device__ void finish_served_pair(const XKernelParams &P, int pair, int bucket) {
     const int d = __ldcg(P.dt + __ldcg(&P.pairs[pair].dt_off));
     ((volatile int32_t *)P.results)[pair] = d;
     __threadfence_system();
@@ -793,6 +816,18 @@ __device__ void finish_served_pair(const XKernelParams &P, int pair) {
     const int n = atomicAdd(&P.slot_done[s], 1) + 1;
     if (n == __ldcg(&P.slot_need[s])) {
         P.slot_done[s] = 0;
+        // Every position left in the query's bucket names one of its own,
+        // now exhausted, entries (a bucket serves one query at a time). Move
+        // the head past them before the host may hand those entry ids to a
+        // new query: a claimer must never find an old position whose entry
+        // id has been reused.
+        volatile int32_t *ctl = P.rq_ctl + 2 * bucket;
+        const unsigned tl = (unsigned)ctl[1];
+        for (int g = 0; g < 1024; g++) {
+            const unsigned h = (unsigned)ctl[0];
+            if ((int)(tl - h) <= 0) break;
+            atomicCAS((int32_t *)&P.rq_ctl[2 * bucket], (int)h, (int)tl);
+        }
         __threadfence_system();
         ((volatile int32_t *)P.flags)[s] = __ldcg(&P.slot_gen[s]);
     }
@@ -804,7 +839,7 @@ __device__ void complete_task(const XKernelParams &P, int e, int pair) {
     const int done = atomicAdd(&P.entry_state[2 * e + 1], 1) + 1;
     if (done == X.ntasks) {
         __threadfence();  // acquire the level's other tasks, release to the next level's claimers
-        if (!rq_publish(P, X.next) && P.serve) finish_served_pair(P, pair);
+        if (!rq_publish(P, X.next) && P.serve) finish_served_pair(P, pair, X.bucket);
     }
     __threadfence();
     atomicAdd(P.done_total, 1);

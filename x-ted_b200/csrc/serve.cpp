@@ -61,25 +61,51 @@ double now_ms() {
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
-// First-fit allocator over [0, cap) (elements).
+// Allocator over [0, cap) (elements): first fit, or next fit from a cursor
+// that follows the last allocation (freed ranges are then reused only after
+// the cursor has gone round the whole pool).
 class Extents {
 public:
-    void reset(int64_t cap) {
+    void reset(int64_t cap, bool next_fit = false) {
         free_.clear();
         if (cap > 0) free_[0] = cap;
         cap_ = cap;
+        next_fit_ = next_fit;
+        cursor_ = 0;
     }
     int64_t cap() const { return cap_; }
     bool alloc(int64_t n, int64_t *off) {
         n = std::max<int64_t>(n, 1);
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < n) continue;
-            *off = it->first;
-            const int64_t rest = it->second - n, o2 = it->first + n;
+        auto take = [&](std::map<int64_t, int64_t>::iterator it, int64_t at) {
+            // [at, at + n) lies inside the free range it
+            const int64_t lo = it->first, len = it->second;
             free_.erase(it);
-            if (rest > 0) free_[o2] = rest;
-            return true;
+            if (at > lo) free_[lo] = at - lo;
+            if (lo + len > at + n) free_[at + n] = lo + len - (at + n);
+            *off = at;
+            cursor_ = at + n;
+        };
+        if (next_fit_) {
+            // a free range holding the cursor, then ranges after it, then from the start
+            auto it = free_.upper_bound(cursor_);
+            if (it != free_.begin()) {
+                auto pv = std::prev(it);
+                if (pv->first + pv->second >= cursor_ + n) {
+                    take(pv, std::max(pv->first, cursor_));
+                    return true;
+                }
+            }
+            for (auto jt = it; jt != free_.end(); ++jt)
+                if (jt->second >= n) {
+                    take(jt, jt->first);
+                    return true;
+                }
         }
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= n) {
+                take(it, it->first);
+                return true;
+            }
         return false;
     }
     void release(int64_t off, int64_t n) {
@@ -101,7 +127,8 @@ public:
 
 private:
     std::map<int64_t, int64_t> free_;
-    int64_t cap_ = 0;
+    int64_t cap_ = 0, cursor_ = 0;
+    bool next_fit_ = false;
 };
 
 struct Query {
@@ -566,7 +593,7 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     s->dt_ext.reset(dt_cap);
     s->u_ext.reset(kUnitCap);
     s->t_ext.reset(kTaskCap);
-    s->e_ext.reset(kEntryCap);
+    s->e_ext.reset(kEntryCap, true);  // entry ids: reused as late as possible
     XKernelParams &K = s->K;
     std::memset(&K, 0, sizeof(K));
     K.rowinfo = s->d_node;
