@@ -455,6 +455,7 @@ def main():
         "gpu_launches": 3 * args.steps,  # ready-queue init, DP, gather per step
         "clocks": clk.summary(),
         "tasks": st["tasks"], "units": st["units"], "grid": st["grid"], "host_plan_ms": round(plan_ms, 2),
+        "cuda_graph": bool(st["graph"]),  # the timed steps replayed the step's captured CUDA graph
     }
     print(json.dumps(res), flush=True)
 

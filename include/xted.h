@@ -96,6 +96,8 @@ typedef struct xted_stats {
     int32_t levels_max;     /* deepest keyroot-level count of any pair        */
     int32_t grid;           /* persistent blocks launched                    */
     double dp_ms;           /* device time of the DP kernel alone            */
+    int32_t graph;          /* 1 if the step replayed its captured CUDA graph */
+    int32_t pad;
 } xted_stats;
 
 void xted_opts_default(xted_opts *opts);

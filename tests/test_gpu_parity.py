@@ -154,12 +154,25 @@ def test_single_pair_1000_mixed_shapes(ctx):
 
 
 def test_prepared_batch_repeatable(ctx):
+    """Repeated runs of one prepared batch: the first is enqueued call by call,
+    later ones replay the step's captured CUDA graph; all give the oracle's
+    distances. A new prepare drops the old graph."""
     pairs = gen.mixed_batch(48, seed=5, hi=400)
+    want = oracle.distance_batch(pairs, nthreads=8)
     ctx.prepare_batch(pairs)
     r1 = ctx.run_prepared()
-    r2 = ctx.run_prepared()
-    assert np.array_equal(r1, r2)
-    assert np.array_equal(r1, oracle.distance_batch(pairs, nthreads=8))
+    assert ctx.stats()["graph"] == 0
+    for _ in range(3):
+        r2 = ctx.run_prepared()
+        assert ctx.stats()["graph"] == 1
+        assert np.array_equal(r1, r2)
+    assert np.array_equal(r1, want)
+    other = gen.mixed_batch(20, seed=6, hi=300)
+    ctx.prepare_batch(other)
+    for k in range(3):
+        got = ctx.run_prepared()
+        assert ctx.stats()["graph"] == (0 if k == 0 else 1)
+        assert np.array_equal(got, oracle.distance_batch(other, nthreads=8))
 
 
 def test_large_pair_properties(ctx):

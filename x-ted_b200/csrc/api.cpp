@@ -91,6 +91,7 @@ int ctx_host_reserve(HostBuf &b, size_t bytes) {
 // repeatedly from device-resident inputs.
 int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs) {
     c->prepared = false;
+    ctx_drop_graph(c);  // the graph holds the previous plan's buffers and sizes
     XKernelParams &K = c->kp;
     int rc = dev_plan(c, a, b, npairs, K);
     if (rc) return rc;
@@ -134,15 +135,17 @@ int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npa
 
 // Runs the prepared plan: counter reset, the persistent DP launch, the
 // gather, and the copy of results + error word to pinned memory. Synchronous.
-int ctx_run(xted_ctx *c, int32_t *out) {
-    if (!c->prepared) return XTED_EINVAL;
+// One step of the prepared plan, enqueued on the context's stream: counter
+// reset, the ready queue's level 0, the persistent DP launch, the gather, and
+// the copy of results + error word to pinned memory.
+static int enqueue_step(xted_ctx *c, bool events) {
     const XKernelParams &K = c->kp;
     const int npairs = c->npairs;
     int32_t *cnt = (int32_t *)c->counters.p;
     int32_t *d_out = cnt + 8 + npairs;
     int32_t *hres = (int32_t *)c->result.p;
     const size_t res_bytes = (size_t)npairs * sizeof(int32_t);
-    cudaEventRecord(c->ev0, c->stream);
+    if (events && cudaEventRecord(c->ev0, c->stream) != cudaSuccess) return XTED_ECUDA;
     // per-run reset of the error words and the ready queue, then level 0 of every pair
     const size_t ne = (size_t)K.nentries;
     if (cudaMemsetAsync(cnt, 0, 8 * sizeof(int32_t), c->stream) != cudaSuccess ||
@@ -153,20 +156,76 @@ int ctx_run(xted_ctx *c, int32_t *out) {
           cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_BUCKETS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
           launch_rq_init(K, c->stream) != cudaSuccess)))
         return XTED_ECUDA;
-    cudaEventRecord(c->evk0, c->stream);
-    if (K.ntasks > 0) {
-        cudaError_t e = launch_dp(K, c->grid, c->stream);
-        if (e != cudaSuccess) {
+    if (events && cudaEventRecord(c->evk0, c->stream) != cudaSuccess) return XTED_ECUDA;
+    if (K.ntasks > 0 && launch_dp(K, c->grid, c->stream) != cudaSuccess) return XTED_ECUDA;
+    if (events && cudaEventRecord(c->evk1, c->stream) != cudaSuccess) return XTED_ECUDA;
+    if (launch_gather(K.pairs, c->d_trivial, K.dt, npairs, d_out, c->stream) != cudaSuccess)
+        return XTED_ECUDA;
+    if ((events && cudaEventRecord(c->ev1, c->stream) != cudaSuccess) ||
+        cudaMemcpyAsync(hres, cnt, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        (npairs && cudaMemcpyAsync(hres + 8, d_out, res_bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess))
+        return XTED_ECUDA;
+    return XTED_OK;
+}
+
+void ctx_drop_graph(xted_ctx *c) {
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+    c->runs_prepared = 0;
+}
+
+// Captures the step into a graph; false (and no graph is tried again for this
+// context) if the runtime refuses any part of it.
+static bool capture_step(xted_ctx *c) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const int rc = enqueue_step(c, false);  // events recorded inside a graph cannot be timed
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    bool ok = rc == XTED_OK && e == cudaSuccess && g != nullptr &&
+              cudaGraphInstantiate(&c->step_graph, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+        cudaGetLastError();
+        c->step_graph = nullptr;
+    }
+    return ok;
+}
+
+// Runs the prepared plan. Synchronous. With allow_graph, the second and later
+// runs of one prepared plan replay a CUDA graph of the step (one launch of
+// the whole sequence instead of eleven enqueues).
+int ctx_run(xted_ctx *c, int32_t *out, bool allow_graph) {
+    if (!c->prepared) return XTED_EINVAL;
+    const XKernelParams &K = c->kp;
+    const int npairs = c->npairs;
+    int32_t *hres = (int32_t *)c->result.p;
+    const size_t res_bytes = (size_t)npairs * sizeof(int32_t);
+    bool replay = false;
+    if (allow_graph && !K.trace && !c->graph_failed && c->runs_prepared >= 1) {
+        if (!c->step_graph && !capture_step(c)) c->graph_failed = true;
+        replay = c->step_graph != nullptr;
+    }
+    c->runs_prepared++;
+    if (replay) {
+        // timed from outside: the DP time of a replay includes the step's
+        // small kernels (ready-queue init and gather, a few microseconds)
+        if (cudaEventRecord(c->ev0, c->stream) != cudaSuccess || cudaEventRecord(c->evk0, c->stream) != cudaSuccess ||
+            cudaGraphLaunch(c->step_graph, c->stream) != cudaSuccess ||
+            cudaEventRecord(c->evk1, c->stream) != cudaSuccess || cudaEventRecord(c->ev1, c->stream) != cudaSuccess) {
             cudaGetLastError();
             return XTED_ECUDA;
         }
+    } else {
+        const int rc = enqueue_step(c, true);
+        if (rc) {
+            cudaGetLastError();
+            return rc;
+        }
     }
-    cudaEventRecord(c->evk1, c->stream);
-    if (launch_gather(K.pairs, c->d_trivial, K.dt, npairs, d_out, c->stream) != cudaSuccess)
-        return XTED_ECUDA;
-    cudaEventRecord(c->ev1, c->stream);
-    cudaMemcpyAsync(hres, cnt, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
-    if (npairs) cudaMemcpyAsync(hres + 8, d_out, res_bytes, cudaMemcpyDeviceToHost, c->stream);
+    c->stats.graph = replay ? 1 : 0;
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
         cudaGetLastError();
         return XTED_ECUDA;
@@ -174,6 +233,7 @@ int ctx_run(xted_ctx *c, int32_t *out) {
     float ms = 0.f, kms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     cudaEventElapsedTime(&kms, c->evk0, c->evk1);
+    cudaGetLastError();  // a failed timing read must not surface in a later call
     c->stats.device_ms = ms;
     c->stats.dp_ms = kms;
     c->stats.h2d_bytes = c->h2d_bytes;
@@ -296,6 +356,7 @@ int xted_destroy(xted_ctx *c) {
     cudaSetDevice(c->opts.device);
     xted::serve_shutdown(c);
     cudaStreamSynchronize(c->stream);
+    ctx_drop_graph(c);
     for (DevBuf *b : {&c->meta, &c->levels, &c->work, &c->dt, &c->scratch, &c->counters, &c->trace})
         if (b->p) cudaFree(b->p);
     for (HostBuf *b : {&c->stage, &c->result, &c->summary})
@@ -316,7 +377,7 @@ int xted_distance_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int
     const double t1 = now_ms();
     std::memset(&c->stats, 0, sizeof(c->stats));
     if (rc) return rc;
-    rc = ctx_run(c, out);
+    rc = ctx_run(c, out, false);
     fill_stats(c, t1 - t0);
     c->stats.total_ms = now_ms() - t0;
     return rc;
@@ -337,7 +398,7 @@ int xted_prepare_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int3
 int xted_run_prepared(xted_ctx *c, int32_t *out) {
     if (!c || !out) return XTED_EINVAL;
     if (cudaSetDevice(c->opts.device) != cudaSuccess) return XTED_ECUDA;
-    const int rc = ctx_run(c, out);
+    const int rc = ctx_run(c, out, true);
     fill_stats(c, c->prep_ms);
     return rc;
 }

@@ -55,6 +55,10 @@ struct xted_ctx {
     int64_t h2d_bytes = 0;
     double prep_ms = 0;
     bool prepared = false;
+    // the prepared step captured as a CUDA graph (from its second run on)
+    cudaGraphExec_t step_graph = nullptr;
+    int32_t runs_prepared = 0;
+    bool graph_failed = false;
 };
 
 namespace xted {
@@ -63,7 +67,8 @@ int ctx_dev_reserve(xted_ctx *c, DevBuf &b, size_t bytes);
 int ctx_host_reserve(HostBuf &b, size_t bytes);
 int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs);
 int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs, XKernelParams &K);
-int ctx_run(xted_ctx *c, int32_t *out);
+int ctx_run(xted_ctx *c, int32_t *out, bool allow_graph);
+void ctx_drop_graph(xted_ctx *c);
 void fill_stats(xted_ctx *c, double plan_ms);
 void serve_shutdown(xted_ctx *c);
 

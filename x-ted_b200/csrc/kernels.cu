@@ -974,11 +974,22 @@ int dp_occupancy(int *blocks_per_sm) {
                                                                DP_SMEM_BYTES);
 }
 
+// Cooperative launch (every block resident at once), expressed as a launch
+// attribute so that the same call also records into a CUDA graph.
 cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
     XKernelParams p = P;
     void *args[] = {&p};
-    return cudaLaunchCooperativeKernel((const void *)xted_dp_kernel, dim3(grid), dim3(XTED_CTA_THREADS), args,
-                                       DP_SMEM_BYTES, s);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(XTED_CTA_THREADS);
+    cfg.dynamicSmemBytes = DP_SMEM_BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, (const void *)xted_dp_kernel, args);
 }
 
 cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s) {

@@ -49,7 +49,8 @@ class CStats(ctypes.Structure):
                 ("tasks", ctypes.c_int64), ("units", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64), ("host_plan_ms", ctypes.c_double),
                 ("device_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
-                ("levels_max", ctypes.c_int32), ("grid", ctypes.c_int32), ("dp_ms", ctypes.c_double)]
+                ("levels_max", ctypes.c_int32), ("grid", ctypes.c_int32), ("dp_ms", ctypes.c_double),
+                ("graph", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
