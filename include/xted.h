@@ -74,7 +74,10 @@ typedef struct xted_opts {
                                width (at most 1024) run on half a block, two
                                at a time; 0 = 512 (fastest on the mixed
                                batch), < 0: none                            */
-    int32_t reserved;
+    int32_t tuned;          /* nonzero (default): run_rows, narrow_width and
+                               half_width come per tree from the autotuned
+                               size-bucket table; 0: the fields above apply
+                               to every tree                                */
     double wait_timeout_s;  /* bound on every device-side wait              */
     int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
 } xted_opts;

@@ -41,6 +41,8 @@ struct HostPlan {
     int stack_rows = 1;
 };
 
+static bool g_table = false;
+
 static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<std::vector<int32_t>> &O,
                  const std::vector<std::vector<int32_t>> &I, const std::vector<int> &nn,
                  const std::vector<int32_t> &pair_trees, int orientation, int narrow_width, int run_rows,
@@ -95,6 +97,12 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     P.run_rows = run_rows;
     P.narrow_width = narrow_width;
     P.half_width = half_width;
+    P.ntune = 0;
+    if (g_table) {  // per tree-size granularity, as the autotuned table gives it
+        P.tune[P.ntune++] = XTuneRow{40, 5, 32, 100};
+        P.tune[P.ntune++] = XTuneRow{150, 64, 7, -1};
+        P.tune[P.ntune++] = XTuneRow{1 << 30, 17, 256, 512};
+    }
     for (int t = 0; t < T; t++) tree_basic(P, t, H.trees.data());
     for (int o = 0; o < 2 * T; o++) orient_tree(P, o);
     const int np = (int)pair_trees.size() / 2;
@@ -209,6 +217,7 @@ int main(int argc, char **argv) {
         const int wr = wrs[(it / 4) % 4];
         const int hws[3] = {XTED_HALF_MAX, -1, 100};
         const int hw = hws[(it / 16) % 3];
+        g_table = it % 5 == 4;
         HostPlan H;
         plan(L, O, I, nn, pt, orient, nw, rr, wr, hw, H);
         int64_t dts = 0;
@@ -241,7 +250,7 @@ int main(int argc, char **argv) {
                 const bool full = (t.kind_n & XTED_TASK_WIDE) != 0, half = (t.kind_n & XTED_TASK_HALF) != 0;
                 const bool wide = full || half;
                 if (nu < 1 || nu > XTED_TASK_UNITS || (full && nu != 1) || (half && nu > 8)) FAIL("bad unit count %d", nu);
-                for (int u = 0; u < nu; u++) {
+                for (int u = 0; u < nu && !g_table; u++) {
                     const int w = H.chunks[(size_t)H.units[(size_t)(t.unit_lo + u)].chunk].width;
                     if (half && (w <= nw || w > XTED_HALF_MAX || w > hw)) FAIL("half unit of width %d", w);
                     if (full && w <= XTED_HALF_MAX && w > nw && hw >= w) FAIL("whole-block unit of width %d", w);
@@ -257,7 +266,7 @@ int main(int argc, char **argv) {
                                     H.stack_rows};
                 for (int u = 0; u < nu; u++) {
                     unit_seen[(size_t)(t.unit_lo + u)]++;
-                    emu::run_unit(EP, x, H.units[(size_t)(t.unit_lo + u)], dt, nw, wide);
+                    emu::run_unit(EP, x, H.units[(size_t)(t.unit_lo + u)], dt, g_table ? XTED_NARROW_MAX : nw, wide);
                 }
             }
             level_done[(size_t)E.pair] = E.level;

@@ -141,3 +141,15 @@ def test_serving_planner_emulation_matches_oracle(tmp_path):
         r = subprocess.run([str(exe), "12", "150", seed], capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout + r.stderr
         assert r.stdout.startswith("ok")
+
+
+def test_tune_table_well_formed():
+    """The autotuned per-size table the library compiles in: sizes ascending,
+    the last row open-ended, every value inside the planner's limits."""
+    src = open(os.path.join(REPO, "x-ted_b200", "csrc", "tune_table.h")).read()
+    rows = re.findall(r"\{\s*([0-9<\s]+),\s*(-?\d+),\s*(-?\d+),\s*(-?\d+)\s*\}", src)
+    assert rows
+    max_n = [eval(r[0]) for r in rows]  # noqa: S307 -- integer literals and shifts from the generated header
+    assert max_n == sorted(max_n) and max_n[-1] >= 1 << 30
+    for _, rr, nw, hw in rows:
+        assert 1 <= int(rr) <= 4096 and 0 <= int(nw) <= 256 and int(hw) <= 1024

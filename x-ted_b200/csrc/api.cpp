@@ -294,6 +294,7 @@ void xted_opts_default(xted_opts *o) {
     o->ctas_per_sm = 0;
     o->wide_rows = 0;
     o->half_width = 0;
+    o->tuned = 1;
     o->wait_timeout_s = 20.0;
     o->mem_limit = 0;
 }

@@ -85,7 +85,24 @@ struct PlanPools {
     DOTree *otrees;
     int32_t run_rows, narrow_width;
     int32_t half_width;   // chunks wider than narrow_width up to this run on half a block
+    // per tree-size bucket granularity (autotuned); ntune == 0: the three fields above
+    int32_t ntune;
+    XTuneRow tune[XTED_TUNE_ROWS];
 };
+
+// The granularity a tree of n nodes is planned with.
+XT_HD inline void tree_granularity(const PlanPools &P, int n, int *run_rows, int *narrow_width, int *half_width) {
+    *run_rows = P.run_rows;
+    *narrow_width = P.narrow_width;
+    *half_width = P.half_width;
+    for (int k = 0; k < P.ntune; k++)
+        if (n < P.tune[k].max_n || k == P.ntune - 1) {
+            *run_rows = P.tune[k].run_rows;
+            *narrow_width = P.tune[k].narrow_width;
+            *half_width = P.tune[k].half_width;
+            return;
+        }
+}
 
 XT_HD inline int32_t mirror_id(int32_t v, int32_t n, const int32_t *size, const int32_t *depth) {
     return n - 1 - (v - depth[v] + size[v] - 1);
@@ -235,10 +252,10 @@ XT_HD inline void orient_tree(const PlanPools &P, int ot) {
     for (int u = 0; u < n; u++)
         if (okd[u] >= 0) P.krd[dep[okd[u]].krd_hi++] = u;
     // column-list positions, row runs and chunks per depth
-    const int nw = P.narrow_width;
+    int run_rows, nw, hw;
+    tree_granularity(P, n, &run_rows, &nw, &hw);
     const int group_w = nw > 0 ? nw : XTED_NARROW_MAX;
-    const int half_w = P.half_width > nw ? (P.half_width < XTED_HALF_MAX ? P.half_width : XTED_HALF_MAX) : nw;
-    const int run_rows = P.run_rows;
+    const int half_w = hw > nw ? (hw < XTED_HALF_MAX ? hw : XTED_HALF_MAX) : nw;
     int32_t run_cur = O.node_base, chunk_cur = O.node_base;
     for (int d = 0; d <= D; d++) {
         DDepth &dd = dep[d];

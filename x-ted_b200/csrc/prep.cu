@@ -23,6 +23,7 @@
 
 #include "ctx.h"
 #include "plan_core.h"
+#include "tune_table.h"
 
 namespace xted {
 
@@ -319,6 +320,9 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     P.run_rows = c->opts.run_rows;
     P.narrow_width = c->opts.narrow_width;
     P.half_width = c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width;
+    P.ntune = 0;
+    if (c->opts.tuned)
+        for (int k = 0; k < kTuneRows && k < XTED_TUNE_ROWS; k++) P.tune[P.ntune++] = kTuneTable[k];
     DPair *d_pairs = cv.take<DPair>((size_t)npairs);
     XPair *d_xpairs = cv.take<XPair>((size_t)npairs);
     int32_t *d_trivial = cv.take<int32_t>((size_t)npairs);

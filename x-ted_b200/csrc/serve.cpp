@@ -44,6 +44,7 @@
 #include "plan.h"
 #include "plan_core.h"
 #include "serve_plan.h"
+#include "tune_table.h"
 
 namespace xted {
 cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s);
@@ -529,7 +530,8 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     if (2 * Nall + 2 * (int64_t)(T + S) >= INT32_MAX / 2 || (int64_t)S * T >= INT32_MAX / 2) return XTED_ENOMEM;
     s->Nc_nonempty = nonempty;
     serve_pools_build(s->pools, tr, T, S, Qm, c->opts.run_rows, c->opts.narrow_width,
-                      c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width);
+                      c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width,
+                      c->opts.tuned ? kTuneTable : nullptr, c->opts.tuned ? kTuneRows : 0);
     const ServePools &H = s->pools;
     const size_t n2 = H.node.size();
     // device memory

@@ -49,7 +49,7 @@ struct QPlan {
 
 // Lays out the pools and plans the corpus. The trees must be valid.
 inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, int Qmax, int run_rows,
-                              int narrow_width, int half_width) {
+                              int narrow_width, int half_width, const XTuneRow *tune = nullptr, int ntune = 0) {
     s.T = T;
     s.S = S;
     s.Qmax = Qmax;
@@ -122,6 +122,8 @@ inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, 
     P.run_rows = run_rows;
     P.narrow_width = narrow_width;
     P.half_width = half_width;
+    P.ntune = 0;
+    for (int k = 0; k < ntune && k < XTED_TUNE_ROWS; k++) P.tune[P.ntune++] = tune[k];
     s.stack_rows = 1;
     for (int t = 0; t < T; t++) {
         tree_basic(P, t, s.trees.data());

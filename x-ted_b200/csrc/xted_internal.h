@@ -47,6 +47,13 @@
 
 // Node record (both trees use the same pool): x = label, y = orl | flags.
 
+// Granularity of one tree-size bucket: trees with fewer than max_n nodes use
+// this row-run length and these narrow / half-block chunk limits.
+#define XTED_TUNE_ROWS 8
+struct XTuneRow {
+    int32_t max_n, run_rows, narrow_width, half_width;
+};
+
 struct XRun {      // a run of keyroots of one depth of a row tree
     int32_t kr_lo; // index into the keyroot pool (global)
     int32_t kr_hi;

@@ -40,7 +40,7 @@ class CTree(ctypes.Structure):
 class COpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("orientation", ctypes.c_int32),
                 ("narrow_width", ctypes.c_int32), ("run_rows", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("wide_rows", ctypes.c_int32), ("half_width", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("wide_rows", ctypes.c_int32), ("half_width", ctypes.c_int32), ("tuned", ctypes.c_int32),
                 ("wait_timeout_s", ctypes.c_double), ("mem_limit", ctypes.c_int64)]
 
 

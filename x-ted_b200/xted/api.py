@@ -29,7 +29,7 @@ class Context:
     def __init__(self, device: int = 0, orientation: int = _lib.ORIENT_AUTO,
                  narrow_width: Optional[int] = None, run_rows: Optional[int] = None,
                  ctas_per_sm: int = 0, wait_timeout_s: float = 20.0, mem_limit: int = 0,
-                 wide_rows: int = 0, half_width: int = 0):
+                 wide_rows: int = 0, half_width: int = 0, tuned: Optional[bool] = None):
         L = _lib.lib()
         o = _lib.COpts()
         L.xted_opts_default(ctypes.byref(o))
@@ -42,6 +42,10 @@ class Context:
         o.ctas_per_sm = ctas_per_sm
         o.wide_rows = wide_rows
         o.half_width = half_width
+        # the autotuned per-size table applies unless the granularity is given explicitly
+        if tuned is None:
+            tuned = narrow_width is None and run_rows is None and half_width == 0
+        o.tuned = 1 if tuned else 0
         o.wait_timeout_s = wait_timeout_s
         o.mem_limit = mem_limit
         self.opts = o
