@@ -148,6 +148,8 @@ def make_workload(name: str, rank: int):
 
 
 def dist_setup(args):
+    """One process per GPU (torchrun env). The process group is NCCL on GPUs;
+    XTED_BENCH_BACKEND=gloo runs the same rank logic on CPU (tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -156,36 +158,48 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        backend = os.environ.get("XTED_BENCH_BACKEND", "nccl")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return world, rank, local
 
 
-def reduce_max(x: float, world: int) -> float:
+def _reduce(x: float, world: int, op: str) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def reduce_max(x: float, world: int) -> float:
+    return _reduce(x, world, "max")
 
 
 def reduce_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, "sum")
 
 
 def barrier(world: int):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def aggregate(npairs: int, steps: int, dev_ms: float, cells: int, world: int):
+    """Whole-job pairs/s and GCUPS: every rank ran its own batch (weak
+    scaling); time is the slowest rank's."""
+    dev_ms_max = reduce_max(dev_ms, world)
+    value = npairs * world * steps / (dev_ms_max / 1000.0)
+    gcups = reduce_sum(cells, world) * steps / (dev_ms_max / 1000.0) / 1e9
+    return value, gcups, dev_ms_max
 
 
 def cpu_reference(pairs, budget_s: float, stride: int):
@@ -380,10 +394,8 @@ def main():
             assert (out == ref_out).all(), "results changed between steps"
     torch.cuda.synchronize()
     barrier(world)
-    dev_ms_max = reduce_max(dev_ms, world)
-    value = npairs * world * args.steps / (dev_ms_max / 1000.0)
     cells = st["cells"]
-    gcups = reduce_sum(cells, world) * args.steps / (dev_ms_max / 1000.0) / 1e9
+    value, gcups, dev_ms_max = aggregate(npairs, args.steps, dev_ms, cells, world)
 
     # ---- end to end through the public batch call ----
     ctx.distance_batch(pairs)
