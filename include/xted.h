@@ -126,6 +126,14 @@ int xted_run_prepared(xted_ctx *ctx, int32_t *out);
 
 int xted_last_stats(const xted_ctx *ctx, xted_stats *out);
 
+/* All pairs of ntrees trees: out[i*ntrees + j] = TED(trees[i], trees[j]),
+ * symmetric with a zero diagonal. The reference harness allocates this
+ * matrix but fills only pair (0, 1) (X-TED_CPU/TED_test.cpp:26-47); here the
+ * ntrees(ntrees-1)/2 pairs run through the batch path in chunks whose
+ * distance tables fit in pair_budget int32 elements (0: 2^30, or a quarter of
+ * the context's mem_limit). Synchronous. */
+int xted_distance_matrix(xted_ctx *ctx, const xted_tree *trees, int32_t ntrees, int64_t pair_budget, int32_t *out);
+
 /* Cell count of a pair under each decomposition, without computing it:
  * out[0] = right path (X-TED), out[1] = left path, out[2] = the chosen one. */
 int xted_pair_cells(const xted_tree *a, const xted_tree *b, int32_t orientation, int64_t *out3);
@@ -139,6 +147,22 @@ int xted_validate(const xted_tree *t);
  * n labels, n+1 offsets and n-1 children into caller buffers. */
 int xted_gen_tree(int32_t shape, int32_t n, uint64_t seed, int32_t label_kind, int32_t alphabet,
                   int32_t *labels, int32_t *child_off, int32_t *child_idx);
+
+/* ---- dataset text formats (large corpora) ----
+ *
+ * xted_parse_adjacency: one line of the reference's adjacency files,
+ * "[[1, 2], [], ...]" (grammar of X-TED_CPU/dataset_preprocess.cpp:7-66),
+ * into CSR: child_off[n+1], child_idx[nchildren]. XTED_ENOMEM if the caps
+ * are too small, XTED_EINVAL on text outside the grammar.
+ * xted_parse_bracket: one tree in bracket notation, "{a{b}{c{d}}}" (the
+ * format of the reference's Sampled_Dataset_Extra_Large_Trees/synthetic/
+ * synthetic_tree_*.txt, which its code never reads), into preorder CSR plus
+ * each node's label as a span of the input (label_at, label_len; backslash
+ * escapes left in place). *end_out = index just past the tree. */
+int xted_parse_adjacency(const char *line, int64_t len, int32_t cap_nodes, int32_t cap_children, int32_t *child_off,
+                         int32_t *child_idx, int32_t *n_out, int32_t *nchildren_out);
+int xted_parse_bracket(const char *s, int64_t len, int32_t cap_nodes, int32_t *child_off, int32_t *child_idx,
+                       int64_t *label_at, int32_t *label_len, int32_t *n_out, int64_t *end_out);
 
 /* ---- allocation-free single pair ----
  *

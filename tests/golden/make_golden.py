@@ -5,6 +5,7 @@ after ``make -C oracle all ref``:
 
     python tests/golden/make_golden.py datasets    # -> datasets.json.gz
     python tests/golden/make_golden.py synthetic   # -> synthetic.json.gz
+    python tests/golden/make_golden.py bracket     # -> bracket.json.gz
 
 datasets: tree pair (0, 1) of every file of the reference's sampled datasets
   (Sampled_Dataset/*, Sampled_Dataset_Extra_Large_Trees/*), which is the pair the
@@ -108,7 +109,34 @@ def synthetic():
     print(f"{len(cases)} synthetic cases")
 
 
+def bracket():
+    """The reference's bracket-notation files (read by none of its code) for
+    1,000 and 2,000 nodes, with the trees its label/adjacency files hold for
+    the same datasets (lines 0 and 1, parsed by the reference's own rules) and
+    the reference distance of the pair."""
+    cases = []
+    for n in (1000, 2000):
+        d = os.path.join(REF, "Sampled_Dataset_Extra_Large_Trees", "synthetic", f"{n}_nodes")
+        with open(os.path.join(d, f"synthetic_tree_{n}.txt"), "rb") as f:
+            text = f.read().decode("utf-8", errors="surrogateescape")
+        lab, adj = (os.path.join(d, f"synthetic_nodes_{n}.txt"), os.path.join(d, f"synthetic_nodes_adj_{n}.txt"))
+        nodes, adjs = trees.read_lines(lab), trees.read_lines(adj)
+        expect = []
+        for k in (0, 1):
+            strings = trees.node_process(nodes[k])
+            t = trees.from_adjacency(list(range(len(strings))), trees.pre_process(adjs[k]))
+            expect.append({"labels": strings, "parent": t.parent().tolist()})
+        a, b, sa, sb = trees.load_pair(lab, adj, 0, 1)
+        dist, _ = oracle.ref_distance_str(sa, a, sb, b, num_threads=8)
+        cases.append({"name": os.path.relpath(os.path.join(d, f"synthetic_tree_{n}.txt"), REF), "text": text,
+                      "trees": expect, "distance": dist})
+        print(f"bracket {n}: d={dist}", flush=True)
+    with gzip.open(os.path.join(HERE, "bracket.json.gz"), "wt") as f:
+        json.dump({"source": "reference bracket files; expected trees from its label/adjacency files; distance "
+                             "from its standard_ted", "cases": cases}, f)
+
+
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["datasets", "synthetic"]
+    what = sys.argv[1:] or ["datasets", "synthetic", "bracket"]
     for w in what:
-        {"datasets": datasets, "synthetic": synthetic}[w]()
+        {"datasets": datasets, "synthetic": synthetic, "bracket": bracket}[w]()

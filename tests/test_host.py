@@ -153,3 +153,64 @@ def test_tune_table_well_formed():
     assert max_n == sorted(max_n) and max_n[-1] >= 1 << 30
     for _, rr, nw, hw in rows:
         assert 1 <= int(rr) <= 4096 and 0 <= int(nw) <= 256 and int(hw) <= 1024
+
+
+def _bracket_cases():
+    import gzip
+    import json
+    with gzip.open(os.path.join(REPO, "tests", "golden", "bracket.json.gz"), "rt") as f:
+        return json.load(f)["cases"]
+
+
+def test_bracket_parser_against_reference_files():
+    """The reference's bracket files hold the same trees as its label and
+    adjacency files (fixture made from both, tests/golden/make_golden.py)."""
+    for case in _bracket_cases():
+        ts, ss = [], []
+        for line in case["text"].split("\n"):
+            if line.strip():
+                t, strings = trees.parse_bracket(line)
+                ts.append(t)
+                ss.append(strings)
+        assert len(ts) == len(case["trees"]) == 2
+        for t, strings, want in zip(ts, ss, case["trees"]):
+            assert strings == want["labels"]
+            assert t.parent().tolist() == want["parent"]
+            assert xted.validate(t)
+
+
+def test_bracket_round_trip_with_escapes():
+    t = gen.tree("random", 300, 12, "zipf", 40)
+    strings = [("{x}" if v % 5 == 0 else "") + str(v) + ("\\" if v % 7 == 0 else "") for v in t.labels.tolist()]
+    u, back = trees.parse_bracket(trees.to_bracket(strings, t))
+    assert back == strings
+    assert np.array_equal(u.off, t.off) and np.array_equal(u.idx, t.idx)
+
+
+def test_adjacency_parser_matches_reference_rules(golden_datasets, tmp_path):
+    """The C adjacency parser against pre_process (the reference's rules) on
+    every golden dataset tree, and whole-file loading."""
+    lab_lines, adj_lines, want = [], [], []
+    for name, a, b, _ in golden_datasets[:12]:
+        for t in (a, b):
+            line = "[" + ", ".join("[" + ", ".join(str(c) for c in t.idx[t.off[v]:t.off[v + 1]]) + "]"
+                                   for v in range(len(t))) + "]"
+            off, idx = trees.parse_adjacency(line)
+            assert np.array_equal(off, t.off) and np.array_equal(idx, t.idx), name
+            assert trees.pre_process(line) == t.adjacency()
+            lab_lines.append("".join(f"L{x} " for x in t.labels.tolist()))
+            adj_lines.append(line)
+            want.append(t)
+    (tmp_path / "n.txt").write_text("\n".join(lab_lines) + "\n")
+    (tmp_path / "a.txt").write_text("\n".join(adj_lines) + "\n")
+    got, strings = trees.load_dataset(str(tmp_path / "n.txt"), str(tmp_path / "a.txt"))
+    assert len(got) == len(want)
+    for g, w, s in zip(got, want, strings):
+        assert np.array_equal(g.off, w.off) and np.array_equal(g.idx, w.idx)
+        assert s == [f"L{x}" for x in w.labels.tolist()]
+
+
+def test_adjacency_parser_rejects_bad_text():
+    for bad in ["[[1, 2], [3", "[[1,, 2]]", "[[a]]", "no brackets"]:
+        with pytest.raises(xted.XtedError):
+            trees.parse_adjacency(bad)

@@ -408,6 +408,48 @@ int xted_distance(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t *
     return xted_distance_batch(c, a, b, 1, out);
 }
 
+int xted_distance_matrix(xted_ctx *c, const xted_tree *trees, int32_t ntrees, int64_t pair_budget, int32_t *out) {
+    if (!c || ntrees < 0 || (ntrees > 0 && (!trees || !out)) || pair_budget < 0) return XTED_EINVAL;
+    int64_t budget = pair_budget > 0 ? pair_budget
+                                     : (c->opts.mem_limit > 0 ? c->opts.mem_limit / 16 : (int64_t)1 << 30);
+    const int64_t max_pairs = (int64_t)1 << 20;
+    std::vector<xted_tree> A, B;
+    std::vector<int64_t> at;  // i * ntrees + j of each pair in the chunk
+    std::vector<int32_t> res;
+    auto flush = [&]() -> int {
+        if (A.empty()) return XTED_OK;
+        res.resize(A.size());
+        const int rc = xted_distance_batch(c, A.data(), B.data(), (int32_t)A.size(), res.data());
+        if (rc) return rc;
+        for (size_t k = 0; k < A.size(); k++) {
+            const int64_t i = at[k] / ntrees, j = at[k] % ntrees;
+            out[i * ntrees + j] = res[k];
+            out[j * ntrees + i] = res[k];
+        }
+        A.clear();
+        B.clear();
+        at.clear();
+        return XTED_OK;
+    };
+    int64_t cells = 0;
+    for (int32_t i = 0; i < ntrees; i++) {
+        out[(int64_t)i * ntrees + i] = 0;
+        for (int32_t j = i + 1; j < ntrees; j++) {
+            const int64_t c2 = (int64_t)std::max(trees[i].n, 1) * std::max(trees[j].n, 1);
+            if (!A.empty() && (cells + c2 > budget || (int64_t)A.size() >= max_pairs)) {
+                const int rc = flush();
+                if (rc) return rc;
+                cells = 0;
+            }
+            A.push_back(trees[i]);
+            B.push_back(trees[j]);
+            at.push_back((int64_t)i * ntrees + j);
+            cells += c2;
+        }
+    }
+    return flush();
+}
+
 int xted_last_stats(const xted_ctx *c, xted_stats *out) {
     if (!c || !out) return XTED_EINVAL;
     *out = c->stats;

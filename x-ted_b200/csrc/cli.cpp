@@ -2,6 +2,11 @@
 //
 //   X-TED_GPU <labels.txt> <adj.txt>              (X-TED_GPU/main.cu:4-14)
 //   X-TED_CPU <threads> <labels.txt> <adj.txt>    (X-TED_CPU/main.cpp:4-16)
+//   X-TED_GPU --matrix <labels.txt> <adj.txt>     all pairs of the file's trees
+//
+// --matrix fills the harness's Distance matrix completely (the reference
+// allocates it, X-TED_CPU/TED_test.cpp:26-30, and fills only pair (0, 1)) and
+// prints it, one row per line, entries separated by spaces.
 //
 // Same argv, same input files, same work as the reference harness
 // (X-TED_CPU/TED_test.cpp:3-49, X-TED_GPU/test_TED.cu:3-56): every line of
@@ -13,6 +18,7 @@
 // "Measured time for total parallel execution = X ms" (parallel_X_TED.cu:392),
 // "The distance = d" (which X-TED_GPU never prints) and a blank line
 // (main.cu:11). X is the device time of the tree-distance launch.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -99,7 +105,47 @@ bool build(const std::vector<std::string> &labs, const std::vector<std::vector<i
 
 }  // namespace
 
+#ifndef XTED_CLI_CPU
+static int matrix_main(const char *lab_path, const char *adj_path) {
+    const std::vector<std::string> nodes = read_lines(lab_path);
+    const std::vector<std::string> adjs = read_lines(adj_path);
+    const size_t n = std::min(nodes.size(), adjs.size());
+    std::unordered_map<std::string, int32_t> ids;
+    std::vector<CSR> csr(n);
+    std::vector<xted_tree> tv(n);
+    for (size_t k = 0; k < n; k++) {
+        std::vector<std::vector<int>> adj;
+        if (!adjacency_of(adjs[k], adj) || !build(labels_of(nodes[k]), adj, ids, csr[k])) {
+            std::fprintf(stderr, "xted: malformed input on line %zu\n", k + 1);
+            return 1;
+        }
+        tv[k] = xted_tree{csr[k].lab.data(), csr[k].off.data(), csr[k].idx.data(), (int32_t)adj.size()};
+    }
+    xted_ctx *ctx = nullptr;
+    int rc = xted_create(&ctx, nullptr);
+    if (rc) {
+        std::fprintf(stderr, "xted: %s\n", xted_strerror(rc));
+        return 1;
+    }
+    std::vector<int32_t> m(n * n, 0);
+    rc = n ? xted_distance_matrix(ctx, tv.data(), (int32_t)n, 0, m.data()) : XTED_OK;
+    xted_destroy(ctx);
+    if (rc) {
+        std::fprintf(stderr, "xted: %s\n", xted_strerror(rc));
+        return 1;
+    }
+    for (size_t i = 0; i < n; i++) {
+        for (size_t j = 0; j < n; j++) std::printf(j ? " %d" : "%d", m[i * n + j]);
+        std::printf("\n");
+    }
+    return 0;
+}
+#endif
+
 int main(int argc, char **argv) {
+#ifndef XTED_CLI_CPU
+    if (argc >= 4 && std::string(argv[1]) == "--matrix") return matrix_main(argv[2], argv[3]);
+#endif
 #ifdef XTED_CLI_CPU
     const int first = 2;
     if (argc < 4) {

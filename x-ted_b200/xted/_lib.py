@@ -82,6 +82,8 @@ def lib():
             "xted_distance_batch": (ctypes.c_int, [ctypes.c_void_p, P(CTree), P(CTree), ctypes.c_int32,
                                                    _i32p]),
             "xted_last_stats": (ctypes.c_int, [ctypes.c_void_p, P(CStats)]),
+            "xted_distance_matrix": (ctypes.c_int, [ctypes.c_void_p, P(CTree), ctypes.c_int32, ctypes.c_int64,
+                                                    _i32p]),
             "xted_prepare_batch": (ctypes.c_int, [ctypes.c_void_p, P(CTree), P(CTree), ctypes.c_int32]),
             "xted_run_prepared": (ctypes.c_int, [ctypes.c_void_p, _i32p]),
             "xted_pair_cells": (ctypes.c_int, [P(CTree), P(CTree), ctypes.c_int32, _i64p]),
@@ -97,6 +99,10 @@ def lib():
             "xted_query_poll_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _i32p, _i32p, _i32p,
                                                      P(ctypes.c_double), P(ctypes.c_double)]),
             "xted_serve_stats": (ctypes.c_int, [ctypes.c_void_p, _i64p]),
+            "xted_parse_adjacency": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                                    _i32p, _i32p, _i32p, _i32p]),
+            "xted_parse_bracket": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, _i32p, _i32p,
+                                                  _i64p, _i32p, _i32p, _i64p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -97,6 +97,15 @@ class Context:
                    "xted_distance_batch")
         return out[:n]
 
+    def distance_matrix(self, trees_: Sequence[Tree], pair_budget: int = 0) -> np.ndarray:
+        """All-pairs TED matrix (symmetric, zero diagonal) through the batch path."""
+        n = len(trees_)
+        arr = _lib.tree_array(list(trees_))
+        out = np.zeros((max(n, 1), max(n, 1)), np.int32)
+        _lib.check(_lib.lib().xted_distance_matrix(self._h, _lib.tree_ptr(arr), n, int(pair_budget),
+                                                   out.ctypes.data_as(_lib._i32p)), "xted_distance_matrix")
+        return out[:n, :n]
+
     def prepare_batch(self, pairs: Sequence[Tuple[Tree, Tree]]) -> None:
         """Plan and upload a batch once (inputs resident on the device)."""
         A, B, keep = self._views(pairs)

@@ -199,3 +199,105 @@ def load_pair(labels_path: str, adj_path: str, i: int = 0, j: int = 1):
     ti = from_adjacency(intern(si), ai)
     tj = from_adjacency(intern(sj), aj)
     return ti, tj, si, sj
+
+
+# ---- large corpora: the library's C parsers ----
+
+def parse_adjacency(line: str):
+    """``[[1, 2], [], ...]`` -> (child_off, child_idx) int32 arrays, read by the
+    library's parser (the grammar of ``pre_process``, at C speed)."""
+    import ctypes
+
+    from . import _lib
+    raw = line.encode("utf-8", errors="surrogateescape")
+    cap_n = raw.count(b"[") + 1
+    cap_e = raw.count(b",") + 2
+    off = np.zeros(cap_n + 1, np.int32)
+    idx = np.zeros(max(cap_e, 1), np.int32)
+    n, e = ctypes.c_int32(0), ctypes.c_int32(0)
+    _lib.check(_lib.lib().xted_parse_adjacency(raw, len(raw), cap_n, cap_e, off.ctypes.data_as(_lib._i32p),
+                                               idx.ctypes.data_as(_lib._i32p), ctypes.byref(n), ctypes.byref(e)),
+               "xted_parse_adjacency")
+    return off[:n.value + 1].copy(), idx[:e.value].copy()
+
+
+def _unescape(label: str) -> str:
+    out, i = [], 0
+    while i < len(label):
+        if label[i] == "\\" and i + 1 < len(label):
+            out.append(label[i + 1])
+            i += 2
+        else:
+            out.append(label[i])
+            i += 1
+    return "".join(out)
+
+
+def parse_bracket(text: str, intern: "Interner | None" = None):
+    """One tree in bracket notation, ``{a{b}{c{d}}}`` -> (Tree, label strings).
+    Labels are interned with ``intern`` (a fresh Interner if None)."""
+    import ctypes
+
+    from . import _lib
+    raw = text.encode("utf-8", errors="surrogateescape")
+    cap = raw.count(b"{") + 1
+    off = np.zeros(cap + 1, np.int32)
+    idx = np.zeros(cap, np.int32)
+    at = np.zeros(cap, np.int64)
+    ln = np.zeros(cap, np.int32)
+    n, end = ctypes.c_int32(0), ctypes.c_int64(0)
+    _lib.check(_lib.lib().xted_parse_bracket(raw, len(raw), cap, off.ctypes.data_as(_lib._i32p),
+                                             idx.ctypes.data_as(_lib._i32p), at.ctypes.data_as(_lib._i64p),
+                                             ln.ctypes.data_as(_lib._i32p), ctypes.byref(n), ctypes.byref(end)),
+               "xted_parse_bracket")
+    k = n.value
+    strings = [_unescape(raw[int(a):int(a) + int(b)].decode("utf-8", errors="surrogateescape"))
+               for a, b in zip(at[:k], ln[:k])]
+    intern = intern if intern is not None else Interner()
+    return Tree(intern(strings), off[:k + 1].copy(), idx[:max(k - 1, 0)].copy()), strings
+
+
+def to_bracket(strings: Sequence[str], t: Tree) -> str:
+    """Bracket notation of a tree (labels escaped)."""
+    def esc(x: str) -> str:
+        return x.replace("\\", "\\\\").replace("{", "\\{").replace("}", "\\}")
+    out = []
+    stack = [(0, False)]
+    while stack:
+        v, closing = stack.pop()
+        if closing:
+            out.append("}")
+            continue
+        out.append("{" + esc(strings[v]))
+        stack.append((v, True))
+        for c in reversed(t.idx[t.off[v]:t.off[v + 1]].tolist()):
+            stack.append((c, False))
+    return "".join(out)
+
+
+def load_dataset(labels_path: str, adj_path: str, intern: "Interner | None" = None):
+    """Every tree of a reference dataset file pair (one tree per line), labels
+    interned jointly. Returns (trees, label strings per tree)."""
+    intern = intern if intern is not None else Interner()
+    nodes, adjs = read_lines(labels_path), read_lines(adj_path)
+    out_t, out_s = [], []
+    for lab_line, adj_line in zip(nodes, adjs):
+        strings = lab_line.split(" ")[:-1]  # node_process's rule: a token ends at each space
+        off, idx = parse_adjacency(adj_line)
+        if len(off) - 1 != len(strings):
+            raise ValueError(f"{len(strings)} labels for {len(off) - 1} adjacency rows")
+        out_t.append(Tree(intern(strings), off, idx))
+        out_s.append(strings)
+    return out_t, out_s
+
+
+def load_bracket(path: str, intern: "Interner | None" = None):
+    """Every tree of a bracket-notation file (one tree per line)."""
+    intern = intern if intern is not None else Interner()
+    out_t, out_s = [], []
+    for line in read_lines(path):
+        if line.strip():
+            t, strings = parse_bracket(line, intern)
+            out_t.append(t)
+            out_s.append(strings)
+    return out_t, out_s
