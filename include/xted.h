@@ -224,8 +224,23 @@ int xted_query_poll_timed(xted_ctx *ctx, uint64_t ticket, int32_t *ids, int32_t 
  * error seen since the last drain, else 0. */
 int xted_serve_drain(xted_ctx *ctx);
 
-/* out4: persistent launches made, queries served, pairs served, cells. */
-int xted_serve_stats(xted_ctx *ctx, int64_t *out4);
+/* Writes the first n of: persistent launches made, queries served, pairs
+ * computed, cells computed, pairs pruned (answered by the lower bound
+ * without computing), queries that needed a second round. */
+int xted_serve_stats(xted_ctx *ctx, int64_t *out, int32_t n);
+
+/* Exact top-k pruning by a lower bound of TED, per corpus tree:
+ *   prune = 1: labels, max(m, n) - min(m, n, I), I the size of the two
+ *              label multisets' intersection;
+ *   prune = 2 (default): the Levenshtein distance of the two preorder label
+ *              sequences (an edit mapping keeps preorder), which is never
+ *              below the label bound;
+ *   prune = 0: no pruning, every pair computed in one round.
+ * Round 1 computes the max(first_round, 4k) trees of lowest (bound, index)
+ * (first_round 0: 32); round 2 computes only the trees whose (bound, index)
+ * still beats the k-th (distance, index) found. The answer equals the
+ * unpruned one. Applies to queries admitted later. */
+int xted_serve_options(xted_ctx *ctx, int32_t prune, int32_t first_round);
 
 #ifdef __cplusplus
 }

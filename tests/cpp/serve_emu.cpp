@@ -69,6 +69,90 @@ static int oracle(const HTree &a, const HTree &b) {
                        b.n ? b.lab.data() : &z, b.off.data(), b.idx.empty() ? &z : b.idx.data());
 }
 
+// The bit-vector Levenshtein distance equals the textbook dynamic program
+// (lengths across the 64-row block edges, symbols absent from the pattern).
+static int64_t check_seq_distance(std::mt19937_64 &g) {
+    int64_t checked = 0;
+    for (int it = 0; it < 300; it++) {
+        const int m = (int)(g() % 260), n = (int)(g() % 260), alpha = 1 + (int)(g() % 6);
+        std::vector<int32_t> a((size_t)m), b((size_t)n);
+        for (int32_t &x : a) x = (int32_t)(g() % (uint64_t)(alpha + 1)) - 1;
+        for (int32_t &x : b) x = (int32_t)(g() % (uint64_t)(alpha + 1)) - 1;
+        std::vector<int32_t> prev((size_t)n + 1), cur((size_t)n + 1);
+        for (int j = 0; j <= n; j++) prev[(size_t)j] = j;
+        for (int i = 1; i <= m; i++) {
+            cur[0] = i;
+            for (int j = 1; j <= n; j++) {
+                const int sub = prev[(size_t)j - 1] + ((a[(size_t)i - 1] == b[(size_t)j - 1] && a[(size_t)i - 1] >= 0) ? 0 : 1);
+                cur[(size_t)j] = std::min(sub, std::min(prev[(size_t)j], cur[(size_t)j - 1]) + 1);
+            }
+            std::swap(prev, cur);
+        }
+        SeqBits P;
+        P.build(a.data(), m, alpha);
+        std::vector<uint64_t> work;
+        const int32_t got = P.distance(b.data(), n, work);
+        if (got != prev[(size_t)n]) FAIL("sequence distance m=%d n=%d: got %d want %d", m, n, got, prev[(size_t)n]);
+        checked++;
+    }
+    return checked;
+}
+
+// Exact top-k pruning (serve_plan.h): the label and preorder bounds never
+// exceed the oracle distance, and the two rounds return the unpruned top k.
+static int64_t check_pruning(std::mt19937_64 &g, int maxn) {
+    const int T = 40 + (int)(g() % 60);
+    std::vector<HTree> corpus((size_t)T);
+    std::vector<std::vector<int32_t>> sl((size_t)T);
+    const int alpha = 2 + (int)(g() % 40);
+    for (int t = 0; t < T; t++) {
+        const int n = (g() % 10 == 0) ? (int)(g() % 2) : 1 + (int)(g() % (uint64_t)maxn);
+        corpus[(size_t)t] = gen(n, g, alpha, (int)(g() % 4));
+        sl[(size_t)t] = corpus[(size_t)t].lab;
+        std::sort(sl[(size_t)t].begin(), sl[(size_t)t].end());
+    }
+    int64_t checked = 0;
+    for (int qi = 0; qi < 6; qi++) {
+        const HTree q = (qi == 0) ? corpus[(size_t)(g() % (uint64_t)T)]  // an exact match is in the corpus
+                                  : gen((g() % 12 == 0) ? 0 : 1 + (int)(g() % (uint64_t)maxn), g, alpha, (int)(g() % 4));
+        std::vector<int32_t> ql(q.lab);
+        std::sort(ql.begin(), ql.end());
+        std::vector<int32_t> full((size_t)T), lb((size_t)T), dist((size_t)T, -1);
+        SeqBits P;
+        P.build(q.lab.data(), q.n, alpha);
+        std::vector<uint64_t> work;
+        for (int t = 0; t < T; t++) {
+            full[(size_t)t] = oracle(corpus[(size_t)t], q);
+            const int32_t l1 = label_lower_bound(ql.data(), q.n, sl[(size_t)t].data(), (int)sl[(size_t)t].size());
+            const int32_t l2 = P.distance(corpus[(size_t)t].lab.data(), corpus[(size_t)t].n, work);
+            if (l2 < l1) FAIL("preorder bound %d below the label bound %d", l2, l1);
+            lb[(size_t)t] = (g() % 2) ? l2 : l1;
+            if (l2 > full[(size_t)t]) FAIL("bound %d above the distance %d", l2, full[(size_t)t]);
+            if (q.n == 0 || corpus[(size_t)t].n == 0) dist[(size_t)t] = full[(size_t)t];
+        }
+        const int k = 1 + (int)(g() % 12);
+        std::vector<uint8_t> inc;
+        prune_round1(lb, dist, 1 + (size_t)(g() % (uint64_t)(2 * k)), true, inc);
+        for (int t = 0; t < T; t++)
+            if (inc[(size_t)t]) {
+                if (dist[(size_t)t] >= 0) FAIL("round 1 picked a known pair");
+                dist[(size_t)t] = full[(size_t)t];
+            }
+        if (prune_round2(lb, dist, k, inc))
+            for (int t = 0; t < T; t++)
+                if (inc[(size_t)t]) {
+                    if (dist[(size_t)t] >= 0) FAIL("round 2 picked a known pair");
+                    dist[(size_t)t] = full[(size_t)t];
+                }
+        std::vector<int32_t> id1((size_t)k), d1((size_t)k), id2((size_t)k), d2((size_t)k);
+        topk_known(dist, k, id1.data(), d1.data());
+        topk_known(full, k, id2.data(), d2.data());
+        if (id1 != id2 || d1 != d2) FAIL("pruned top-%d differs from the unpruned one", k);
+        checked += T;
+    }
+    return checked;
+}
+
 int main(int argc, char **argv) {
     const int rounds = argc > 1 ? std::atoi(argv[1]) : 10;
     const int maxn = argc > 2 ? std::atoi(argv[2]) : 120;
@@ -100,12 +184,17 @@ int main(int argc, char **argv) {
         std::vector<HTree> qs((size_t)nq);
         std::vector<QPlan> plans((size_t)nq);
         std::vector<int64_t> dt_base((size_t)nq);
+        std::vector<std::vector<uint8_t>> incs((size_t)nq);
         for (int q = 0; q < nq; q++) {
             const int n = (g() % 8 == 0) ? 0 : 1 + (int)(g() % (uint64_t)Qmax);
             qs[(size_t)q] = gen(n, g, 1 + (int)(g() % 5), (int)(g() % 4));
             const HTree &h = qs[(size_t)q];
+            std::vector<uint8_t> inc((size_t)T, 1);
+            if (r % 4 == 1)  // a pruned round: a random subset of the corpus
+                for (int t = 0; t < T; t++) inc[(size_t)t] = (uint8_t)(g() % 2);
+            incs[(size_t)q] = inc;
             serve_plan_query(H, q, h.lab.data(), h.off.data(), h.idx.data(), h.n, orient, narrow,
-                             (r % 2) ? 5 : 256, plans[(size_t)q]);
+                             (r % 2) ? 5 : 256, plans[(size_t)q], inc.data());
             QPlan &p = plans[(size_t)q];
             u_at += (int64_t)(g() % 1000);
             t_at += (int64_t)(g() % 1000);
@@ -195,6 +284,10 @@ int main(int argc, char **argv) {
             int need = 0;
             for (int t = 0; t < T; t++) {
                 const int pi = q * T + t;
+                if (p.trivial[(size_t)t] < 0 && !incs[(size_t)q][(size_t)t]) {
+                    if (p.first[(size_t)t] != -1 || result[(size_t)pi] != -1) FAIL("excluded pair was computed");
+                    continue;
+                }
                 const int got = p.trivial[(size_t)t] >= 0 ? p.trivial[(size_t)t] : result[(size_t)pi];
                 if (p.trivial[(size_t)t] < 0) need++;
                 const int want = oracle(corpus[(size_t)t], qs[(size_t)q]);
@@ -206,6 +299,8 @@ int main(int argc, char **argv) {
             if (need != p.need) FAIL("need count %d != %d", p.need, need);
         }
     }
-    std::printf("ok %lld pairs\n", (long long)checked);
+    int64_t pruned = check_seq_distance(g);
+    for (int r = 0; r < std::max(1, rounds / 2); r++) pruned += check_pruning(g, std::min(maxn, 40));
+    std::printf("ok %lld pairs, %lld pruning pairs\n", (long long)checked, (long long)pruned);
     return 0;
 }

@@ -135,6 +135,7 @@ private:
 struct Query {
     std::vector<int32_t> lab, off, idx;
     int32_t n = 0, k = 0;
+    std::vector<int32_t> lb, dist;  // per corpus tree: label lower bound; distance once known (-1 before)
     int state = 0;  // 0 queued, 1 admitted, 2 done, < 0 error code
     std::vector<int32_t> ids, dists;
     double t_submit = 0, t_admit = 0, t_done = 0;
@@ -143,6 +144,9 @@ struct Query {
 struct Slot {
     bool busy = false;
     bool planned = false;
+    int round = 1;               // 1: the most promising corpus trees; 2: what may still beat them
+    bool need_post = false;      // a planned next round waits for device room
+    std::vector<uint8_t> inc;    // corpus trees computed in this round
     uint64_t ticket = 0;
     int64_t seq = 0;
     int32_t gen = 0;
@@ -191,7 +195,13 @@ struct ServeState {
     bool stop = false;
     std::thread worker;
     // counters
-    int64_t launches = 0, served = 0, pairs_served = 0, cells_served = 0;
+    int64_t launches = 0, served = 0, pairs_served = 0, cells_served = 0, pairs_pruned = 0, second_rounds = 0;
+    // exact top-k pruning by lower bounds: 0 off, 1 label multisets, 2 preorder sequences
+    int prune = 2;
+    int first_round = 32;                            // at least this many trees, and 4k, in round 1
+    std::vector<std::vector<int32_t>> sorted_labels;  // per corpus tree
+    std::unordered_map<int32_t, int32_t> dense;       // corpus label -> dense symbol
+    std::vector<std::vector<int32_t>> dense_seq;      // per corpus tree: preorder dense symbols
 };
 
 namespace {
@@ -261,6 +271,14 @@ bool never_fits(ServeState *s, const QPlan &p) {
            (int64_t)p.tasks.size() > s->t_ext.cap() || (int64_t)p.entries.size() > s->e_ext.cap();
 }
 
+void release_extents(ServeState *s, Slot &sl) {
+    s->dt_ext.release(sl.dt_off, sl.dt_n);
+    s->u_ext.release(sl.u_off, sl.u_n);
+    s->t_ext.release(sl.t_off, sl.t_n);
+    s->e_ext.release(sl.e_off, sl.e_n);
+    sl.dt_n = sl.u_n = sl.t_n = sl.e_n = 0;
+}
+
 void release(ServeState *s, Slot &sl) {
     s->dt_ext.release(sl.dt_off, sl.dt_n);
     s->u_ext.release(sl.u_off, sl.u_n);
@@ -305,32 +323,59 @@ int post(ServeState *s, int slot, Slot &sl) {
     return XTED_OK;
 }
 
-void finish_query(ServeState *s, Query &q, const QPlan &p, const int32_t *dist) {
-    const int T = s->T;
-    std::vector<int32_t> order((size_t)T);
-    std::vector<int32_t> d((size_t)T);
-    for (int t = 0; t < T; t++) {
-        d[(size_t)t] = p.trivial[(size_t)t] >= 0 ? p.trivial[(size_t)t] : dist[t];
-        order[(size_t)t] = t;
-    }
-    const int k = std::min(q.k, T);
-    std::partial_sort(order.begin(), order.begin() + k, order.end(), [&](int32_t x, int32_t y) {
-        return d[(size_t)x] != d[(size_t)y] ? d[(size_t)x] < d[(size_t)y] : x < y;
-    });
+// Finishes a query from its known distances: every corpus tree not computed
+// has a bound that cannot beat the k-th of them (prune_round2 saw to it).
+void finish_query(ServeState *s, Query &q) {
     q.ids.assign((size_t)q.k, -1);
     q.dists.assign((size_t)q.k, -1);
-    for (int i = 0; i < k; i++) {
-        q.ids[(size_t)i] = order[(size_t)i];
-        q.dists[(size_t)i] = d[(size_t)order[(size_t)i]];
-    }
+    topk_known(q.dist, q.k, q.ids.data(), q.dists.data());
+    for (int32_t d : q.dist) s->pairs_pruned += d < 0;
     q.state = 2;
     q.t_done = now_ms();
+}
+
+// Round 1 of a query: the bound of every corpus tree (host threads), the
+// distances of empty-tree pairs, and the trees computed first.
+void first_round(ServeState *s, const Query &q, std::vector<int32_t> &lb, std::vector<int32_t> &dist,
+                 std::vector<uint8_t> &inc) {
+    const int T = s->T, level = s->prune;
+    lb.assign((size_t)T, 0);
+    dist.assign((size_t)T, -1);
+    for (int t = 0; t < T; t++)
+        if (q.n == 0 || s->sorted_labels[(size_t)t].empty())
+            dist[(size_t)t] = std::max<int32_t>(q.n, (int32_t)s->sorted_labels[(size_t)t].size());
+    if (level == 1) {
+        std::vector<int32_t> ql(q.lab);
+        std::sort(ql.begin(), ql.end());
+        parallel_for(T, 64, [&](int64_t lo, int64_t hi) {
+            for (int64_t t = lo; t < hi; t++) {
+                const std::vector<int32_t> &tl = s->sorted_labels[(size_t)t];
+                lb[(size_t)t] = label_lower_bound(ql.data(), q.n, tl.data(), (int)tl.size());
+            }
+        });
+    } else if (level >= 2 && q.n > 0) {
+        std::vector<int32_t> qd((size_t)q.n);
+        for (int v = 0; v < q.n; v++) {
+            auto it = s->dense.find(q.lab[(size_t)v]);
+            qd[(size_t)v] = it == s->dense.end() ? -1 : it->second;
+        }
+        SeqBits P;
+        P.build(qd.data(), q.n, (int)s->dense.size());
+        parallel_for(T, 16, [&](int64_t lo, int64_t hi) {
+            std::vector<uint64_t> work;
+            for (int64_t t = lo; t < hi; t++) {
+                const std::vector<int32_t> &sq = s->dense_seq[(size_t)t];
+                if (dist[(size_t)t] < 0) lb[(size_t)t] = P.distance(sq.data(), (int)sq.size(), work);
+            }
+        });
+    }
+    prune_round1(lb, dist, std::max<size_t>((size_t)s->first_round, 4 * (size_t)q.k), level > 0, inc);
 }
 
 int64_t oldest_seq(ServeState *s) {
     int64_t o = INT64_MAX;
     for (const Slot &sl : s->slots)
-        if (sl.busy && sl.planned && sl.gen != 0) o = std::min(o, sl.seq);
+        if (sl.busy && sl.planned) o = std::min(o, sl.seq);  // between rounds too: its bucket stays its own
     return o;
 }
 
@@ -354,12 +399,53 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
         if (!sl.busy || sl.gen == 0) continue;
         if (((volatile int32_t *)s->h_flags)[i] != sl.gen) continue;
         std::atomic_thread_fence(std::memory_order_acquire);
-        auto it = s->queries.find(sl.ticket);
-        if (it != s->queries.end()) finish_query(s, it->second, sl.plan, s->h_results + (size_t)i * T);
-        s->served++;
         s->pairs_served += sl.plan.need;
         s->cells_served += sl.plan.cells;
+        progress = true;
+        auto it = s->queries.find(sl.ticket);
+        if (it == s->queries.end()) {
+            release(s, sl);
+            continue;
+        }
+        Query &q = it->second;
+        const int32_t *res = s->h_results + (size_t)i * T;
+        for (int t = 0; t < T; t++)
+            if (sl.plan.trivial[(size_t)t] < 0 && sl.inc[(size_t)t]) q.dist[(size_t)t] = res[t];
+        if (sl.round == 1 && s->prune > 0) {
+            std::vector<uint8_t> inc2;
+            if (prune_round2(q.lb, q.dist, q.k, inc2)) {  // plan round 2 in the same slot (its bucket stays reserved)
+                release_extents(s, sl);
+                sl.gen = 0;
+                sl.round = 2;
+                sl.inc = std::move(inc2);
+                Query qcopy = q;
+                const int wr = s->c->opts.wide_rows;
+                lk.unlock();
+                serve_plan_query(s->pools, i, qcopy.lab.data(), qcopy.off.data(), qcopy.idx.data(), qcopy.n,
+                                 s->c->opts.orientation, s->c->opts.narrow_width, wr > 0 ? wr : -1, sl.plan,
+                                 sl.inc.data());
+                lk.lock();
+                sl.need_post = true;
+                s->second_rounds++;
+                continue;
+            }
+        }
+        finish_query(s, q);
+        s->served++;
         release(s, sl);
+    }
+    // next rounds waiting for device room
+    for (int i = 0; i < s->S; i++) {
+        Slot &sl = s->slots[i];
+        if (!sl.busy || !sl.need_post || !reserve(s, sl)) continue;
+        sl.need_post = false;
+        sl.gen = s->next_gen++;
+        if (s->next_gen <= 0) s->next_gen = 1;
+        auto it = s->queries.find(sl.ticket);
+        if (post(s, i, sl) != XTED_OK) {
+            if (it != s->queries.end()) it->second.state = XTED_ECUDA;
+            release(s, sl);
+        }
         progress = true;
     }
     if (progress) s->cv_done.notify_all();
@@ -409,12 +495,19 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
             s->next_seq++;
             Query qcopy = q;  // plan outside the lock
             lk.unlock();
+            std::vector<int32_t> lb, dist;
+            std::vector<uint8_t> inc;
+            first_round(s, qcopy, lb, dist, inc);
             const int wr = s->c->opts.wide_rows;
             serve_plan_query(s->pools, slot, qcopy.lab.data(), qcopy.off.data(), qcopy.idx.data(), qcopy.n,
                              s->c->opts.orientation, s->c->opts.narrow_width, wr > 0 ? wr : -1,
-                             sl.plan);
+                             sl.plan, inc.data());
             lk.lock();
             if (s->stop || !sl.busy || sl.ticket != ticket) break;  // shut down meanwhile
+            q.lb = std::move(lb);
+            q.dist = std::move(dist);
+            sl.inc = std::move(inc);
+            sl.round = 1;
             sl.planned = true;
             progress = true;
         }
@@ -427,8 +520,7 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
             continue;
         }
         if (sl.plan.need == 0) {  // empty query or empty corpus trees only
-            std::vector<int32_t> none((size_t)T, 0);
-            finish_query(s, q, sl.plan, none.data());
+            finish_query(s, q);
             sl = Slot{};
             s->pending.pop_front();
             s->cv_done.notify_all();
@@ -529,6 +621,17 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     const int64_t Nall = N + (int64_t)S * Qm;
     if (2 * Nall + 2 * (int64_t)(T + S) >= INT32_MAX / 2 || (int64_t)S * T >= INT32_MAX / 2) return XTED_ENOMEM;
     s->Nc_nonempty = nonempty;
+    s->sorted_labels.resize((size_t)T);
+    s->dense_seq.resize((size_t)T);
+    for (int t = 0; t < T; t++) {
+        std::vector<int32_t> &v = s->sorted_labels[(size_t)t];
+        v.assign(tr[t].labels, tr[t].labels + tr[t].n);
+        std::sort(v.begin(), v.end());
+        std::vector<int32_t> &d = s->dense_seq[(size_t)t];
+        d.resize((size_t)tr[t].n);
+        for (int v2 = 0; v2 < tr[t].n; v2++)
+            d[(size_t)v2] = s->dense.emplace(tr[t].labels[v2], (int32_t)s->dense.size()).first->second;
+    }
     serve_pools_build(s->pools, tr, T, S, Qm, c->opts.run_rows, c->opts.narrow_width,
                       c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width,
                       c->opts.tuned ? kTuneTable : nullptr, c->opts.tuned ? kTuneRows : 0);
@@ -747,15 +850,24 @@ int xted_serve_drain(xted_ctx *c) {
     return e;
 }
 
-int xted_serve_stats(xted_ctx *c, int64_t *out4) {
-    if (!c || !out4) return XTED_EINVAL;
+int xted_serve_stats(xted_ctx *c, int64_t *out, int32_t n) {
+    if (!c || !out || n < 0) return XTED_EINVAL;
     ServeState *s = c->serve;
     if (!s) return XTED_EINVAL;
     std::lock_guard<std::mutex> g(s->mu);
-    out4[0] = s->launches;
-    out4[1] = s->served;
-    out4[2] = s->pairs_served;
-    out4[3] = s->cells_served;
+    const int64_t v[6] = {s->launches, s->served, s->pairs_served, s->cells_served, s->pairs_pruned, s->second_rounds};
+    for (int k = 0; k < n && k < 6; k++) out[k] = v[k];
+    return XTED_OK;
+}
+
+int xted_serve_options(xted_ctx *c, int32_t prune, int32_t first_round) {
+    if (!c || first_round < 0) return XTED_EINVAL;
+    ServeState *s = c->serve;
+    if (!s) return XTED_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (prune < 0 || prune > 2) return XTED_EINVAL;
+    s->prune = prune;
+    s->first_round = first_round > 0 ? first_round : 32;
     return XTED_OK;
 }
 

@@ -10,6 +10,7 @@
 #pragma once
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <vector>
 
@@ -135,9 +136,12 @@ inline void serve_pools_build(ServePools &s, const xted_tree *tr, int T, int S, 
 
 // Plans query (lab, off, idx, n <= Qmax, valid) in slot `slot`: the tree into
 // the slot's region, then every (corpus tree, query) pair as the batch
-// planner does (k_pair_setup ... k_level_fill in prep.cu).
+// planner does (k_pair_setup ... k_level_fill in prep.cu); with `include`,
+// only the pairs of the corpus trees it marks (pairs with an empty tree are
+// always answered on the host).
 inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const int32_t *off, const int32_t *idx,
-                             int n, int orientation, int narrow_width, int wide_rows, QPlan &out) {
+                             int n, int orientation, int narrow_width, int wide_rows, QPlan &out,
+                             const uint8_t *include = nullptr) {
     const int T = s.T, tq = T + slot;
     DTree &Q = s.trees[(size_t)tq];
     Q.n = n;
@@ -170,6 +174,7 @@ inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const 
             out.trivial[(size_t)t] = d.trivial;
             continue;
         }
+        if (include && !include[t]) continue;  // not computed in this round (first = -1)
         x.dt_off = dt;
         x.m = s.trees[(size_t)t].n;
         x.n = n;
@@ -217,6 +222,159 @@ inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const 
         X.ntasks = E.ntasks;
         X.bucket = 0;
         X.next = E.level + 1 < dp[(size_t)E.pair].L ? (int32_t)e + 1 : -1;
+    }
+}
+
+// ---- exact top-k pruning ---------------------------------------------------
+//
+// Unit-cost lower bound of TED(a, b) from the sorted label lists of the two
+// trees: an edit mapping M costs (m - |M|) deletions + (n - |M|) insertions
+// + its renames, and at most I (the size of the label multisets'
+// intersection) of its pairs keep their label, so
+//   TED >= m + n - 2|M| + max(0, |M| - I),
+// which falls as |M| grows; at |M| = min(m, n) it is max(m, n) - min(m, n, I).
+inline int32_t label_lower_bound(const int32_t *a, int m, const int32_t *b, int n) {
+    int i = 0, j = 0, common = 0;
+    while (i < m && j < n) {
+        if (a[i] < b[j]) i++;
+        else if (b[j] < a[i]) j++;
+        else {
+            common++;
+            i++;
+            j++;
+        }
+    }
+    return std::max(m, n) - std::min(std::min(m, n), common);
+}
+
+// Preorder bound (S. Guha, H. V. Jagadish, N. Koudas, D. Srivastava, T. Yu,
+// SIGMOD 2002): an edit mapping keeps preorder, so its pairs align the two
+// trees' preorder label sequences at the same unit cost, and the sequences'
+// Levenshtein distance is a lower bound of TED. It dominates the label bound.
+//
+// Computed with Myers' bit-vector algorithm (G. Myers, J. ACM 46(3), 1999),
+// global-distance form (H. Hyyrö, 2003), in 64-row blocks: the pattern's
+// column of vertical deltas is held as bit vectors Pv (+1) and Mv (-1), one
+// text symbol advances every block by a few word operations, and the score
+// D[m][j] follows the horizontal delta leaving the last row.
+struct SeqBits {
+    int m = 0, W = 0;
+    std::vector<uint64_t> peq;  // [rows][W]: bit i of row r set where a[i] is symbol r
+    std::vector<int32_t> row;   // dense symbol -> row of peq, -1 where the pattern lacks it
+
+    // a: m dense symbols in [0, alphabet), or -1 for symbols that match nothing
+    void build(const int32_t *a, int m_, int alphabet) {
+        m = m_;
+        W = (m + 63) / 64;
+        row.assign((size_t)std::max(alphabet, 1), -1);
+        peq.clear();
+        for (int i = 0; i < m; i++) {
+            if (a[i] < 0) continue;
+            int32_t &r = row[(size_t)a[i]];
+            if (r < 0) {
+                r = (int32_t)(peq.size() / (size_t)W);
+                peq.resize(peq.size() + (size_t)W, 0);
+            }
+            peq[(size_t)r * W + (size_t)(i >> 6)] |= 1ull << (i & 63);
+        }
+    }
+
+    // Levenshtein distance of the pattern and text b[0..n) (dense symbols or -1).
+    int32_t distance(const int32_t *b, int n, std::vector<uint64_t> &work) const {
+        if (m == 0) return n;
+        work.assign(2 * (size_t)W, 0);
+        uint64_t *Pv = work.data(), *Mv = Pv + W;
+        for (int w = 0; w < W; w++) Pv[w] = ~0ull;  // D[i][0] = i
+        const uint64_t last = 1ull << ((m - 1) & 63);
+        int32_t score = m;
+        for (int j = 0; j < n; j++) {
+            const int32_t r = b[j] >= 0 && b[j] < (int32_t)row.size() ? row[(size_t)b[j]] : -1;
+            const uint64_t *E = r >= 0 ? &peq[(size_t)r * W] : nullptr;
+            int hin = 1;  // D[0][j] = j: the top row always steps up by one
+            for (int w = 0; w < W; w++) {
+                uint64_t eq = E ? E[w] : 0;
+                const uint64_t pv = Pv[w], mv = Mv[w];
+                const uint64_t xv = eq | mv;
+                if (hin < 0) eq |= 1;
+                const uint64_t xh = (((eq & pv) + pv) ^ pv) | eq;
+                uint64_t ph = mv | ~(xh | pv);
+                uint64_t mh = pv & xh;
+                const uint64_t high = w == W - 1 ? last : (1ull << 63);
+                const int hout = (ph & high) ? 1 : ((mh & high) ? -1 : 0);
+                ph <<= 1;
+                mh <<= 1;
+                if (hin < 0) mh |= 1;
+                else if (hin > 0) ph |= 1;
+                Pv[w] = mh | ~(xv | ph);
+                Mv[w] = ph & xv;
+                hin = hout;
+            }
+            score += hin;
+        }
+        return score;
+    }
+};
+
+// (distance or bound, corpus index) order: ties go to the lower index.
+inline bool key_less(int32_t dx, int32_t x, int32_t dy, int32_t y) { return dx != dy ? dx < dy : x < y; }
+
+// Round 1: of the trees whose distance is unknown (dist < 0), the `want`
+// lowest (bound, index); all of them when prune is off or few are unknown.
+inline void prune_round1(const std::vector<int32_t> &lb, const std::vector<int32_t> &dist, size_t want, bool prune,
+                         std::vector<uint8_t> &inc) {
+    const size_t T = lb.size();
+    inc.assign(T, 0);
+    std::vector<int32_t> order;
+    for (size_t t = 0; t < T; t++)
+        if (dist[t] < 0) order.push_back((int32_t)t);
+    if (prune && order.size() > want) {
+        std::nth_element(order.begin(), order.begin() + (long)want, order.end(), [&](int32_t x, int32_t y) {
+            return key_less(lb[(size_t)x], x, lb[(size_t)y], y);
+        });
+        order.resize(want);
+    }
+    for (int32_t t : order) inc[(size_t)t] = 1;
+}
+
+// Round 2: the unknown trees whose (bound, index) beats the k-th smallest
+// known (distance, index) -- every unknown tree when fewer than k are known.
+// The others cannot enter the top k. Returns false when none is left.
+inline bool prune_round2(const std::vector<int32_t> &lb, const std::vector<int32_t> &dist, int k,
+                         std::vector<uint8_t> &inc) {
+    const size_t T = lb.size();
+    std::vector<int32_t> known;
+    for (size_t t = 0; t < T; t++)
+        if (dist[t] >= 0) known.push_back((int32_t)t);
+    int32_t dk = INT32_MAX, ik = INT32_MAX;
+    if ((int)known.size() >= k) {
+        std::nth_element(known.begin(), known.begin() + (k - 1), known.end(), [&](int32_t x, int32_t y) {
+            return key_less(dist[(size_t)x], x, dist[(size_t)y], y);
+        });
+        ik = known[(size_t)(k - 1)];
+        dk = dist[(size_t)ik];
+    }
+    inc.assign(T, 0);
+    bool any = false;
+    for (size_t t = 0; t < T; t++)
+        if (dist[t] < 0 && key_less(lb[t], (int32_t)t, dk, ik)) {
+            inc[t] = 1;
+            any = true;
+        }
+    return any;
+}
+
+// The k smallest (distance, index) among the known distances; -1 past them.
+inline void topk_known(const std::vector<int32_t> &dist, int k, int32_t *ids, int32_t *dists) {
+    std::vector<int32_t> order;
+    for (size_t t = 0; t < dist.size(); t++)
+        if (dist[t] >= 0) order.push_back((int32_t)t);
+    const int kk = std::min<int>(k, (int)order.size());
+    std::partial_sort(order.begin(), order.begin() + kk, order.end(), [&](int32_t x, int32_t y) {
+        return key_less(dist[(size_t)x], x, dist[(size_t)y], y);
+    });
+    for (int i = 0; i < k; i++) {
+        ids[i] = i < kk ? order[(size_t)i] : -1;
+        dists[i] = i < kk ? dist[(size_t)order[(size_t)i]] : -1;
     }
 }
 

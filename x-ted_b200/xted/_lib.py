@@ -98,7 +98,8 @@ def lib():
             "xted_distance_noalloc": (ctypes.c_int, [P(CTree), P(CTree), ctypes.c_int32, _i32p]),
             "xted_query_poll_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, _i32p, _i32p, _i32p,
                                                      P(ctypes.c_double), P(ctypes.c_double)]),
-            "xted_serve_stats": (ctypes.c_int, [ctypes.c_void_p, _i64p]),
+            "xted_serve_stats": (ctypes.c_int, [ctypes.c_void_p, _i64p, ctypes.c_int32]),
+            "xted_serve_options": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
             "xted_parse_adjacency": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                                                     _i32p, _i32p, _i32p, _i32p]),
             "xted_parse_bracket": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, _i32p, _i32p,
