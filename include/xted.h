@@ -226,7 +226,8 @@ int xted_serve_drain(xted_ctx *ctx);
 
 /* Writes the first n of: persistent launches made, queries served, pairs
  * computed, cells computed, pairs pruned (answered by the lower bound
- * without computing), queries that needed a second round. */
+ * without computing), queries that needed a second round, and the host
+ * microseconds spent computing bounds and planning. */
 int xted_serve_stats(xted_ctx *ctx, int64_t *out, int32_t n);
 
 /* Exact top-k pruning by a lower bound of TED, per corpus tree:

@@ -196,6 +196,7 @@ struct ServeState {
     std::thread worker;
     // counters
     int64_t launches = 0, served = 0, pairs_served = 0, cells_served = 0, pairs_pruned = 0, second_rounds = 0;
+    int64_t bound_us = 0, plan_us = 0;  // host time spent on bounds and on planning
     // exact top-k pruning by lower bounds: 0 off, 1 label multisets, 2 preorder sequences
     int prune = 2;
     int first_round = 32;                            // at least this many trees, and 4k, in round 1
@@ -421,10 +422,13 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
                 Query qcopy = q;
                 const int wr = s->c->opts.wide_rows;
                 lk.unlock();
+                const double t1 = now_ms();
                 serve_plan_query(s->pools, i, qcopy.lab.data(), qcopy.off.data(), qcopy.idx.data(), qcopy.n,
                                  s->c->opts.orientation, s->c->opts.narrow_width, wr > 0 ? wr : -1, sl.plan,
                                  sl.inc.data());
+                const double t2 = now_ms();
                 lk.lock();
+                s->plan_us += (int64_t)((t2 - t1) * 1e3);
                 sl.need_post = true;
                 s->second_rounds++;
                 continue;
@@ -495,14 +499,19 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
             s->next_seq++;
             Query qcopy = q;  // plan outside the lock
             lk.unlock();
+            const double t0 = now_ms();
             std::vector<int32_t> lb, dist;
             std::vector<uint8_t> inc;
             first_round(s, qcopy, lb, dist, inc);
+            const double t1 = now_ms();
             const int wr = s->c->opts.wide_rows;
             serve_plan_query(s->pools, slot, qcopy.lab.data(), qcopy.off.data(), qcopy.idx.data(), qcopy.n,
                              s->c->opts.orientation, s->c->opts.narrow_width, wr > 0 ? wr : -1,
                              sl.plan, inc.data());
+            const double t2 = now_ms();
             lk.lock();
+            s->bound_us += (int64_t)((t1 - t0) * 1e3);
+            s->plan_us += (int64_t)((t2 - t1) * 1e3);
             if (s->stop || !sl.busy || sl.ticket != ticket) break;  // shut down meanwhile
             q.lb = std::move(lb);
             q.dist = std::move(dist);
@@ -855,8 +864,9 @@ int xted_serve_stats(xted_ctx *c, int64_t *out, int32_t n) {
     ServeState *s = c->serve;
     if (!s) return XTED_EINVAL;
     std::lock_guard<std::mutex> g(s->mu);
-    const int64_t v[6] = {s->launches, s->served, s->pairs_served, s->cells_served, s->pairs_pruned, s->second_rounds};
-    for (int k = 0; k < n && k < 6; k++) out[k] = v[k];
+    const int64_t v[8] = {s->launches,     s->served,        s->pairs_served, s->cells_served,
+                          s->pairs_pruned, s->second_rounds, s->bound_us,     s->plan_us};
+    for (int k = 0; k < n && k < 8; k++) out[k] = v[k];
     return XTED_OK;
 }
 

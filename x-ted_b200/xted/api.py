@@ -177,10 +177,11 @@ class Context:
         _lib.check(_lib.lib().xted_serve_drain(self._h), "xted_serve_drain")
 
     def serve_stats(self) -> dict:
-        out = np.zeros(6, np.int64)
-        _lib.check(_lib.lib().xted_serve_stats(self._h, out.ctypes.data_as(_lib._i64p), 6), "xted_serve_stats")
+        out = np.zeros(8, np.int64)
+        _lib.check(_lib.lib().xted_serve_stats(self._h, out.ctypes.data_as(_lib._i64p), 8), "xted_serve_stats")
         return {"launches": int(out[0]), "queries": int(out[1]), "pairs": int(out[2]), "cells": int(out[3]),
-                "pairs_pruned": int(out[4]), "second_rounds": int(out[5])}
+                "pairs_pruned": int(out[4]), "second_rounds": int(out[5]), "bound_us": int(out[6]),
+                "plan_us": int(out[7])}
 
     def serve_options(self, prune: int = 2, first_round: int = 0) -> None:
         """Exact top-k pruning: 0 off, 1 label bound, 2 preorder-sequence bound
