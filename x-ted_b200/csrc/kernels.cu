@@ -714,6 +714,7 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 
 #define CLAIM_EXIT (-1)
 #define CLAIM_RECORD (-2)
+#define CLAIM_NONE (-3)
 
 // Returns a task index (and its entry), CLAIM_EXIT when the launch is over
 // (all tasks done, an error, or in a serving session the stop word or an
@@ -723,12 +724,15 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 // Within a bucket entries are served first in, first out: a block claims the
 // next task of the entry at the bucket's head, and whoever finds that entry
 // exhausted moves the head on. Idle polling is bounded by time and by
-// iterations.
+// iterations. With wait = false (the block still has units in flight, whose
+// completions may publish work) one pass is made and CLAIM_NONE returned if it
+// finds nothing; only a block with nothing in flight waits, counts as idle in
+// a serving session, or ends the launch.
 // Serving: rq_ctl words after the done counter.
 #define CTL_IDLE (2 * XTED_BUCKETS + 1)     // blocks currently idle (or gone)
 #define CTL_LEAVING (2 * XTED_BUCKETS + 2)  // nonzero once blocks have started to leave
 
-__device__ int claim_task(const XKernelParams &P, int *entry) {
+__device__ int claim_task(const XKernelParams &P, int *entry, bool wait) {
     volatile int32_t *ctl = P.rq_ctl;
     volatile int32_t *state = P.entry_state;
     volatile int32_t *mbox = P.mbox;
@@ -773,6 +777,7 @@ __device__ int claim_task(const XKernelParams &P, int *entry) {
                 atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));  // exhausted: next entry
             }
         }
+        if (!wait) return CLAIM_NONE;
         if (P.serve) {
             // A block leaves a serving launch only once every block has been
             // idle (then the others follow as soon as they are idle too), so
@@ -845,21 +850,23 @@ __device__ void complete_task(const XKernelParams &P, int e, int pair) {
     atomicAdd(P.done_total, 1);
 }
 
-// A block publishes level 0 of every pair of mailbox record r.
-__device__ void publish_record(const XKernelParams &P, int r, int *s_rec) {
-    if (threadIdx.x == 0) {
+// A warp publishes level 0 of every pair of mailbox record r (claimed, and
+// acquired, by its lane 0).
+__device__ void publish_record(const XKernelParams &P, int r, int lane) {
+    int lo = 0, n = 0;
+    if (lane == 0) {
         const volatile int32_t *rec = P.mbox + XTED_MBOX_REC + 4 * (r & (XTED_SERVE_RECS - 1));
-        s_rec[0] = rec[1];
-        s_rec[1] = rec[2];
+        lo = rec[1];
+        n = rec[2];
     }
-    __syncthreads();
-    const int lo = s_rec[0], n = s_rec[1];
+    lo = __shfl_sync(FULLMASK, lo, 0);
+    n = __shfl_sync(FULLMASK, n, 0);
     __threadfence();
-    for (int p = lo + (int)threadIdx.x; p < lo + n; p += XTED_CTA_THREADS) {
+    for (int p = lo + lane; p < lo + n; p += 32) {
         const int e = __ldcg(&P.first[p]);
         if (e >= 0) rq_publish(P, e);
     }
-    __syncthreads();
+    __syncwarp();
 }
 
 __global__ void xted_rq_init_kernel(XKernelParams P) {
@@ -867,8 +874,51 @@ __global__ void xted_rq_init_kernel(XKernelParams P) {
     if (p < P.npairs && P.first[p] >= 0) rq_publish(P, P.first[p]);
 }
 
+// Trace record of a finished task (XTED_TRACE): end time and
+// group(1) | units(7) | sm(8) | widest chunk(16) | cells(32).
+__device__ void trace_task_end(const XKernelParams &P, int t) {
+    const XTask T = P.tasks[t];
+    unsigned sm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+    const int nu = (int)(T.kind_n & 0xffff);
+    unsigned long long cells = 0, wmax = 0;
+    for (int k = 0; k < nu; k++) {
+        const XUnit u = P.units[T.unit_lo + k];
+        const unsigned long long w = (unsigned)P.chunks[u.chunk].width;
+        cells += w * (unsigned)P.runs[u.run].rows;
+        if (w > wmax) wmax = w;
+    }
+    P.trace[4 * (int64_t)t + 2] = global_ns();
+    P.trace[4 * (int64_t)t + 3] = ((T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) ? 1ull : 0ull) |
+                                  ((unsigned long long)(nu & 127) << 1) | ((unsigned long long)(sm & 255) << 8) |
+                                  ((wmax & 0xffff) << 16) | ((cells & 0xffffffffull) << 32);
+}
+
+// Narrow tasks open in a block. The block's warps take units one at a time
+// from any open task and never wait for each other: the warp that finishes a
+// task's last unit completes the task, and a warp that finds no unit left
+// claims the next task (one claimer at a time). A group task (half or whole
+// block) gathers every warp at a block barrier once they are between units.
+#define FLOW_SLOTS 16  // > warps + 1: every open task has a unit running or unclaimed
+#define FLOW_RUN 0
+#define FLOW_GROUP 1
+#define FLOW_EXIT 2
+// A slot's units are handed out through one word, (units << 8) | handed out:
+// a warp's atomicAdd on it yields a unit index and the unit count of the same
+// filling, so a warp racing with the slot's reuse never takes a unit of the
+// old task by the new one's count. A free slot holds 0 units.
+struct FlowSlot {
+    int word;  // (units << 8) | next unit; units == 0: free
+    int done;  // units finished
+    int task, entry, pair, unit_lo;
+    int pad[2];
+};
+static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot");
+
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
-    __shared__ int s_task, s_entry, s_next, s_rec[2], s_k[2];
+    __shared__ int s_next, s_k[2];
+    __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch;
+    __shared__ FlowSlot s_fs[FLOW_SLOTS];
     __shared__ WideShared S[2];
     extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache | column nodes (DP_SMEM_BYTES)
     int32_t *s_ring = s_dyn;
@@ -878,83 +928,220 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
     // columns past a chunk's end read ring and stack cells nobody writes for
     // that unit: start them at zero so those inert columns stay non-negative
     for (int x = tid; x < RING_INTS + CACHE_INTS; x += XTED_CTA_THREADS) s_dyn[x] = 0;
+    if (tid < FLOW_SLOTS) {
+        s_fs[tid].word = 0;
+        s_fs[tid].done = 0;
+        s_fs[tid].task = -1;
+    }
+    if (tid == 0) {
+        s_mode = FLOW_RUN;
+        s_lock = -1;
+        s_progress = 0;
+        s_epoch = 0;
+    }
     __syncthreads();
+    volatile int *vmode = &s_mode, *vlock = &s_lock, *vprog = &s_progress, *vepoch = &s_epoch;
+    volatile FlowSlot *vfs = s_fs;
     int32_t *scratch = P.scratch + (int64_t)blockIdx.x * P.scratch_per_cta;
+    // this warp's regions for narrow units
+    int32_t *n_stk = scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX;
+    int32_t *n_ring = s_ring + warp * (XTED_PREFETCH * NARROW_SLOT);
+    int32_t *n_cache = s_cache + warp * (XTED_STACK_CACHE * NARROW_ROW);
+    int32_t *n_cnode = s_cnode + warp * XTED_NARROW_MAX;
+    // A warp without work either is the block's claimer (one at a time: it
+    // polls the ready queue, its waits bounded inside claim_task) or sleeps
+    // until the block's epoch moves (a task opened, the mode changed, the
+    // claimer left). As a guard, a warp that sees its block make no progress
+    // for far longer than any claim may wait gives up.
+    const uint64_t idle_limit = (P.serve ? 16ull : 2ull) * P.timeout_ns;
     for (;;) {
-        if (tid == 0) {
-            int e = -1;
-            const int t = claim_task(P, &e);
-            if (t >= 0 && P.trace) P.trace[4 * (int64_t)t] = global_ns();
-            s_task = t;
-            s_entry = e;
-            s_next = 0;
+        // one read per warp, broadcast: every lane takes the same branch
+        // (lanes woken from a sleep one by one could otherwise read two modes)
+        int mode = 0, epoch = 0;
+        if (lane == 0) {
+            epoch = *vepoch;  // before the slot scan: a task opened later moves it
+            mode = *vmode;
         }
-        __syncthreads();
-        const int t = s_task;
-        if (t == CLAIM_RECORD) {
-            publish_record(P, s_entry, s_rec);
+        mode = __shfl_sync(FULLMASK, mode, 0);
+        epoch = __shfl_sync(FULLMASK, epoch, 0);
+        if (mode == FLOW_EXIT) break;
+        if (mode == FLOW_GROUP) {
+            __syncwarp();
+            __syncthreads();  // every warp is between units
+            const int t = s_gtask;
+            const XTask T = P.tasks[t];
+            const XPair pr = P.pairs[T.pair];
+            if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
+            if (T.kind_n & XTED_TASK_WIDE) {
+                dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S[0], s_ring, s_cache, s_cnode);
+            } else {
+                // the block's two halves take the task's units one at a time
+                const int nu = (int)(T.kind_n & 0xffff);
+                const int gid = warp >> 2, gtid = tid & 127;
+                int32_t *stk = scratch + (int64_t)gid * P.stack_rows * XTED_HALF_MAX;
+                int32_t *ring = s_ring + gid * (4 * XTED_PREFETCH * NARROW_SLOT);
+                int32_t *cache = s_cache + gid * (4 * XTED_STACK_CACHE * NARROW_ROW);
+                int32_t *cnode = s_cnode + gid * (4 * XTED_NARROW_MAX);
+                for (;;) {
+                    if (gtid == 0) s_k[gid] = atomicAdd(&s_next, 1);
+                    group_sync<4>(gid);
+                    const int k = s_k[gid];
+                    group_sync<4>(gid);  // every thread of the half has read s_k before its next claim
+                    if (k >= nu) break;
+                    dispatch_half(P, pr, P.units[T.unit_lo + k], stk, S[gid], ring, cache, cnode, gtid, gid);
+                }
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) {
+                complete_task(P, s_gentry, T.pair);
+                if (P.trace) trace_task_end(P, t);
+                s_progress++;
+                *vmode = FLOW_RUN;
+            }
+            __syncthreads();
             continue;
         }
-        if (t < 0) break;
-        const XTask T = P.tasks[t];
-        const XPair pr = P.pairs[T.pair];
-        if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
-        if (T.kind_n & XTED_TASK_WIDE) {
-            dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S[0], s_ring, s_cache, s_cnode);
-        } else if (T.kind_n & XTED_TASK_HALF) {
-            // the block's two halves take the task's units one at a time
-            const int nu = (int)(T.kind_n & 0xffff);
-            const int gid = warp >> 2, gtid = tid & 127;
-            int32_t *stk = scratch + (int64_t)gid * P.stack_rows * XTED_HALF_MAX;
-            int32_t *ring = s_ring + gid * (4 * XTED_PREFETCH * NARROW_SLOT);
-            int32_t *cache = s_cache + gid * (4 * XTED_STACK_CACHE * NARROW_ROW);
-            int32_t *cnode = s_cnode + gid * (4 * XTED_NARROW_MAX);
-            for (;;) {
-                if (gtid == 0) s_k[gid] = atomicAdd(&s_next, 1);
-                group_sync<4>(gid);
-                const int k = s_k[gid];
-                group_sync<4>(gid);  // every thread of the half has read s_k before its next claim
-                if (k >= nu) break;
-                dispatch_half(P, pr, P.units[T.unit_lo + k], stk, S[gid], ring, cache, cnode, gtid, gid);
-            }
-        } else {
-            // the block's warps take the task's units one at a time
-            const int nu = (int)(T.kind_n & 0xffff);
-            int32_t *stk = scratch + (int64_t)warp * P.stack_rows * XTED_NARROW_MAX;
-            int32_t *ring = s_ring + warp * (XTED_PREFETCH * NARROW_SLOT);
-            int32_t *cache = s_cache + warp * (XTED_STACK_CACHE * NARROW_ROW);
-            int32_t *cnode = s_cnode + warp * XTED_NARROW_MAX;
-            for (;;) {
-                int k = 0;
-                if (lane == 0) k = atomicAdd(&s_next, 1);
-                k = __shfl_sync(FULLMASK, k, 0);
-                if (k >= nu) break;
-                dispatch_narrow(P, pr, P.units[T.unit_lo + k], lane, stk, ring, cache, cnode);
-            }
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) {
-            complete_task(P, s_entry, T.pair);
-            if (P.trace) {  // info: wide(1) | units(7) | sm(8) | widest chunk(16) | cells(32)
-                unsigned sm;
-                asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
-                const int nu = (int)(T.kind_n & 0xffff);
-                unsigned long long cells = 0, wmax = 0;
-                for (int k = 0; k < nu; k++) {
-                    const XUnit u = P.units[T.unit_lo + k];
-                    const unsigned long long w = (unsigned)P.chunks[u.chunk].width;
-                    cells += w * (unsigned)P.runs[u.run].rows;
-                    if (w > wmax) wmax = w;
+        // a unit of an open narrow task
+        int slot = -1, k = 0;
+        if (lane == 0) {
+            for (int q = 0; q < FLOW_SLOTS && slot < 0; q++) {
+                const int w = vfs[q].word;
+                if ((w & 255) < (w >> 8)) {
+                    const int got = atomicAdd(&s_fs[q].word, 1);
+                    if ((got & 255) < (got >> 8)) {
+                        slot = q;
+                        k = got & 255;
+                    }
                 }
-                P.trace[4 * (int64_t)t + 2] = global_ns();
-                P.trace[4 * (int64_t)t + 3] = ((T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) ? 1ull : 0ull) |
-                                              ((unsigned long long)(nu & 127) << 1) |
-                                              ((unsigned long long)(sm & 255) << 8) |
-                                              ((wmax & 0xffff) << 16) | ((cells & 0xffffffffull) << 32);
             }
         }
+        slot = __shfl_sync(FULLMASK, slot, 0);
+        if (slot >= 0) {
+            int pair = 0, ulo = 0;
+            if (lane == 0) {
+                pair = vfs[slot].pair;
+                ulo = vfs[slot].unit_lo + k;
+            }
+            pair = __shfl_sync(FULLMASK, pair, 0);
+            ulo = __shfl_sync(FULLMASK, ulo, 0);
+            __threadfence();  // acquire: the task's inputs, seen by the claimer, are visible here too
+            const XPair pr = P.pairs[pair];
+            dispatch_narrow(P, pr, P.units[ulo], lane, n_stk, n_ring, n_cache, n_cnode);
+            __threadfence();  // release this unit's writes before it is counted done
+            __syncwarp();
+            if (lane == 0) {
+                if (atomicAdd(&s_fs[slot].done, 1) + 1 == (vfs[slot].word >> 8)) {
+                    const int e = vfs[slot].entry, t = vfs[slot].task;
+                    __threadfence();  // acquire the task's other units
+                    complete_task(P, e, pair);
+                    if (P.trace) trace_task_end(P, t);
+                    atomicExch(&s_fs[slot].word, 0);  // free (every unit was handed out)
+                    atomicAdd(&s_progress, 1);
+                }
+            }
+            __syncwarp();
+            continue;
+        }
+        // no unit left: claim the next task (one warp of the block at a time)
+        int t = CLAIM_NONE, e = -1;
+        if (lane == 0 && *vlock < 0 && atomicCAS(&s_lock, -1, warp) == -1) {
+            unsigned ns = 64;
+            const uint64_t c0 = global_ns();
+            const int pg0 = *vprog;
+            for (;;) {
+                // a slot stays filled until its last unit is done: no filled
+                // slot, no unit of this block in flight
+                bool busy = false, room = false, open = false;
+                for (int q = 0; q < FLOW_SLOTS; q++) {
+                    const int w = vfs[q].word;
+                    if ((w >> 8) != 0) {
+                        busy = true;
+                        if ((w & 255) < (w >> 8)) open = true;
+                    } else {
+                        room = true;
+                    }
+                }
+                if (*vmode != FLOW_RUN || open || !room) break;
+                t = claim_task(P, &e, !busy);
+                if (t != CLAIM_NONE) break;
+                // nothing ready while units of this block run: poll again soon
+                if (*vprog == pg0 && global_ns() - c0 > idle_limit) {
+                    set_error(P, XTED_ETIMEOUT, 8, warp, pg0);
+                    t = CLAIM_EXIT;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 1024) ns <<= 1;
+            }
+            if (t >= 0) {
+                atomicAdd(&s_progress, 1);
+                const XTask T = P.tasks[t];
+                if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
+                if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
+                    s_gtask = t;
+                    s_gentry = e;
+                    s_next = 0;
+                    __threadfence_block();
+                    *vmode = FLOW_GROUP;
+                } else {
+                    int q = 0;
+                    while (q < FLOW_SLOTS - 1 && (vfs[q].word >> 8) != 0) q++;  // room was seen; only the claimer fills
+                    vfs[q].task = t;
+                    vfs[q].entry = e;
+                    vfs[q].pair = T.pair;
+                    vfs[q].unit_lo = T.unit_lo;
+                    vfs[q].done = 0;
+                    __threadfence_block();
+                    atomicExch(&s_fs[q].word, (int)(T.kind_n & 0xffff) << 8);  // open: units handed out from here
+                    if (P.trace) P.trace[4 * (int64_t)t + 1] = global_ns();
+                }
+            } else if (t == CLAIM_EXIT) {
+                atomicCAS(&s_mode, FLOW_RUN, FLOW_EXIT);
+            }
+            if (t != CLAIM_RECORD) {
+                __threadfence_block();
+                *vlock = -1;
+                atomicAdd(&s_epoch, 1);  // wake the sleepers: a task, a mode change, or a free claimer seat
+            }
+        }
+        t = __shfl_sync(FULLMASK, t, 0);
+        e = __shfl_sync(FULLMASK, e, 0);
+        if (t == CLAIM_RECORD) {
+            publish_record(P, e, lane);
+            if (lane == 0) {
+                __threadfence_block();
+                *vlock = -1;
+                atomicAdd(&s_epoch, 1);
+            }
+            __syncwarp();
+            continue;
+        }
+        if (t != CLAIM_NONE) continue;  // claimed (or ended), or left the claimer seat with units open
+        // another warp is the claimer: sleep until the block's epoch moves
+        if (lane == 0) {
+            unsigned ns = 128;
+            const uint64_t i0 = global_ns();
+            int pg = *vprog;
+            uint64_t p0 = i0;
+            for (long it = 0; *vepoch == epoch; it++) {
+                __nanosleep(ns);
+                if (ns < 2048) ns <<= 1;
+                const uint64_t now = global_ns();
+                const int pg2 = *vprog;
+                if (pg2 != pg) {
+                    pg = pg2;
+                    p0 = now;
+                } else if (now - p0 > idle_limit || it > (1L << 28)) {
+                    set_error(P, XTED_ETIMEOUT, 7, warp, pg);
+                    atomicCAS(&s_mode, FLOW_RUN, FLOW_EXIT);  // never while a group task gathers the block
+                    break;
+                }
+            }
+        }
+        __syncwarp();
     }
+    cp_async_wait<0>();
 }
 
 // Result of pair p: Dtree[0][0] of its table (X-TED_CPU/TED.cpp:188).
