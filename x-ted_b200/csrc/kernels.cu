@@ -400,11 +400,12 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
 // is a suffix scan within each warp, then across the group's warps through
 // shared memory, with the group's own named barrier.
 // ---------------------------------------------------------------------------
-struct WideShared {
-    int wtot[XTED_WARPS];       // per-warp suffix minima of the current row
+struct __align__(16) WideShared {
+    int wtot[XTED_WARPS];       // per-warp suffix minima of the current row (16-byte aligned: vector reads)
     int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
     int ends[XTED_WARPS];
 };
+static_assert(XTED_WARPS == 8, "carry combination reads the warp minima as two int4");
 
 template <int G>
 __device__ __forceinline__ void group_sync(int gid) {
@@ -499,7 +500,24 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
             group_sync<G>(gid);
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
             if (lane == 31) carry = XTED_INF;
-            for (int w = warp + 1; w < G; w++) carry = min(carry, S.wtot[w]);
+            {
+                // minima of the warps to the right: independent vector reads,
+                // then a select-min per warp (no chain of dependent loads)
+                const int4 lo4 = *reinterpret_cast<const int4 *>(&S.wtot[0]);
+                int v[XTED_WARPS] = {lo4.x, lo4.y, lo4.z, lo4.w, 0, 0, 0, 0};
+                if (G > 4) {
+                    const int4 hi4 = *reinterpret_cast<const int4 *>(&S.wtot[4]);
+                    v[4] = hi4.x;
+                    v[5] = hi4.y;
+                    v[6] = hi4.z;
+                    v[7] = hi4.w;
+                }
+                int right = XTED_INF;
+#pragma unroll
+                for (int w = 1; w < G; w++)
+                    if (w > warp) right = min(right, v[w]);
+                carry = min(carry, right);
+            }
             int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
             for (int k = 0; k < W; k++) prev[k] = min(loc[k], carry) - C.key[k];
