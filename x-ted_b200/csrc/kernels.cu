@@ -306,6 +306,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     // a table at keyroot depth d nests at most d stack rows (nested keyroots have
     // strictly smaller depths), so only deep runs need the global copy of the stack
     const bool deep = run.depth > XTED_STACK_CACHE;
+    const int stack_rows = P.stack_rows;
 
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
@@ -365,25 +366,24 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
                     const int32_t *src = stk + (sp - 1) * stride + c0;
                     int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * NARROW_ROW + pbase;
 #pragma unroll
-                    for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = src[k];
+                    for (int k = 0; k < W; k++) dst[k] = src[k];
                     lo = sp - 1;
                 }
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
-                if (sp < P.stack_rows) {
+                if (sp < stack_rows) {
+                    // whole rows: only far columns are ever read back, and the
+                    // others (inert ones included) hold this row's bounded values
                     int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * NARROW_ROW + pbase;
 #pragma unroll
-                    for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = prev[k];
+                    for (int k = 0; k < W; k++) dst[k] = prev[k];
                     if (deep) {
                         int32_t *g = stk + sp * stride + c0;
 #pragma unroll
-                        for (int k = 0; k < W; k++)
-                            if ((C.far >> k) & 1u) g[k] = prev[k];
+                        for (int k = 0; k < W; k++) g[k] = prev[k];
                     }
                 } else if (lane == 0) {
-                    set_error(P, XTED_ENOMEM, 1, sp, P.stack_rows);
+                    set_error(P, XTED_ENOMEM, 1, sp, stack_rows);
                 }
                 sp++;
                 if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
@@ -432,6 +432,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
     const int pbase = pad(c0);  // pad(c0 + k) == pbase + k for k < W (W divides 32)
     constexpr int PF = XTED_PREFETCH;
     const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
+    const int stack_rows = P.stack_rows;
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, 256 * G - 1);
     group_sync<G>(gid);  // the group's previous unit is done with cnode and S
@@ -539,11 +540,10 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
                 }
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
-                if (sp < P.stack_rows) {
+                if (sp < stack_rows) {
                     int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * GROW + pbase;
 #pragma unroll
-                    for (int k = 0; k < W; k++)
-                        if ((C.far >> k) & 1u) dst[k] = prev[k];
+                    for (int k = 0; k < W; k++) dst[k] = prev[k];  // whole rows in shared memory, as in run_narrow
                     if (deep) {
                         int32_t *g = stk + (int64_t)sp * stride + c0;
 #pragma unroll
@@ -551,7 +551,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
                             if ((C.far >> k) & 1u) g[k] = prev[k];
                     }
                 } else if (gtid == 0) {
-                    set_error(P, XTED_ENOMEM, 2, sp, P.stack_rows);
+                    set_error(P, XTED_ENOMEM, 2, sp, stack_rows);
                 }
                 sp++;
                 if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
