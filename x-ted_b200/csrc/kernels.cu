@@ -730,6 +730,15 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
     return (unsigned)(v >> 32) == pos ? (int)(unsigned)v : -1;
 }
 
+// Longest sleeps between polls (ns; a sleep lasts anywhere up to twice the
+// request): a claimer polling the ready queue, and a warp waiting for its
+// block's claimer.
+#ifndef XTED_CLAIM_SLEEP_MAX
+#define XTED_CLAIM_SLEEP_MAX 1024
+#endif
+#ifndef XTED_IDLE_SLEEP_MAX
+#define XTED_IDLE_SLEEP_MAX 2048
+#endif
 #define CLAIM_EXIT (-1)
 #define CLAIM_RECORD (-2)
 #define CLAIM_NONE (-3)
@@ -750,81 +759,113 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 #define CTL_IDLE (2 * XTED_BUCKETS + 1)     // blocks currently idle (or gone)
 #define CTL_LEAVING (2 * XTED_BUCKETS + 2)  // nonzero once blocks have started to leave
 
-__device__ int claim_task(const XKernelParams &P, int *entry, bool wait) {
+__device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lane) {
+    // Called by a whole warp; lane 0 claims, the warp reads every bucket's
+    // head and tail in one coalesced load so that only non-empty buckets are
+    // probed. Returns the same result in every lane.
     volatile int32_t *ctl = P.rq_ctl;
     volatile int32_t *state = P.entry_state;
     volatile int32_t *mbox = P.mbox;
     unsigned ns = 32;
     uint64_t t0 = 0;
     bool idle_counted = false;  // serving: this block is counted in CTL_IDLE
+    static_assert(2 * XTED_BUCKETS == 32, "one lane per bucket head or tail");
     for (long it = 0; it < (1L << 28); it++) {
-        if (*(volatile int32_t *)P.error != 0) return CLAIM_EXIT;
-        if (P.serve) {
-            // admit posted queries first: their level-0 entries go to the new
-            // query's own (least urgent) bucket, and a busy launch would
-            // otherwise only look at the mailbox once it ran out of work
-            int cons = mbox[XTED_MBOX_CONSUMED];
-            while (cons < mbox[XTED_MBOX_POSTED]) {
-                if (atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons + 1) == cons) {
-                    __threadfence();  // acquire: the record and its query's plan are visible from here on
-                    if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
-                    *entry = cons;
-                    return CLAIM_RECORD;
+        int res = CLAIM_NONE, e_out = -1, top = XTED_BUCKETS - 1;
+        if (lane == 0) {
+            if (*(volatile int32_t *)P.error != 0) {
+                res = CLAIM_EXIT;
+            } else if (P.serve) {
+                // admit posted queries first: their level-0 entries go to the new
+                // query's own (least urgent) bucket, and a busy launch would
+                // otherwise only look at the mailbox once it ran out of work
+                int cons = mbox[XTED_MBOX_CONSUMED];
+                while (cons < mbox[XTED_MBOX_POSTED]) {
+                    if (atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons + 1) == cons) {
+                        __threadfence();  // acquire: the record and its query's plan are visible from here on
+                        if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
+                        e_out = cons;
+                        res = CLAIM_RECORD;
+                        break;
+                    }
+                    cons = mbox[XTED_MBOX_CONSUMED];
                 }
-                cons = mbox[XTED_MBOX_CONSUMED];
+                top = mbox[XTED_MBOX_TOP];
             }
         }
-        const int top = P.serve ? mbox[XTED_MBOX_TOP] : XTED_BUCKETS - 1;
-        for (int i = 0; i < XTED_BUCKETS; i++) {
-            const int b = (top - i) & (XTED_BUCKETS - 1);
-            for (int guard = 0; guard < 256; guard++) {
-                const unsigned h = (unsigned)ctl[2 * b];
-                if ((int)((unsigned)ctl[2 * b + 1] - h) <= 0) break;  // empty
-                const int e = rq_entry(P, b, h);
-                if (e < 0) break;  // the head position is reserved but not yet written
-                const XEntry X = P.entries[e];
-                if (state[2 * e] < X.ntasks) {
-                    const int k = atomicAdd(&P.entry_state[2 * e], 1);
-                    if (k < X.ntasks) {
-                        __threadfence();  // acquire: the level's inputs are visible from here on
-                        if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
-                        *entry = e;
-                        return X.task_off + k;
+        res = __shfl_sync(FULLMASK, res, 0);
+        if (res != CLAIM_NONE) {
+            *entry = __shfl_sync(FULLMASK, e_out, 0);
+            return res;
+        }
+        top = __shfl_sync(FULLMASK, top, 0);
+        // snapshot: lane 2b holds bucket b's head, lane 2b+1 its tail
+        const int v = ctl[lane];
+        const int tl = __shfl_down_sync(FULLMASK, v, 1);
+        const unsigned nonempty = __ballot_sync(FULLMASK, (lane & 1) == 0 && (int)((unsigned)tl - (unsigned)v) > 0);
+        if (lane == 0) {
+            for (int i = 0; i < XTED_BUCKETS && res == CLAIM_NONE; i++) {
+                const int b = (top - i) & (XTED_BUCKETS - 1);
+                if (!((nonempty >> (2 * b)) & 1u)) continue;  // empty when looked at
+                for (int guard = 0; guard < 256; guard++) {
+                    const unsigned h = (unsigned)ctl[2 * b];
+                    if ((int)((unsigned)ctl[2 * b + 1] - h) <= 0) break;  // empty
+                    const int e = rq_entry(P, b, h);
+                    if (e < 0) break;  // the head position is reserved but not yet written
+                    const XEntry X = P.entries[e];
+                    if (state[2 * e] < X.ntasks) {
+                        const int k = atomicAdd(&P.entry_state[2 * e], 1);
+                        if (k < X.ntasks) {
+                            __threadfence();  // acquire: the level's inputs are visible from here on
+                            if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
+                            e_out = e;
+                            res = X.task_off + k;
+                            break;
+                        }
+                    }
+                    atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));  // exhausted: next entry
+                }
+            }
+            if (res == CLAIM_NONE && wait) {
+                if (P.serve) {
+                    // A block leaves a serving launch only once every block has been
+                    // idle (then the others follow as soon as they are idle too), so
+                    // the launch never runs on a few blocks while work arrives; the
+                    // host relaunches when the last one is gone and work is posted.
+                    if (!idle_counted) {
+                        atomicAdd(&P.rq_ctl[CTL_IDLE], 1);
+                        idle_counted = true;
+                    }
+                    if (mbox[XTED_MBOX_STOP] != 0 || ctl[CTL_LEAVING] != 0) res = CLAIM_EXIT;
+                } else if (ld_acquire(P.done_total) >= P.ntasks) {
+                    res = CLAIM_EXIT;
+                }
+                if (res == CLAIM_NONE) {
+                    const uint64_t now = global_ns();
+                    if (t0 == 0) {
+                        t0 = now;
+                    } else if (P.serve) {
+                        if (now - t0 > P.idle_exit_ns && ctl[CTL_IDLE] >= (int)gridDim.x) {
+                            atomicExch(&P.rq_ctl[CTL_LEAVING], 1);
+                            res = CLAIM_EXIT;  // idle everywhere: the host relaunches on new work
+                        }
+                    } else if (now - t0 > P.timeout_ns) {
+                        set_error(P, XTED_ETIMEOUT, 0, 0, 0);
+                        res = CLAIM_EXIT;
                     }
                 }
-                atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));  // exhausted: next entry
             }
         }
-        if (!wait) return CLAIM_NONE;
-        if (P.serve) {
-            // A block leaves a serving launch only once every block has been
-            // idle (then the others follow as soon as they are idle too), so
-            // the launch never runs on a few blocks while work arrives; the
-            // host relaunches when the last one is gone and work is posted.
-            if (!idle_counted) {
-                atomicAdd(&P.rq_ctl[CTL_IDLE], 1);
-                idle_counted = true;
-            }
-            if (mbox[XTED_MBOX_STOP] != 0 || ctl[CTL_LEAVING] != 0) return CLAIM_EXIT;
-        } else if (ld_acquire(P.done_total) >= P.ntasks) {
-            return CLAIM_EXIT;
-        }
-        const uint64_t now = global_ns();
-        if (t0 == 0) {
-            t0 = now;
-        } else if (P.serve) {
-            if (now - t0 > P.idle_exit_ns && ctl[CTL_IDLE] >= (int)gridDim.x) {
-                atomicExch(&P.rq_ctl[CTL_LEAVING], 1);
-                return CLAIM_EXIT;  // idle everywhere: the host relaunches on new work
-            }
-        } else if (now - t0 > P.timeout_ns) {
-            set_error(P, XTED_ETIMEOUT, 0, 0, 0);
-            return CLAIM_EXIT;
+        res = __shfl_sync(FULLMASK, res, 0);
+        if (res != CLAIM_NONE || !wait) {
+            *entry = __shfl_sync(FULLMASK, e_out, 0);
+            return res;
         }
         __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
+        __syncwarp();
+        if (ns < XTED_CLAIM_SLEEP_MAX) ns <<= 1;
     }
-    set_error(P, XTED_ETIMEOUT, 1, 0, 0);
+    if (lane == 0) set_error(P, XTED_ETIMEOUT, 1, 0, 0);
     return CLAIM_EXIT;
 }
 
@@ -1063,64 +1104,74 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         }
         // no unit left: claim the next task (one warp of the block at a time)
         int t = CLAIM_NONE, e = -1;
-        if (lane == 0 && *vlock < 0 && atomicCAS(&s_lock, -1, warp) == -1) {
+        int seat = 0;
+        if (lane == 0) seat = *vlock < 0 && atomicCAS(&s_lock, -1, warp) == -1;
+        if (__shfl_sync(FULLMASK, seat, 0)) {
             unsigned ns = 64;
             const uint64_t c0 = global_ns();
             const int pg0 = *vprog;
             for (;;) {
                 // a slot stays filled until its last unit is done: no filled
                 // slot, no unit of this block in flight
-                bool busy = false, room = false, open = false;
-                for (int q = 0; q < FLOW_SLOTS; q++) {
-                    const int w = vfs[q].word;
-                    if ((w >> 8) != 0) {
-                        busy = true;
-                        if ((w & 255) < (w >> 8)) open = true;
-                    } else {
-                        room = true;
+                int busy = 0, stop = 0;
+                if (lane == 0) {
+                    bool room = false, open = false;
+                    for (int q = 0; q < FLOW_SLOTS; q++) {
+                        const int w = vfs[q].word;
+                        if ((w >> 8) != 0) {
+                            busy = 1;
+                            if ((w & 255) < (w >> 8)) open = true;
+                        } else {
+                            room = true;
+                        }
+                    }
+                    stop = *vmode != FLOW_RUN || open || !room;
+                    if (!stop && busy && *vprog == pg0 && global_ns() - c0 > idle_limit) {
+                        set_error(P, XTED_ETIMEOUT, 8, warp, pg0);
+                        stop = 2;
                     }
                 }
-                if (*vmode != FLOW_RUN || open || !room) break;
-                t = claim_task(P, &e, !busy);
+                stop = __shfl_sync(FULLMASK, stop, 0);
+                busy = __shfl_sync(FULLMASK, busy, 0);
+                if (stop == 2) t = CLAIM_EXIT;
+                if (stop) break;
+                t = claim_task(P, &e, !busy, lane);
                 if (t != CLAIM_NONE) break;
-                // nothing ready while units of this block run: poll again soon
-                if (*vprog == pg0 && global_ns() - c0 > idle_limit) {
-                    set_error(P, XTED_ETIMEOUT, 8, warp, pg0);
-                    t = CLAIM_EXIT;
-                    break;
-                }
-                __nanosleep(ns);
-                if (ns < 1024) ns <<= 1;
+                __nanosleep(ns);  // nothing ready while units of this block run: poll again soon
+                __syncwarp();
+                if (ns < XTED_CLAIM_SLEEP_MAX) ns <<= 1;
             }
-            if (t >= 0) {
-                atomicAdd(&s_progress, 1);
-                const XTask T = P.tasks[t];
-                if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
-                if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
-                    s_gtask = t;
-                    s_gentry = e;
-                    s_next = 0;
-                    __threadfence_block();
-                    *vmode = FLOW_GROUP;
-                } else {
-                    int q = 0;
-                    while (q < FLOW_SLOTS - 1 && (vfs[q].word >> 8) != 0) q++;  // room was seen; only the claimer fills
-                    vfs[q].task = t;
-                    vfs[q].entry = e;
-                    vfs[q].pair = T.pair;
-                    vfs[q].unit_lo = T.unit_lo;
-                    vfs[q].done = 0;
-                    __threadfence_block();
-                    atomicExch(&s_fs[q].word, (int)(T.kind_n & 0xffff) << 8);  // open: units handed out from here
-                    if (P.trace) P.trace[4 * (int64_t)t + 1] = global_ns();
+            if (lane == 0) {
+                if (t >= 0) {
+                    atomicAdd(&s_progress, 1);
+                    const XTask T = P.tasks[t];
+                    if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
+                    if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
+                        s_gtask = t;
+                        s_gentry = e;
+                        s_next = 0;
+                        __threadfence_block();
+                        *vmode = FLOW_GROUP;
+                    } else {
+                        int q = 0;
+                        while (q < FLOW_SLOTS - 1 && (vfs[q].word >> 8) != 0) q++;  // room was seen; only the claimer fills
+                        vfs[q].task = t;
+                        vfs[q].entry = e;
+                        vfs[q].pair = T.pair;
+                        vfs[q].unit_lo = T.unit_lo;
+                        vfs[q].done = 0;
+                        __threadfence_block();
+                        atomicExch(&s_fs[q].word, (int)(T.kind_n & 0xffff) << 8);  // open: units handed out from here
+                        if (P.trace) P.trace[4 * (int64_t)t + 1] = global_ns();
+                    }
+                } else if (t == CLAIM_EXIT) {
+                    atomicCAS(&s_mode, FLOW_RUN, FLOW_EXIT);
                 }
-            } else if (t == CLAIM_EXIT) {
-                atomicCAS(&s_mode, FLOW_RUN, FLOW_EXIT);
-            }
-            if (t != CLAIM_RECORD) {
-                __threadfence_block();
-                *vlock = -1;
-                atomicAdd(&s_epoch, 1);  // wake the sleepers: a task, a mode change, or a free claimer seat
+                if (t != CLAIM_RECORD) {
+                    __threadfence_block();
+                    *vlock = -1;
+                    atomicAdd(&s_epoch, 1);  // wake the sleepers: a task, a mode change, or a free claimer seat
+                }
             }
         }
         t = __shfl_sync(FULLMASK, t, 0);
@@ -1144,7 +1195,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
             uint64_t p0 = i0;
             for (long it = 0; *vepoch == epoch; it++) {
                 __nanosleep(ns);
-                if (ns < 2048) ns <<= 1;
+                if (ns < XTED_IDLE_SLEEP_MAX) ns <<= 1;
                 const uint64_t now = global_ns();
                 const int pg2 = *vprog;
                 if (pg2 != pg) {

@@ -166,9 +166,15 @@ XT_HD inline int32_t level_bundle_half(int64_t nhalf) {
 // few units, so its units spread over several blocks and the level (often on
 // a pair's critical path) finishes sooner; up to XTED_TASK_UNITS when there
 // are plenty, to keep per-task overhead low.
+#ifndef XTED_BUNDLE_MIN
+#define XTED_BUNDLE_MIN XTED_WARPS
+#endif
+#ifndef XTED_BUNDLE_DIV
+#define XTED_BUNDLE_DIV 16
+#endif
 XT_HD inline int32_t level_bundle(int64_t nnarrow) {
-    int64_t b = (nnarrow + 15) / 16;
-    if (b < XTED_WARPS) b = XTED_WARPS;
+    int64_t b = (nnarrow + XTED_BUNDLE_DIV - 1) / XTED_BUNDLE_DIV;
+    if (b < XTED_BUNDLE_MIN) b = XTED_BUNDLE_MIN;
     if (b > XTED_TASK_UNITS) b = XTED_TASK_UNITS;
     return (int32_t)b;
 }

@@ -84,7 +84,9 @@ struct XUnit {
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
 #define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
 #define XTED_HALF_DEFAULT 512       // default limit: wider chunks run faster on the whole block
+#ifndef XTED_TASK_UNITS
 #define XTED_TASK_UNITS 32   // narrow units per task (claimed by the block's warps dynamically)
+#endif
 #define XTED_PREFETCH 4      // rows of tree distances in flight per unit (cp.async ring depth)
 
 struct XTask {
