@@ -101,8 +101,7 @@ int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npa
     // per-block scratch: far-row stacks (+ rows of the generic wide path)
     int64_t per = stack_rows * (XTED_WARPS * XTED_NARROW_MAX);
     if (max_wide > 0 && max_wide <= XTED_WIDE_REG_MAX) per = std::max<int64_t>(per, stack_rows * max_wide);
-    if (max_wide > XTED_WIDE_REG_MAX)  // prev | loc | column records (int4) | stack
-        per = std::max<int64_t>(per, 2 * max_wide + 8 + 4 * max_wide + stack_rows * max_wide);
+    if (max_wide > XTED_WIDE_REG_MAX) per = std::max<int64_t>(per, xted_wide_big_scratch(max_wide, stack_rows));
     per = (int64_t)align_up((size_t)per, 64);
     rc = ctx_dev_reserve(c, c->scratch, (size_t)per * (size_t)c->grid * sizeof(int32_t));
     if (rc) return rc;

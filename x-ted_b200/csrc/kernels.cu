@@ -575,8 +575,13 @@ __device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const X
 // ---------------------------------------------------------------------------
 // Wide unit wider than the register path (one segment of > 2048 columns):
 // the same row step with the row above, the local minima and the far-row
-// stack in block-private global scratch (L1-resident), metadata re-read per row.
-// Scratch layout: prev[width + 1] | loc[width] | stack[stack_rows][width].
+// stack in block-private global scratch, on one block. Each thread owns
+// `per` consecutive columns; the scratch rows are stored interleaved (a
+// thread's k-th column at k * 256 + thread), so every access of the block's
+// threads to their k-th columns is one coalesced line instead of 32 lines
+// `per` columns apart.
+// Scratch layout (Wp = per * 256): prev[Wp + 1] | loc[Wp] | column records
+// (int4)[Wp] | stack[stack_rows][Wp]; the size is xted_wide_big_scratch().
 // ---------------------------------------------------------------------------
 __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *scr,
                              WideShared &S) {
@@ -585,34 +590,45 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     const XChunk ch = P.chunks[u.chunk];
     const int width = ch.width;
     const int per = (width + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS;
-    const int c0 = tid * per;
+    const int64_t Wp = (int64_t)per * XTED_CTA_THREADS;
+    const int c0 = min(tid * per, width);
     const int c1 = min(c0 + per, width);
-    int32_t *prevb = scr;
-    int32_t *locb = scr + width + 1;
-    int4 *cols = (int4 *)(scr + ((2 * width + 4) & ~3));
-    int32_t *stk = (int32_t *)(cols + width);
+    const int nk = c1 - c0;  // this thread's columns (0 for threads past the end)
+    int32_t *prevb = scr;    // prevb[Wp]: D[i+1][width] (0)
+    int32_t *locb = scr + Wp + 1;
+    int4 *cols = (int4 *)(scr + ((2 * Wp + 4) & ~3));
+    int32_t *stk = (int32_t *)(cols + Wp);
+    // interleaved index of column f (any thread's)
+    auto ix = [&](int f) -> int64_t {
+        const int t = f / per;
+        return (int64_t)(f - t * per) * XTED_CTA_THREADS + t;
+    };
     {   // derive this thread's columns once per unit (single segment: keyroot k_lo)
         const int2 *nodes = P.rowinfo + pr.col_base;
         const int j0 = __ldg(&P.krd[ch.k_lo]);
         const int je = j0 + width;
-        for (int c = c0; c < c1; c++) {
+        for (int k = 0; k < nk; k++) {
+            const int c = c0 + k;
             const int j = j0 + c;
             const int2 nd = __ldg(&nodes[j]);
             uint32_t z = (uint32_t)((nd.y & XTED_ROW_ORL_MASK) + 1 - j);
             if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) z |= XTED_COL_FARCOL;
-            cols[c] = make_int4(j, nd.x, (int)z, je - j);
+            cols[(int64_t)k * XTED_CTA_THREADS + tid] = make_int4(j, nd.x, (int)z, je - j);
         }
     }
     const int n = pr.n;
     const int32_t *dt_in = P.dt + pr.dt_off;
     int32_t *dt_out = P.dt + pr.dt_off;
     const int2 *rows = P.rowinfo + pr.row_base;
+    const int stack_rows = P.stack_rows;
+    // the next thread's first column (the diagonal of this thread's last one)
+    const int64_t next_ix = c1 < width ? (int64_t)tid + 1 : Wp;
     // single segment: key = column index
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
-        for (int c = c0; c < c1; c++) prevb[c] = cols[c].w;
-        if (tid == 0) prevb[width] = 0;
+        for (int k = 0; k < nk; k++) prevb[(int64_t)k * XTED_CTA_THREADS + tid] = cols[(int64_t)k * XTED_CTA_THREADS + tid].w;
+        if (tid == 0) prevb[Wp] = 0;
         int sp = 0;
         __syncthreads();
         for (int i = imax - 1; i >= i0; i--) {
@@ -621,14 +637,16 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
             const bool trow = ro == imax - 1;
             const int bord = imax - i;
             const int rowfar = imax - ro - 1;
-            const int32_t *top = stk + (int64_t)(sp > 0 ? sp - 1 : 0) * width;
+            const int32_t *top = stk + (int64_t)(sp > 0 ? sp - 1 : 0) * Wp;
             const int32_t *drow = dt_in + (int64_t)i * n;
             int run_min = XTED_INF;
-            int diag_next = prevb[c1];  // D[i+1][c1]
-            for (int c = c1 - 1; c >= c0; c--) {
-                const int4 ci = cols[c];
+            int diag_next = nk > 0 ? prevb[next_ix] : 0;  // D[i+1][c1]
+            for (int k = nk - 1; k >= 0; k--) {
+                const int c = c0 + k;
+                const int64_t at = (int64_t)k * XTED_CTA_THREADS + tid;
+                const int4 ci = cols[at];
                 const int foff = ci.z & XTED_COL_FOFF_MASK, dend = ci.w;
-                const int up = prevb[c];
+                const int up = prevb[at];
                 int diag = diag_next;
                 diag_next = up;
                 const bool segend = dend == 1;
@@ -638,13 +656,19 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
                 if (trow && tcol) {
                     a = diag + (ri.x != ci.y);
                 } else {
-                    int far = trow ? dend - foff : (tcol ? rowfar : top[c + foff]);
+                    int far;
+                    if (trow) far = dend - foff;
+                    else if (tcol) far = rowfar;
+                    else {
+                        const int f = c + foff;
+                        far = top[k + foff < nk ? (int64_t)(k + foff) * XTED_CTA_THREADS + tid : ix(f)];
+                    }
                     a = __ldcg(drow + ci.x) + far;
                 }
                 int A = min(a, up + 1);
                 if (segend) A = min(A, bord + 1);
                 run_min = min(run_min, A + c);
-                locb[c] = run_min;
+                locb[at] = run_min;
             }
             const int incl = warp_suffix_min(run_min, lane);
             if (lane == 0) S.wtot[warp] = incl;
@@ -656,14 +680,15 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
             const bool pop = i != i0 && (ri.y & XTED_ROW_ISKR);
             const bool push = i > i0 && (ri.y & XTED_ROW_PREVLEAF);
             const int spush = pop ? sp - 1 : sp;
-            if (push && spush >= P.stack_rows && tid == 0) set_error(P, XTED_ENOMEM, 3, spush, P.stack_rows);
-            for (int c = c0; c < c1; c++) {
-                const int4 ci = cols[c];
-                const int d = min(locb[c], carry) - c;
-                prevb[c] = d;
+            if (push && spush >= stack_rows && tid == 0) set_error(P, XTED_ENOMEM, 3, spush, stack_rows);
+            for (int k = 0; k < nk; k++) {
+                const int c = c0 + k;
+                const int64_t at = (int64_t)k * XTED_CTA_THREADS + tid;
+                const int4 ci = cols[at];
+                const int d = min(locb[at], carry) - c;
+                prevb[at] = d;
                 if (trow && (ci.z & XTED_COL_FOFF_MASK) == ci.w) orow[ci.x] = d;
-                if (push && spush < P.stack_rows && (ci.z & XTED_COL_FARCOL))
-                    stk[(int64_t)spush * width + c] = d;
+                if (push && spush < stack_rows && (ci.z & XTED_COL_FARCOL)) stk[(int64_t)spush * Wp + at] = d;
             }
             sp = push ? spush + 1 : spush;
             __syncthreads();

@@ -673,7 +673,7 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     const int64_t sr = H.stack_rows;
     int64_t per = sr * (XTED_WARPS * XTED_NARROW_MAX);
     per = std::max<int64_t>(per, sr * std::min(Qm, XTED_WIDE_REG_MAX));
-    if (Qm > XTED_WIDE_REG_MAX) per = std::max<int64_t>(per, 2 * (int64_t)Qm + 8 + 4 * (int64_t)Qm + sr * Qm);
+    if (Qm > XTED_WIDE_REG_MAX) per = std::max<int64_t>(per, xted_wide_big_scratch(Qm, sr));
     per = (per + 63) / 64 * 64;
     rc |= dev_alloc(s, &s->d_scratch, (size_t)per * (size_t)c->grid);
     if (rc) return XTED_ENOMEM;

@@ -84,6 +84,14 @@ struct XUnit {
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
 #define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
 #define XTED_HALF_DEFAULT 512       // default limit: wider chunks run faster on the whole block
+// Per-block scratch ints of a wide unit on the generic path (one segment of
+// w > XTED_WIDE_REG_MAX columns, far-row stack of sr rows): rows padded to
+// whole columns per thread, prev | loc | column records (int4) | stack.
+static inline int64_t xted_wide_big_scratch(int64_t w, int64_t sr) {
+    const int64_t wp = (w + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS * XTED_CTA_THREADS;
+    return ((2 * wp + 4) & ~(int64_t)3) + 4 * wp + sr * wp;
+}
+
 #ifndef XTED_TASK_UNITS
 #define XTED_TASK_UNITS 32   // narrow units per task (claimed by the block's warps dynamically)
 #endif
