@@ -582,9 +582,13 @@ __device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const X
 // `per` columns apart.
 // Scratch layout (Wp = per * 256): prev[Wp + 1] | loc[Wp] | column records
 // (int4)[Wp] | stack[stack_rows][Wp]; the size is xted_wide_big_scratch().
+// The segment's tree distances of a row (contiguous nodes) are staged in the
+// block's shared memory by coalesced cp.async, the next row's while this one
+// is computed when two rows fit, else row by row; wider segments read them
+// straight from global memory.
 // ---------------------------------------------------------------------------
 __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *scr,
-                             WideShared &S) {
+                             WideShared &S, int32_t *smem) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
@@ -623,6 +627,14 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     const int stack_rows = P.stack_rows;
     // the next thread's first column (the diagonal of this thread's last one)
     const int64_t next_ix = c1 < width ? (int64_t)tid + 1 : Wp;
+    const int j0s = __ldg(&P.krd[ch.k_lo]);  // the segment's first node: row slice drow[j0s, j0s + width)
+    constexpr int kStageInts = DP_SMEM_BYTES / 4;
+    const bool staged = width <= kStageInts, dbl = 2 * width <= kStageInts;
+    auto stage_row = [&](int r, int32_t *dst) {
+        const int32_t *src = dt_in + (int64_t)r * n + j0s;
+        for (int c = tid; c < width; c += XTED_CTA_THREADS) cp_async4(dst + c, src + c);
+        cp_async_commit();
+    };
     // single segment: key = column index
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
@@ -631,7 +643,25 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
         if (tid == 0) prevb[Wp] = 0;
         int sp = 0;
         __syncthreads();
+        if (staged && dbl) stage_row(imax - 1, smem + ((imax - 1) & 1) * width);
         for (int i = imax - 1; i >= i0; i--) {
+            const int32_t *srow = nullptr;
+            if (staged) {
+                if (dbl) {
+                    srow = smem + (i & 1) * width;
+                    if (i - 1 >= i0) {
+                        stage_row(i - 1, smem + ((i - 1) & 1) * width);  // its buffer's last readers passed the row-end barrier
+                        cp_async_wait<1>();
+                    } else {
+                        cp_async_wait<0>();
+                    }
+                } else {
+                    srow = smem;
+                    stage_row(i, smem);
+                    cp_async_wait<0>();
+                }
+                __syncthreads();  // every thread's copies of row i have landed
+            }
             const int2 ri = __ldg(&rows[i]);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
@@ -663,7 +693,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
                         const int f = c + foff;
                         far = top[k + foff < nk ? (int64_t)(k + foff) * XTED_CTA_THREADS + tid : ix(f)];
                     }
-                    a = __ldcg(drow + ci.x) + far;
+                    a = (staged ? srow[c] : __ldcg(drow + ci.x)) + far;
                 }
                 int A = min(a, up + 1);
                 if (segend) A = min(A, bord + 1);
@@ -704,7 +734,7 @@ __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUn
     else if (width <= 512) run_group<2, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
     else if (width <= 1024) run_group<4, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
     else if (width <= XTED_WIDE_REG_MAX) run_group<8, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
-    else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S);
+    else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S, ring);
     else if (tid == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
 }
 
