@@ -189,3 +189,17 @@ def test_large_pair_properties(ctx):
     for orient in (xted.ORIENT_RIGHT, xted.ORIENT_LEFT):
         with xted.Context(orientation=orient) as c:
             assert c.distance(r, s) == want
+
+
+@pytest.mark.parametrize("n", [2049, 2300, 2817])
+def test_generic_wide_path_edges(ctx, n):
+    """Column segments just above the register paths' 2,048-column limit run on
+    the generic wide path (per-thread column runs of uneven length, the last
+    threads short or idle, far columns owned by other threads): caterpillars
+    and random trees of these sizes against the oracle."""
+    a = gen.tree("caterpillar", n, 100 + n, "uniform", 8)
+    b = gen.tree("caterpillar", n - 7, 200 + n, "uniform", 8)
+    r = gen.tree("random", n, 300 + n, "uniform", 8)
+    pairs = [(a, b), (r, a), (b, r)]
+    got = ctx.distance_batch(pairs)
+    assert list(got) == [oracle.distance(x, y) for x, y in pairs]
