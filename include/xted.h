@@ -80,6 +80,10 @@ typedef struct xted_opts {
                                to every tree                                */
     double wait_timeout_s;  /* bound on every device-side wait              */
     int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
+    int64_t stripe_min_cells; /* a table whose column segment is wider than
+                               2,048 and whose unit has at least this many
+                               cells runs in 2,048-column stripes on up to 16
+                               blocks at once (0 = 2^24; < 0: one block)    */
 } xted_opts;
 
 typedef struct xted_ctx xted_ctx;

@@ -203,3 +203,35 @@ def test_generic_wide_path_edges(ctx, n):
     pairs = [(a, b), (r, a), (b, r)]
     got = ctx.distance_batch(pairs)
     assert list(got) == [oracle.distance(x, y) for x, y in pairs]
+
+
+@pytest.mark.parametrize("n", [2049, 2817])
+def test_striped_wide_units_match_oracle(n):
+    """Striped units (a column segment wider than 2,048 split into stripes run
+    by several blocks at once, carries and far columns passed between them),
+    forced on every wide unit: caterpillars and random trees against the oracle,
+    and a 4,000-node random pair in both decompositions."""
+    a = gen.tree("caterpillar", n, 100 + n, "uniform", 8)
+    b = gen.tree("caterpillar", n - 7, 200 + n, "uniform", 8)
+    r = gen.tree("random", n, 300 + n, "uniform", 8)
+    pairs = [(a, b), (r, a), (b, r)]
+    with xted.Context(stripe_min_cells=1) as c:
+        got = c.distance_batch(pairs)
+    assert list(got) == [oracle.distance(x, y) for x, y in pairs]
+    if n == 2817:
+        r4, s4 = gen.tree("random", 4000, 41, "uniform", 64), gen.tree("random", 4000, 42, "uniform", 64)
+        want = oracle.distance(r4, s4)
+        for orient in (xted.ORIENT_RIGHT, xted.ORIENT_LEFT):
+            with xted.Context(orientation=orient, stripe_min_cells=1) as c:
+                assert c.distance(r4, s4) == want
+
+
+def test_striped_equals_one_block_on_20000_node_pairs():
+    """The 20,000-node pairs with stripes (the default) and with every wide
+    unit on one block give the same distances."""
+    pairs = [gen.single_pair_20000(shape="random"), gen.single_pair_20000(shape="caterpillar")]
+    with xted.Context(stripe_min_cells=-1) as c:
+        one = c.distance_batch(pairs)
+    with xted.Context() as c:
+        striped = c.distance_batch(pairs)
+    assert list(one) == list(striped)

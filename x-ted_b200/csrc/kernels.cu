@@ -404,6 +404,7 @@ struct __align__(16) WideShared {
     int wtot[XTED_WARPS];       // per-warp suffix minima of the current row (16-byte aligned: vector reads)
     int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
     int ends[XTED_WARPS];
+    int cin;                    // stripes: the right neighbour's carry for the current row
 };
 static_assert(XTED_WARPS == 8, "carry combination reads the warp minima as two int4");
 
@@ -558,6 +559,226 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
             }
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
             group_sync<G>(gid);       // ... and everyone's, the record and the stack push
+        }
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Stripe s of a striped unit: columns [C0, C1) = [2048 s, min(2048 (s+1), w))
+// of a single column segment of width w, on the whole block (8 columns per
+// thread), concurrently with the other stripes on the other gang blocks. It
+// is run_group's row step with three additions:
+//   * the row's suffix minimum continues from the right: before the scan
+//     barrier the block waits for its right neighbour to finish the row and
+//     takes that stripe's carry (its minimum of A[k] + k over k >= C1);
+//   * a far column to the right of the stripe (f = orl(j)+1 >= C1) is read
+//     from the exported values of its owner, kept per pushed row (the owner
+//     is ahead, and its stack slot may since hold another row);
+//   * the tree rows' diagonal at the last column is the right neighbour's
+//     first column one row below.
+// Each stripe publishes per row its carry and first column, its exported
+// columns on pushed rows, then its progress (rows done, flat over the unit's
+// keyroots). Waits are bounded by the launch's timeout.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool wait_progress(const XKernelParams &P, volatile int32_t *prog, int want) {
+    const uint64_t t0 = global_ns();
+    for (long it = 0; it < (1L << 26); it++) {
+        if (prog[0] >= want) {
+            __threadfence();  // acquire: the neighbour's row outputs are visible from here on
+            return true;
+        }
+        if (*(volatile int32_t *)P.error != 0) return false;
+        if (global_ns() - t0 > P.timeout_ns) break;
+        __nanosleep(32);
+    }
+    set_error(P, XTED_ETIMEOUT, 10, want, prog[0]);
+    return false;
+}
+
+__device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
+                           int32_t *ring, int32_t *cache, int32_t *cnode, int s, int K, int X, int R,
+                           const int32_t *expmap, int32_t *prog, int32_t *CR, int32_t *FC, int32_t *E) {
+    constexpr int W = 8, G = XTED_WARPS;
+    constexpr int GROW = 256 * G + 8 * G;
+    constexpr int GSLOT = GROW + 8;
+    constexpr int PF = XTED_PREFETCH;
+    const int gtid = threadIdx.x, lane = gtid & 31, warp = gtid >> 5;
+    const XRun run = P.runs[u.run];
+    const XChunk ch = P.chunks[u.chunk];
+    const int w = ch.width;
+    const int C0 = s * XTED_STRIPE, C1 = min(C0 + XTED_STRIPE, w), tw = C1 - C0;
+    const bool right = s + 1 < K, left = s > 0;
+    const int lc0 = gtid * W, c0 = C0 + lc0;  // this thread's first column: local, in the segment
+    const int pbase = pad(lc0);
+    const bool deep = run.depth > XTED_STACK_CACHE;
+    const int stack_rows = P.stack_rows;
+    Cols<W> C;
+    load_cols<W>(P, pr, ch, c0, C, w - 1);
+    unsigned expm = 0;  // this thread's columns that stripes to the left read as far columns
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        const int c = c0 + k;
+        if (c >= C1) {  // past the stripe: an inert column
+            C.valid &= ~(1u << k);
+            C.far &= ~(1u << k);
+            C.tcol &= ~(1u << k);
+            C.node[k] = 0;
+            C.lab[k] = 0;
+            C.dend[k] = 2;
+            C.fb[k] = 1;
+            C.segor[k] = NOSEG;
+            C.fidx[k] = pad(min(lc0 + k, XTED_STRIPE - 1));
+        } else {
+            const int f = c + (C.dend[k] - C.fb[k]);  // orl(j)+1 in segment columns
+            if (f >= w) C.fidx[k] = pad(lc0 + k);     // the border: a tree-path column (rowfar)
+            else if (f < C1) C.fidx[k] = pad(f - C0);
+            else C.fidx[k] = -1 - __ldcg(&expmap[f]);  // exported by a stripe to the right
+            if (__ldcg(&expmap[c]) >= 0) expm |= 1u << k;
+        }
+    }
+    __syncthreads();  // the block's previous unit is done with cnode and S
+#pragma unroll
+    for (int k = 0; k < W; k++)
+        if ((C.valid >> k) & 1u) cnode[lc0 + k] = C.node[k];
+    set_keys<W>(C, c0, 0);  // one segment: key = segment column
+    const int n = pr.n;
+    const int32_t *dt_in = P.dt + pr.dt_off;
+    int32_t *dt_out = P.dt + pr.dt_off;
+    const int2 *rows = P.rowinfo + pr.row_base;
+    volatile int32_t *prog_right = prog + s + 1;
+    int tflat = 0;
+    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+        const int i0 = __ldg(&P.krd[kr]);
+        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        const int tbase = tflat;
+        int prev[W];
+#pragma unroll
+        for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        int sp = 0, lo = 0;
+        __syncthreads();  // the ring's and S's previous readers are done
+        if (lane == 0) S.first[warp] = prev[0];
+        if (gtid == 0) S.first[G] = right ? w - C1 : 0;  // D[imax][C1]: the bottom border
+#pragma unroll
+        for (int q = 0; q < PF - 1; q++) {
+            const int r = imax - 1 - q;
+            if (r >= i0)
+                issue_row<W>(cnode, tw, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                             gtid == 0);
+            cp_async_commit();
+        }
+        cp_async_wait<PF - 2>();
+        __syncthreads();
+        for (int i = imax - 1; i >= i0; i--, tflat++) {
+            {
+                const int r = i - (PF - 1);
+                if (r >= i0)
+                    issue_row<W>(cnode, tw, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                                 gtid == 0);
+                cp_async_commit();
+            }
+            const int32_t *slot = ring + (i & (PF - 1)) * GSLOT;
+            const int2 ri = *(const int2 *)(slot + GROW);
+            const int ro = ri.y & XTED_ROW_ORL_MASK;
+            const bool trow = ro == imax - 1;
+            const int bord = imax - i;
+            int loc[W];
+            int mine;
+            if (!trow) {
+                // forest row: far values from the stack top, or exported by the stripe that owns them
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
+                const int32_t *erow = E + (int64_t)(tbase + (imax - 1 - (ro + 1))) * X;
+                const int32_t *cur = slot + pbase;
+                const int rowfar = imax - ro - 1, bord1 = bord + 1;
+                int run_min = XTED_INF;
+#pragma unroll
+                for (int k = W - 1; k >= 0; k--) {
+                    int far;
+                    if ((C.tcol >> k) & 1u) far = rowfar;
+                    else if (C.fidx[k] >= 0) far = top[C.fidx[k]];
+                    else far = __ldcg(erow + (-1 - C.fidx[k]));
+                    int A = __viaddmin_s32(prev[k], 1, cur[k] + far);
+                    A = min(A, bord1 | C.segor[k]);
+                    run_min = __viaddmin_s32(A, C.key[k], run_min);
+                    loc[k] = run_min;
+                }
+                mine = run_min;
+            } else {
+                int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
+                if (lane == 31) dnext = S.first[warp + 1];
+                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, loc);
+            }
+            const int incl = warp_suffix_min(mine, lane);
+            if (lane == 0) S.wtot[warp] = incl;
+            if (gtid == 0) {
+                int cin = XTED_INF;
+                if (right && wait_progress(P, prog_right, tflat + 1)) cin = __ldcg(CR + (int64_t)(s + 1) * R + tflat);
+                S.cin = cin;
+            }
+            __syncthreads();
+            int carry = __shfl_down_sync(FULLMASK, incl, 1);
+            if (lane == 31) carry = XTED_INF;
+            {
+                const int4 lo4 = *reinterpret_cast<const int4 *>(&S.wtot[0]);
+                const int4 hi4 = *reinterpret_cast<const int4 *>(&S.wtot[4]);
+                const int v[XTED_WARPS] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
+                int rmin = S.cin;
+#pragma unroll
+                for (int q = 1; q < G; q++)
+                    if (q > warp) rmin = min(rmin, v[q]);
+                carry = min(carry, rmin);
+            }
+            int32_t *orow = dt_out + (int64_t)i * n;
+#pragma unroll
+            for (int k = 0; k < W; k++) prev[k] = min(loc[k], carry) - C.key[k];
+            if (trow) {
+#pragma unroll
+                for (int k = 0; k < W; k++)
+                    if ((C.tcol >> k) & 1u) orow[C.node[k]] = prev[k];
+            }
+            if (lane == 0) S.first[warp] = prev[0];
+            if (gtid == 0 && left) {  // for the left neighbour: carry at C0 and D[i][C0]
+                CR[(int64_t)s * R + tflat] = prev[0] + C.key[0];
+                FC[(int64_t)s * R + tflat] = prev[0];
+            }
+            if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
+                sp--;
+                if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
+                    const int32_t *src = stk + (int64_t)(sp - 1) * XTED_STRIPE + lc0;
+                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * GROW + pbase;
+#pragma unroll
+                    for (int k = 0; k < W; k++) dst[k] = src[k];
+                    lo = sp - 1;
+                }
+            }
+            if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
+                if (sp < stack_rows) {
+                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * GROW + pbase;
+#pragma unroll
+                    for (int k = 0; k < W; k++) dst[k] = prev[k];
+                    if (deep) {
+                        int32_t *g = stk + (int64_t)sp * XTED_STRIPE + lc0;
+#pragma unroll
+                        for (int k = 0; k < W; k++) g[k] = prev[k];
+                    }
+                } else if (gtid == 0) {
+                    set_error(P, XTED_ENOMEM, 11, sp, stack_rows);
+                }
+                if (expm) {  // a pushed row is a far row: export the columns stripes to the left read
+                    int32_t *erow = E + (int64_t)tflat * X;
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if ((expm >> k) & 1u) erow[__ldcg(&expmap[c0 + k])] = prev[k];
+                }
+                sp++;
+                if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
+            }
+            // the next row's diagonal at C1: the right neighbour's first column of this row
+            if (gtid == 0 && right) S.first[G] = __ldcg(FC + (int64_t)(s + 1) * R + tflat);
+            __threadfence();          // this row's outputs, before the progress word
+            cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
+            __syncthreads();          // ... and everyone's, the record and the stack push
+            if (gtid == 0 && left) ((volatile int32_t *)prog)[s] = tflat + 1;
         }
     }
     cp_async_wait<0>();
@@ -797,6 +1018,7 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 #define CLAIM_EXIT (-1)
 #define CLAIM_RECORD (-2)
 #define CLAIM_NONE (-3)
+#define CLAIM_GANG (-4)  // a gang block: a striped unit waits for the gang
 
 // Returns a task index (and its entry), CLAIM_EXIT when the launch is over
 // (all tasks done, an error, or in a serving session the stop word or an
@@ -830,6 +1052,10 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
         if (lane == 0) {
             if (*(volatile int32_t *)P.error != 0) {
                 res = CLAIM_EXIT;
+            } else if ((int)blockIdx.x < P.gang_blocks &&
+                       ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_TAIL] > ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_HEAD]) {
+                if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
+                res = CLAIM_GANG;  // every gang block takes part in every striped unit
             } else if (P.serve) {
                 // admit posted queries first: their level-0 entries go to the new
                 // query's own (least urgent) bucket, and a busy launch would
@@ -1008,6 +1234,183 @@ __device__ void trace_task_end(const XKernelParams &P, int t) {
                                   ((wmax & 0xffff) << 16) | ((cells & 0xffffffffull) << 32);
 }
 
+// ---- striped units: the gang ----
+// A block that claims a striped unit hands it to the gang ring instead of
+// running it (on one block when the ring is full or there is no gang); the
+// gang blocks (0 .. gang_blocks-1) notice pending units when they look for
+// work, meet at a barrier, the leader (block 0) lays the unit out, and each
+// block runs one stripe. One striped unit at a time.
+__device__ bool gang_push(const XKernelParams &P, int t, int e) {
+    volatile int32_t *g = P.gang_ctl;
+    for (int it = 0; it < 1024; it++) {
+        const int tl = g[XTED_GCTL_TAIL], hd = g[XTED_GCTL_HEAD];
+        if (tl - hd >= XTED_GANG_RING) return false;
+        if (atomicCAS(&P.gang_ctl[XTED_GCTL_TAIL], tl, tl + 1) == tl) {
+            volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (tl & (XTED_GANG_RING - 1));
+            slot[1] = t;
+            slot[2] = e;
+            __threadfence();
+            slot[0] = tl + 1;  // the slot holds position tl
+            return true;
+        }
+    }
+    return false;
+}
+
+// Barrier of the gang blocks (a global arrival count; phases counted per
+// block, equal in every gang block). False after an error or a timeout.
+__device__ bool gang_barrier(const XKernelParams &P, int *s_phase, int *s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int target = (*s_phase + 1) * P.gang_blocks;
+        atomicAdd(&P.gang_ctl[XTED_GCTL_BAR], 1);
+        bool ok = false;
+        const uint64_t t0 = global_ns();
+        for (long it = 0; it < (1L << 26); it++) {
+            if (((volatile int32_t *)P.gang_ctl)[XTED_GCTL_BAR] >= target) {
+                ok = true;
+                break;
+            }
+            if (*(volatile int32_t *)P.error != 0) break;
+            if (global_ns() - t0 > P.timeout_ns) {
+                set_error(P, XTED_ETIMEOUT, 9, target, ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_BAR]);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+        *s_phase += 1;
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// One striped unit, run by every gang block (all threads).
+__device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S, int32_t *ring, int32_t *cache,
+                         int32_t *cnode, int *s_g) {
+    // s_g: [0] phase, [1] ok, [2] task, [3] entry, [4] stripes, [5] exports, [6] feasible, [7] scan scratch
+    const int tid = threadIdx.x, b = blockIdx.x;
+    volatile int32_t *g = P.gang_ctl;
+    if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // A: every gang block is here
+    if (b == 0) {
+        if (tid == 0) {
+            const int hd = g[XTED_GCTL_HEAD];
+            volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (hd & (XTED_GANG_RING - 1));
+            const uint64_t t0 = global_ns();
+            bool ok = false;
+            for (long it = 0; it < (1L << 26); it++) {
+                if (slot[0] == hd + 1) {
+                    ok = true;
+                    break;
+                }
+                if (global_ns() - t0 > P.timeout_ns) break;
+                __nanosleep(32);
+            }
+            if (!ok) set_error(P, XTED_ETIMEOUT, 12, hd, 0);
+            __threadfence();
+            s_g[2] = ok ? slot[1] : -1;
+            s_g[3] = ok ? slot[2] : -1;
+        }
+        __syncthreads();
+        const int t = s_g[2];
+        int K = 0, X = 0, feasible = 0;
+        if (t >= 0) {
+            const XTask T = P.tasks[t];
+            const XUnit u = P.units[T.unit_lo];
+            const XChunk ch = P.chunks[u.chunk];
+            const XPair pr = P.pairs[T.pair];
+            const int w = ch.width, R = P.runs[u.run].rows;
+            K = (w + XTED_STRIPE - 1) / XTED_STRIPE;
+            int32_t *expmap = P.gang_buf;
+            // mark the far columns that cross a stripe boundary, then number them
+            for (int c = tid; c < w; c += XTED_CTA_THREADS) expmap[c] = 0;
+            __syncthreads();
+            {
+                const int2 *nodes = P.rowinfo + pr.col_base;
+                const int j0 = __ldg(&P.krd[ch.k_lo]);
+                for (int c = tid; c < w; c += XTED_CTA_THREADS) {
+                    const int j = j0 + c;
+                    const int f = c + ((__ldg(&nodes[j]).y & XTED_ROW_ORL_MASK) + 1 - j);
+                    if (f < w && f / XTED_STRIPE != c / XTED_STRIPE) expmap[f] = 1;
+                }
+            }
+            __syncthreads();
+            const int per = (w + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS;
+            const int a0 = min(tid * per, w), a1 = min(a0 + per, w);
+            int cnt = 0;
+            for (int c = a0; c < a1; c++) cnt += expmap[c];
+            // block exclusive scan of cnt (warp scan, then the warps' totals)
+            const int lane = tid & 31, warp = tid >> 5;
+            const int incl = warp_prefix_sum(cnt, lane);
+            if (lane == 31) S.ends[warp] = incl;
+            __syncthreads();
+            int before = incl - cnt;
+            for (int q = 0; q < warp; q++) before += S.ends[q];
+            int total = 0;
+            for (int q = 0; q < XTED_WARPS; q++) total += S.ends[q];
+            for (int c = a0; c < a1; c++) {
+                const int m = expmap[c];
+                expmap[c] = m ? before : -1;
+                before += m;
+            }
+            X = total;
+            const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
+            const int64_t need = wal + 32 + 2 * (int64_t)K * R + (int64_t)R * X;
+            feasible = K <= P.gang_blocks && need <= P.gang_cap;
+            if (tid < XTED_GANG_MAX) P.gang_buf[wal + tid] = 0;  // progress words
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) {
+            g[XTED_GCTL_DESC + 0] = t;
+            g[XTED_GCTL_DESC + 1] = s_g[3];
+            g[XTED_GCTL_DESC + 2] = K;
+            g[XTED_GCTL_DESC + 3] = X;
+            g[XTED_GCTL_DESC + 4] = feasible;
+            __threadfence();
+        }
+    }
+    if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // B: the layout is ready
+    if (tid == 0) {
+        for (int q = 0; q < 5; q++) s_g[2 + q] = g[XTED_GCTL_DESC + q];
+    }
+    __syncthreads();
+    const int t = s_g[2], e = s_g[3], K = s_g[4], X = s_g[5], feasible = s_g[6];
+    if (t >= 0) {
+        __threadfence();  // acquire: the unit's inputs (complete before it was published) and the layout
+        const XTask T = P.tasks[t];
+        const XUnit u = P.units[T.unit_lo];
+        const XPair pr = P.pairs[T.pair];
+        if (P.trace && b == 0 && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
+        if (feasible) {
+            if (b < K) {
+                const int w = P.chunks[u.chunk].width, R = P.runs[u.run].rows;
+                const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
+                int32_t *prog = P.gang_buf + wal;
+                int32_t *CR = prog + 32;
+                int32_t *FC = CR + (int64_t)K * R;
+                int32_t *E = FC + (int64_t)K * R;
+                run_stripe(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
+            }
+        } else if (b == 0) {
+            dispatch_wide(P, pr, u, scratch, S, ring, cache, cnode);  // too wide or too many exports: one block
+        }
+        __threadfence();
+    }
+    if (b == 0 && tid == 0) {  // the ring slot is consumed before anyone looks for the next unit
+        g[XTED_GCTL_HEAD] = g[XTED_GCTL_HEAD] + 1;
+        __threadfence();
+    }
+    if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // C: every stripe is done
+    if (b == 0 && tid == 0 && t >= 0) {
+        complete_task(P, e, P.tasks[t].pair);
+        if (P.trace) trace_task_end(P, t);
+    }
+    __syncthreads();
+}
+
 // Narrow tasks open in a block. The block's warps take units one at a time
 // from any open task and never wait for each other: the warp that finishes a
 // task's last unit completes the task, and a warp that finds no unit left
@@ -1032,6 +1435,7 @@ static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot")
 __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
     __shared__ int s_next, s_k[2];
     __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch;
+    __shared__ int s_gang[8];  // gang protocol: barrier phase, status, descriptor
     __shared__ FlowSlot s_fs[FLOW_SLOTS];
     __shared__ WideShared S[2];
     extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache | column nodes (DP_SMEM_BYTES)
@@ -1052,6 +1456,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         s_lock = -1;
         s_progress = 0;
         s_epoch = 0;
+        s_gang[0] = 0;
     }
     __syncthreads();
     volatile int *vmode = &s_mode, *vlock = &s_lock, *vprog = &s_progress, *vepoch = &s_epoch;
@@ -1082,6 +1487,16 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         if (mode == FLOW_GROUP) {
             __syncwarp();
             __syncthreads();  // every warp is between units
+            if (s_gtask == CLAIM_GANG) {  // this gang block's part in a striped unit
+                run_gang(P, scratch, S[0], s_ring, s_cache, s_cnode, s_gang);
+                __syncthreads();
+                if (tid == 0) {
+                    s_progress++;
+                    *vmode = FLOW_RUN;
+                }
+                __syncthreads();
+                continue;
+            }
             const int t = s_gtask;
             const XTask T = P.tasks[t];
             const XPair pr = P.pairs[T.pair];
@@ -1197,11 +1612,17 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
                 if (ns < XTED_CLAIM_SLEEP_MAX) ns <<= 1;
             }
             if (lane == 0) {
-                if (t >= 0) {
+                if (t == CLAIM_GANG) {
+                    s_gtask = CLAIM_GANG;
+                    __threadfence_block();
+                    *vmode = FLOW_GROUP;
+                } else if (t >= 0) {
                     atomicAdd(&s_progress, 1);
                     const XTask T = P.tasks[t];
                     if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
-                    if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
+                    if ((T.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 && gang_push(P, t, e)) {
+                        // handed to the gang: its blocks run it in stripes
+                    } else if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
                         s_gtask = t;
                         s_gentry = e;
                         s_next = 0;

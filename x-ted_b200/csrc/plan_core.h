@@ -363,6 +363,7 @@ struct LevelCtx {
     const DPair *pairs;
     int32_t narrow_width;
     int32_t wide_rows;  // narrow-chunk units of runs longer than this are wide tasks (< 0: none)
+    int64_t stripe_min_cells = 0;  // > 0: wide single-segment units with this many cells run in stripes
 };
 
 // A unit of a narrow chunk whose run is long (one big keyroot) would keep a
@@ -499,7 +500,12 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
                 }
             for (int32_t c = cw_lo; c < cw_hi; c++) {
                 units[u] = XUnit{r, c};
-                tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
+                uint32_t kind = XTED_TASK_WIDE | 1u;
+                const int32_t w = C.chunks[c].width;
+                if (C.stripe_min_cells > 0 && w > XTED_WIDE_REG_MAX && w <= XTED_GANG_MAX * XTED_STRIPE &&
+                    (int64_t)C.runs[r].rows * w >= C.stripe_min_cells)
+                    kind |= XTED_TASK_STRIPED;
+                tasks[t++] = XTask{E.pair, E.entry, kind, u};
                 u++;
             }
         }

@@ -372,6 +372,8 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     C.pairs = d_pairs;
     C.narrow_width = c->opts.narrow_width;
     C.wide_rows = c->opts.wide_rows > 0 ? c->opts.wide_rows : -1;
+    C.stripe_min_cells = c->opts.stripe_min_cells < 0 ? 0
+                         : (c->opts.stripe_min_cells > 0 ? c->opts.stripe_min_cells : XTED_GANG_MIN_CELLS_DEFAULT);
     if (nent > 0) {
         k_level_expand<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv);
         k_level_count<<<blocks_for(nent, BS), BS, 0, s>>>(C, d_lv, nent, d_units, d_tasks);
@@ -394,6 +396,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     const size_t rq_slots = (size_t)XTED_BUCKETS << rq_log2;
     rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
                                          8 * rq_slots + 4 * (2 * E1 + (size_t)npairs + 2 * XTED_BUCKETS + 8) +
+                                         4 * XTED_GCTL_INTS +
                                          8 * 256);
     if (rc) return rc;
     Carver cw{(char *)c->work.p};
@@ -403,6 +406,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     int32_t *d_state = cw.take<int32_t>(2 * E1);  // claimed, done per entry
     unsigned long long *d_rq = cw.take<unsigned long long>(rq_slots);
     int32_t *d_ctl = cw.take<int32_t>(2 * XTED_BUCKETS + 8);  // heads/tails, then the done counter
+    int32_t *d_gctl = cw.take<int32_t>(XTED_GCTL_INTS);       // striped units: ring, barrier, descriptor
     if (nent > 0) k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out);
     k_pair_finalize<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_xpairs,
                                                                        d_trivial, d_first);
@@ -427,6 +431,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.rq_log2 = rq_log2;
     K.rq_ctl = d_ctl;
     K.done_total = d_ctl + 2 * XTED_BUCKETS;
+    K.gang_ctl = d_gctl;
     c->d_trivial = d_trivial;
     c->plan_dt_elems = hs->dt_elems;
     c->plan_stack_rows = std::max(hs->stack_rows, 1);

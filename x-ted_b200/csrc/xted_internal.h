@@ -81,6 +81,23 @@ struct XUnit {
 };
 
 #define XTED_TASK_WIDE 0x80000000u  // one unit run by the whole block
+#define XTED_TASK_STRIPED 0x20000000u  // (with WIDE) the unit runs in column stripes on the gang blocks
+// Striped units: a single column segment wider than the register paths split
+// into XTED_STRIPE-column stripes, one per gang block (blocks 0 .. gang_blocks-1
+// of the launch), run concurrently with the stripes' row carries passed right
+// to left through the gang buffer.
+#define XTED_STRIPE 2048
+#define XTED_GANG_MAX 16
+#define XTED_GANG_RING 256
+#define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 24)
+// gang control words: ring tail, ring head, barrier count, descriptor, then
+// the ring (XTED_GANG_RING slots of 4 ints: tag, task, entry, 0)
+#define XTED_GCTL_TAIL 0
+#define XTED_GCTL_HEAD 1
+#define XTED_GCTL_BAR 2
+#define XTED_GCTL_DESC 4   // task, entry, stripes, exports, feasible (5 ints)
+#define XTED_GCTL_RING 16
+#define XTED_GCTL_INTS (XTED_GCTL_RING + 4 * XTED_GANG_RING)
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
 #define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
 #define XTED_HALF_DEFAULT 512       // default limit: wider chunks run faster on the whole block
@@ -148,6 +165,11 @@ struct XKernelParams {
     int32_t *error_info;  // [4] diagnostics of the first error
     uint64_t timeout_ns;  // bound on every idle wait
     unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, info
+    // ---- striped units (gang_blocks = 0: a striped unit runs on one block) ----
+    int32_t gang_blocks;    // blocks 0 .. gang_blocks-1 run striped units together
+    int32_t *gang_ctl;      // XTED_GCTL_INTS words, zeroed per run
+    int32_t *gang_buf;      // export map, progress, carries, first columns, exported far values
+    int64_t gang_cap;       // ints in gang_buf
     // ---- serving session (serve = 1); a batch launch leaves these zero ----
     int32_t serve;
     int32_t serve_pairs;    // pairs per query slot (the corpus size)

@@ -41,7 +41,8 @@ class COpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("orientation", ctypes.c_int32),
                 ("narrow_width", ctypes.c_int32), ("run_rows", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("wide_rows", ctypes.c_int32), ("half_width", ctypes.c_int32), ("tuned", ctypes.c_int32),
-                ("wait_timeout_s", ctypes.c_double), ("mem_limit", ctypes.c_int64)]
+                ("wait_timeout_s", ctypes.c_double), ("mem_limit", ctypes.c_int64),
+                ("stripe_min_cells", ctypes.c_int64)]
 
 
 class CStats(ctypes.Structure):

@@ -29,7 +29,8 @@ class Context:
     def __init__(self, device: int = 0, orientation: int = _lib.ORIENT_AUTO,
                  narrow_width: Optional[int] = None, run_rows: Optional[int] = None,
                  ctas_per_sm: int = 0, wait_timeout_s: float = 20.0, mem_limit: int = 0,
-                 wide_rows: int = 0, half_width: int = 0, tuned: Optional[bool] = None):
+                 wide_rows: int = 0, half_width: int = 0, tuned: Optional[bool] = None,
+                 stripe_min_cells: int = 0):
         L = _lib.lib()
         o = _lib.COpts()
         L.xted_opts_default(ctypes.byref(o))
@@ -48,6 +49,7 @@ class Context:
         o.tuned = 1 if tuned else 0
         o.wait_timeout_s = wait_timeout_s
         o.mem_limit = mem_limit
+        o.stripe_min_cells = stripe_min_cells
         self.opts = o
         h = ctypes.c_void_p()
         _lib.check(L.xted_create(ctypes.byref(h), ctypes.byref(o)), "xted_create")
