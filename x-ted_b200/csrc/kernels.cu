@@ -1036,6 +1036,7 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 #define CTL_IDLE (2 * XTED_BUCKETS + 1)     // blocks currently idle (or gone)
 #define CTL_LEAVING (2 * XTED_BUCKETS + 2)  // nonzero once blocks have started to leave
 
+template <bool STRIPES>
 __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lane) {
     // Called by a whole warp; lane 0 claims, the warp reads every bucket's
     // head and tail in one coalesced load so that only non-empty buckets are
@@ -1052,7 +1053,7 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
         if (lane == 0) {
             if (*(volatile int32_t *)P.error != 0) {
                 res = CLAIM_EXIT;
-            } else if ((int)blockIdx.x < P.gang_blocks &&
+            } else if (STRIPES && (int)blockIdx.x < P.gang_blocks &&
                        ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_TAIL] > ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_HEAD]) {
                 if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
                 res = CLAIM_GANG;  // every gang block takes part in every striped unit
@@ -1432,7 +1433,11 @@ struct FlowSlot {
 };
 static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot");
 
-__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) {
+// The persistent DP kernel. Two instantiations: without striped units (every
+// batch whose column segments fit the register paths: the gang code is left
+// out of the hot loop entirely), and with them.
+template <bool STRIPES>
+__device__ __forceinline__ void dp_main(const XKernelParams &P) {
     __shared__ int s_next, s_k[2];
     __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch;
     __shared__ int s_gang[8];  // gang protocol: barrier phase, status, descriptor
@@ -1487,7 +1492,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
         if (mode == FLOW_GROUP) {
             __syncwarp();
             __syncthreads();  // every warp is between units
-            if (s_gtask == CLAIM_GANG) {  // this gang block's part in a striped unit
+            if (STRIPES && s_gtask == CLAIM_GANG) {  // this gang block's part in a striped unit
                 run_gang(P, scratch, S[0], s_ring, s_cache, s_cnode, s_gang);
                 __syncthreads();
                 if (tid == 0) {
@@ -1605,7 +1610,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
                 busy = __shfl_sync(FULLMASK, busy, 0);
                 if (stop == 2) t = CLAIM_EXIT;
                 if (stop) break;
-                t = claim_task(P, &e, !busy, lane);
+                t = claim_task<STRIPES>(P, &e, !busy, lane);
                 if (t != CLAIM_NONE) break;
                 __nanosleep(ns);  // nothing ready while units of this block run: poll again soon
                 __syncwarp();
@@ -1620,7 +1625,7 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
                     atomicAdd(&s_progress, 1);
                     const XTask T = P.tasks[t];
                     if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
-                    if ((T.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 && gang_push(P, t, e)) {
+                    if (STRIPES && (T.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 && gang_push(P, t, e)) {
                         // handed to the gang: its blocks run it in stripes
                     } else if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
                         s_gtask = t;
@@ -1689,6 +1694,9 @@ __global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelPar
     cp_async_wait<0>();
 }
 
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) { dp_main<false>(P); }
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel_striped(XKernelParams P) { dp_main<true>(P); }
+
 // Result of pair p: Dtree[0][0] of its table (X-TED_CPU/TED.cpp:188).
 __global__ void xted_gather_kernel(const XPair *pairs, const int32_t *trivial, const int32_t *dt,
                                    int npairs, int32_t *out) {
@@ -1702,8 +1710,14 @@ __global__ void xted_gather_kernel(const XPair *pairs, const int32_t *trivial, c
 int dp_occupancy(int *blocks_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(xted_dp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_BYTES);
     if (e != cudaSuccess) return (int)e;
-    return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, xted_dp_kernel, XTED_CTA_THREADS,
-                                                               DP_SMEM_BYTES);
+    e = cudaFuncSetAttribute(xted_dp_kernel_striped, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_BYTES);
+    if (e != cudaSuccess) return (int)e;
+    int other = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&other, xted_dp_kernel_striped, XTED_CTA_THREADS, DP_SMEM_BYTES);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, xted_dp_kernel, XTED_CTA_THREADS, DP_SMEM_BYTES);
+    if (e == cudaSuccess && other < *blocks_per_sm) *blocks_per_sm = other;  // one grid size for both
+    return (int)e;
 }
 
 // Cooperative launch (every block resident at once), expressed as a launch
@@ -1721,7 +1735,8 @@ cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, (const void *)xted_dp_kernel, args);
+    return cudaLaunchKernelExC(&cfg, P.gang_blocks > 0 ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel,
+                               args);
 }
 
 cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s) {
