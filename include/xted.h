@@ -83,7 +83,7 @@ typedef struct xted_opts {
     int64_t stripe_min_cells; /* a table whose column segment is wider than
                                2,048 and whose unit has at least this many
                                cells runs in 2,048-column stripes on up to 16
-                               blocks at once (0 = 2^24; < 0: one block)    */
+                               blocks at once (0 = 2^20; < 0: one block)    */
 } xted_opts;
 
 typedef struct xted_ctx xted_ctx;

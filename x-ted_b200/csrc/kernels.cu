@@ -584,10 +584,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 __device__ __forceinline__ bool wait_progress(const XKernelParams &P, volatile int32_t *prog, int want) {
     const uint64_t t0 = global_ns();
     for (long it = 0; it < (1L << 26); it++) {
-        if (prog[0] >= want) {
-            __threadfence();  // acquire: the neighbour's row outputs are visible from here on
-            return true;
-        }
+        if (ld_acquire((const int32_t *)prog) >= want) return true;  // acquire: the neighbour's row outputs
         if (*(volatile int32_t *)P.error != 0) return false;
         if (global_ns() - t0 > P.timeout_ns) break;
         __nanosleep(32);
@@ -648,6 +645,10 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const int2 *rows = P.rowinfo + pr.row_base;
     volatile int32_t *prog_right = prog + s + 1;
     int tflat = 0;
+    // thread 0: the right neighbour's carry and first column of the current
+    // row, loaded at the row's start when that stripe is already past it
+    int cin_pf = XTED_INF, fc_pf = 0;
+    bool have_pf = false;
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
@@ -676,6 +677,11 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                     issue_row<W>(cnode, tw, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
                                  gtid == 0);
                 cp_async_commit();
+            }
+            if (gtid == 0 && right && ld_acquire((const int32_t *)prog_right) >= tflat + 1) {
+                cin_pf = __ldcg(CR + (int64_t)(s + 1) * R + tflat);
+                fc_pf = __ldcg(FC + (int64_t)(s + 1) * R + tflat);
+                have_pf = true;
             }
             const int32_t *slot = ring + (i & (PF - 1)) * GSLOT;
             const int2 ri = *(const int2 *)(slot + GROW);
@@ -711,9 +717,12 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
             if (gtid == 0) {
-                int cin = XTED_INF;
-                if (right && wait_progress(P, prog_right, tflat + 1)) cin = __ldcg(CR + (int64_t)(s + 1) * R + tflat);
-                S.cin = cin;
+                if (right && !have_pf && wait_progress(P, prog_right, tflat + 1)) {
+                    cin_pf = __ldcg(CR + (int64_t)(s + 1) * R + tflat);
+                    fc_pf = __ldcg(FC + (int64_t)(s + 1) * R + tflat);
+                }
+                S.cin = right ? cin_pf : XTED_INF;
+                have_pf = false;
             }
             __syncthreads();
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
@@ -774,11 +783,13 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                 if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
             }
             // the next row's diagonal at C1: the right neighbour's first column of this row
-            if (gtid == 0 && right) S.first[G] = __ldcg(FC + (int64_t)(s + 1) * R + tflat);
-            __threadfence();          // this row's outputs, before the progress word
+            if (gtid == 0 && right) S.first[G] = fc_pf;
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
-            __syncthreads();          // ... and everyone's, the record and the stack push
-            if (gtid == 0 && left) ((volatile int32_t *)prog)[s] = tflat + 1;
+            __syncthreads();          // ... and everyone's, the record and the stack push; this row's outputs
+            if (gtid == 0 && left) {  // one fence after the barrier orders the whole block's outputs
+                __threadfence();
+                ((volatile int32_t *)prog)[s] = tflat + 1;
+            }
         }
     }
     cp_async_wait<0>();
@@ -1241,11 +1252,12 @@ __device__ void trace_task_end(const XKernelParams &P, int t) {
 // gang blocks (0 .. gang_blocks-1) notice pending units when they look for
 // work, meet at a barrier, the leader (block 0) lays the unit out, and each
 // block runs one stripe. One striped unit at a time.
-__device__ bool gang_push(const XKernelParams &P, int t, int e) {
+__device__ bool gang_push(const XKernelParams &P, int t, int e, bool small) {
     volatile int32_t *g = P.gang_ctl;
+    const int limit = small ? XTED_GANG_SMALL_QUEUE : XTED_GANG_RING;
     for (int it = 0; it < 1024; it++) {
         const int tl = g[XTED_GCTL_TAIL], hd = g[XTED_GCTL_HEAD];
-        if (tl - hd >= XTED_GANG_RING) return false;
+        if (tl - hd >= limit) return false;
         if (atomicCAS(&P.gang_ctl[XTED_GCTL_TAIL], tl, tl + 1) == tl) {
             volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (tl & (XTED_GANG_RING - 1));
             slot[1] = t;
@@ -1625,7 +1637,9 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                     atomicAdd(&s_progress, 1);
                     const XTask T = P.tasks[t];
                     if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
-                    if (STRIPES && (T.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 && gang_push(P, t, e)) {
+                    if (STRIPES && (T.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 &&
+                        gang_push(P, t, e, (int64_t)P.runs[P.units[T.unit_lo].run].rows *
+                                                   P.chunks[P.units[T.unit_lo].chunk].width < XTED_GANG_BIG_CELLS)) {
                         // handed to the gang: its blocks run it in stripes
                     } else if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
                         s_gtask = t;

@@ -89,7 +89,13 @@ struct XUnit {
 #define XTED_STRIPE 2048
 #define XTED_GANG_MAX 16
 #define XTED_GANG_RING 256
-#define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 24)
+#define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
+// Units under XTED_GANG_BIG_CELLS go to the gang only while fewer than
+// XTED_GANG_SMALL_QUEUE units wait for it (the gang runs one unit at a time;
+// when many are ready, one block each in parallel is faster); bigger ones
+// always queue.
+#define XTED_GANG_BIG_CELLS ((int64_t)1 << 24)
+#define XTED_GANG_SMALL_QUEUE 4
 // gang control words: ring tail, ring head, barrier count, descriptor, then
 // the ring (XTED_GANG_RING slots of 4 ints: tag, task, entry, 0)
 #define XTED_GCTL_TAIL 0
