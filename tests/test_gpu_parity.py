@@ -235,3 +235,16 @@ def test_striped_equals_one_block_on_20000_node_pairs():
     with xted.Context() as c:
         striped = c.distance_batch(pairs)
     assert list(one) == list(striped)
+
+
+@pytest.mark.parametrize("shape", ["deep", "wide"])
+def test_striped_deep_and_wide_shapes(shape):
+    """Forced stripes on a deep-narrow tree (many far columns cross stripe
+    boundaries) and a wide-shallow one (short subtrees), as either tree of the
+    pair, against the oracle."""
+    a = gen.tree(shape, 2600, 7, "uniform", 8)
+    b = gen.tree("random", 2500, 8, "uniform", 8)
+    with xted.Context(stripe_min_cells=1) as c:
+        got = c.distance_batch([(a, b), (b, a)])
+    want = oracle.distance(a, b)
+    assert list(got) == [want, want]
