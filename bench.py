@@ -233,6 +233,39 @@ def cpu_reference(pairs, budget_s: float, stride: int):
                                  f"{ncpu} threads per pair"}
 
 
+def _ref_pair_worker(pair):
+    """One pair on the reference X-TED_CPU with one thread (a spawned worker
+    process: the reference's harness captures std::cout, one call per process)."""
+    import oracle
+    a, b = pair
+    return oracle.ref_distance(a, b, num_threads=1)[0] if oracle.ref_available() else oracle.distance(a, b)
+
+
+def cpu_reference_pair_parallel(pairs, budget_s: float, stride: int):
+    """The reference X-TED_CPU with one thread per pair and one worker process
+    per host core, pairs spread over the workers, on the same strided sample.
+    Returns (pairs/s, info)."""
+    import multiprocessing as mp
+    import oracle
+    ncpu = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    sample = pairs[::stride]
+    ctx = mp.get_context("spawn")  # after CUDA is up in this process: never fork
+    done = 0
+    with ctx.Pool(ncpu) as pool:
+        pool.map(_ref_pair_worker, sample[:ncpu])  # workers up and the library loaded
+        t0 = time.perf_counter()
+        for _ in pool.imap_unordered(_ref_pair_worker, sample, chunksize=1):
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        dt = time.perf_counter() - t0
+        pool.terminate()
+    return done / dt, {"kind": kind, "cores": ncpu, "pairs": done, "seconds": round(dt, 3),
+                       "sample": f"every {stride}th pair of the workload, {done} pairs in {dt:.1f} s, "
+                                 f"1 thread per pair, {ncpu} worker processes (pair-parallel)"}
+
+
 def serve_bench(ctx, budget_s: float = 30.0, seed: int = 6):
     """Serving: a corpus of 1,000 resident trees (sizes uniform 100-1,000, mixed
     shapes, Zipf(1.1) labels over 1,000 ids) and an open-loop Poisson stream of
@@ -436,12 +469,15 @@ def main():
                  "sample": f"every {args.plain_stride}th pair ({len(sample)} pairs), one xted_distance call each"}
 
     # ---- CPU baseline (reference X-TED_CPU), rank 0 at N = 1 ----
-    cpu = None
+    cpu = cpu_pp = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         stride = 32 if npairs > 256 else 1
         v, info = cpu_reference(pairs, args.ref_budget, stride)
         cpu = {"value": round(v, 3), "unit": "pairs/s", "cores": info["cores"], "kind": info["kind"],
                "sample": info["sample"]}
+        vp, infop = cpu_reference_pair_parallel(pairs, min(args.ref_budget, 15.0), stride)
+        cpu_pp = {"value": round(vp, 3), "unit": "pairs/s", "cores": infop["cores"], "kind": infop["kind"],
+                  "sample": infop["sample"]}
 
     # ---- serving (1 GPU) ----
     serve = None
@@ -470,6 +506,7 @@ def main():
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,
                      "kernel": "xted_dp_kernel", "bytes_per_cell": BYTES_PER_CELL},
         "cpu_baseline": cpu,
+        "cpu_baseline_pair_parallel": cpu_pp,  # the same reference code, 1 thread per pair x all cores
         "serve": serve,
         "gpu_launches": 3 * args.steps,  # ready-queue init, DP, gather per step
         "clocks": clk.summary(),
