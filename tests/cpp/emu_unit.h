@@ -146,4 +146,116 @@ inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vecto
     }
 }
 
+// The same unit (one column segment) computed in column stripes of S columns
+// the way the kernels' multi-block path does it: stripes right to left, each
+// with its own rows and far-row stack, the row's suffix minimum continued
+// from the stripe to the right (its carry per row), the tree rows' diagonal at
+// a stripe's last column from the right stripe's first column one row below,
+// and far columns owned by a stripe to the right read from that stripe's
+// values kept per pushed row. Writes the unit's tree distances into dtv.
+inline void run_unit_striped(const Pools &H, const XPair &pr, const XUnit &u, std::vector<int32_t> &dtv, int S) {
+    int32_t *dt = dtv.data() + pr.dt_off;
+    const XRun run = H.runs[(size_t)u.run];
+    const XChunk ch = H.chunks[(size_t)u.chunk];
+    if (ch.nseg != 1) FAIL("striped unit with %d segments", ch.nseg);
+    const int W = ch.width, n = pr.n;
+    const int2 *cn = H.node + pr.col_base;
+    const int2 *rn = H.node + pr.row_base;
+    const int j0 = H.krd[(size_t)ch.k_lo];
+    std::vector<int> node(W), lab(W), foff(W), dend(W);
+    for (int c = 0; c < W; c++) {
+        const int j = j0 + c;
+        node[c] = j;
+        lab[c] = cn[j].x;
+        foff[c] = (cn[j].y & XTED_ROW_ORL_MASK) + 1 - j;
+        dend[c] = W - c;
+    }
+    const int K = (W + S - 1) / S, R = run.rows;
+    // exported columns: far columns of some column in a stripe further left
+    std::vector<char> exported(W, 0);
+    for (int c = 0; c < W; c++) {
+        const int f = c + foff[c];
+        if (f < W && f / S != c / S) exported[f] = 1;
+    }
+    std::vector<std::vector<int>> CR((size_t)K, std::vector<int>((size_t)R, -999)), FC = CR;
+    std::vector<std::vector<int>> E((size_t)R, std::vector<int>((size_t)W, -999));
+    for (int st = K - 1; st >= 0; st--) {
+        const int C0 = st * S, C1 = std::min(C0 + S, W), w = C1 - C0;
+        const bool right = st + 1 < K;
+        std::vector<int> prev(w), loc(w);
+        int tflat = 0;
+        for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+            const int i0 = H.krd[(size_t)kr];
+            const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
+            const int tbase = tflat;
+            for (int c = 0; c < w; c++) prev[c] = dend[C0 + c];
+            int edge = right ? dend[C1] : 0;  // D[i+1][C1]: the bottom border first
+            std::vector<std::vector<int>> stk;
+            for (int i = imax - 1; i >= i0; i--, tflat++) {
+                const int2 ri = rn[i];
+                const int ro = ri.y & XTED_ROW_ORL_MASK;
+                const bool trow = ro == imax - 1;
+                const int bord = imax - i, rowfar = imax - ro - 1;
+                int runmin = XTED_INF;
+                for (int lc = w - 1; lc >= 0; lc--) {
+                    const int c = C0 + lc;
+                    const bool se = dend[c] == 1;
+                    const int diag = se ? bord - 1 : (lc + 1 < w ? prev[lc + 1] : edge);
+                    const bool tcol = foff[c] == dend[c];
+                    int a;
+                    if (trow && tcol) {
+                        a = diag + (ri.x != lab[c]);
+                    } else {
+                        int fv;
+                        if (trow) fv = dend[c] - foff[c];
+                        else if (tcol) fv = rowfar;
+                        else {
+                            const int f = c + foff[c];
+                            if (f < C1) {
+                                if (stk.empty()) FAIL("stripe stack underflow");
+                                fv = stk.back()[(size_t)(f - C0)];
+                            } else {
+                                if (!exported[f]) FAIL("far column %d not exported", f);
+                                fv = E[(size_t)(tbase + (imax - 1 - (ro + 1)))][(size_t)f];
+                                if (fv == -999) FAIL("exported far value read before it was written");
+                            }
+                        }
+                        const int dv = dt[(size_t)i * n + node[c]];
+                        if (dv < 0) FAIL("tree distance (%d,%d) read before it was written", i, node[c]);
+                        a = dv + fv;
+                    }
+                    int Av = std::min(a, prev[lc] + 1);
+                    if (se) Av = std::min(Av, bord + 1);
+                    runmin = std::min(runmin, Av + c);
+                    loc[lc] = runmin;
+                }
+                int carry = XTED_INF;
+                if (right) {
+                    carry = CR[(size_t)st + 1][(size_t)tflat];
+                    if (carry == -999) FAIL("carry of the right stripe missing");
+                }
+                for (int lc = 0; lc < w; lc++) {
+                    const int c = C0 + lc;
+                    prev[lc] = std::min(loc[lc], carry) - c;
+                    if (trow && foff[c] == dend[c]) {
+                        int32_t &slot = dt[(size_t)i * n + node[c]];
+                        if (slot >= 0) FAIL("tree distance (%d,%d) written twice", i, node[c]);
+                        slot = prev[lc];
+                    }
+                }
+                CR[(size_t)st][(size_t)tflat] = prev[0] + C0;
+                FC[(size_t)st][(size_t)tflat] = prev[0];
+                if (right) edge = FC[(size_t)st + 1][(size_t)tflat];
+                if (i != i0 && (ri.y & XTED_ROW_ISKR)) stk.pop_back();
+                if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
+                    stk.push_back(prev);
+                    for (int lc = 0; lc < w; lc++)
+                        if (exported[C0 + lc]) E[(size_t)tflat][(size_t)(C0 + lc)] = prev[lc];
+                }
+            }
+            if (!stk.empty()) FAIL("stripe stack not empty at table end");
+        }
+    }
+}
+
 }  // namespace emu

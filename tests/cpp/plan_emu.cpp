@@ -200,6 +200,7 @@ int main(int argc, char **argv) {
     const int maxn = argc > 2 ? std::atoi(argv[2]) : 300;
     std::mt19937_64 g(argc > 3 ? (uint64_t)std::atoll(argv[3]) : 12345);
     int64_t pairs_checked = 0;
+    int64_t stripes_checked = 0;
     const int nws[4] = {0, 7, 64, XTED_NARROW_MAX};
     for (int it = 0; it < iters; it++) {
         const int ntrees = 1 + (int)(g() % 8);
@@ -265,8 +266,24 @@ int main(int argc, char **argv) {
                 const emu::Pools EP{H.node.data(), H.krd.data(), H.cumw.data(), H.runs.data(), H.chunks.data(),
                                     H.stack_rows};
                 for (int u = 0; u < nu; u++) {
-                    unit_seen[(size_t)(t.unit_lo + u)]++;
-                    emu::run_unit(EP, x, H.units[(size_t)(t.unit_lo + u)], dt, g_table ? XTED_NARROW_MAX : nw, wide);
+                    const int ui = t.unit_lo + u;
+                    unit_seen[(size_t)ui]++;
+                    const XUnit &U = H.units[(size_t)ui];
+                    const XChunk &UC = H.chunks[(size_t)U.chunk];
+                    // every fourth single-segment unit is also computed in column stripes
+                    // (multi-block path) on a copy of the pair's table: same tree distances
+                    std::vector<int32_t> alt;
+                    if (UC.nseg == 1 && UC.width >= 4 && ui % 4 == 0) {
+                        alt.assign(dt.begin() + x.dt_off, dt.begin() + x.dt_off + (int64_t)x.m * x.n);
+                        XPair x0 = x;
+                        x0.dt_off = 0;
+                        static const int kStripe[4] = {2, 3, 5, 16};
+                        emu::run_unit_striped(EP, x0, U, alt, kStripe[(ui / 4) % 4]);
+                        stripes_checked++;
+                    }
+                    emu::run_unit(EP, x, U, dt, g_table ? XTED_NARROW_MAX : nw, wide);
+                    if (!alt.empty() && !std::equal(alt.begin(), alt.end(), dt.begin() + x.dt_off))
+                        FAIL("striped unit %d (width %d) differs from the one-block unit", ui, UC.width);
                 }
             }
             level_done[(size_t)E.pair] = E.level;
@@ -291,6 +308,6 @@ int main(int argc, char **argv) {
             pairs_checked++;
         }
     }
-    std::printf("ok %lld pairs\n", (long long)pairs_checked);
+    std::printf("ok %lld pairs, %lld striped units\n", (long long)pairs_checked, (long long)stripes_checked);
     return 0;
 }

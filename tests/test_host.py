@@ -113,7 +113,9 @@ def test_context_without_device_fails_loudly():
 def test_planner_emulation_matches_oracle(tmp_path):
     """Runs the batch planner's functions (plan_core.h, the code of the device
     planning kernels) sequentially with a CPU emulation of the unit execution
-    (tests/cpp/plan_emu.cpp) and checks distances and plan invariants."""
+    (tests/cpp/plan_emu.cpp) and checks distances and plan invariants; every
+    fourth single-segment unit is also computed in column stripes of 2-16
+    columns (the multi-block decomposition) and must write the same table."""
     obj = tmp_path / "xo.o"
     exe = tmp_path / "plan_emu"
     subprocess.run(["gcc", "-O2", "-c", os.path.join(REPO, "oracle", "xted_oracle.c"), "-o", str(obj)], check=True)
