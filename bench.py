@@ -480,8 +480,11 @@ def main():
     # ---- serving (1 GPU) ----
     serve = None
     if world == 1 and not args.no_serve:
-        serve = serve_bench(ctx, args.serve_budget)
-        if not args.no_cpu_baseline:
+        try:
+            serve = serve_bench(ctx, args.serve_budget)
+        except Exception as ex:  # reported in the line; the batch numbers above stand on their own
+            serve = {"error": f"{type(ex).__name__}: {ex}"[:300]}
+        if not args.no_cpu_baseline and "error" not in serve:
             serve["cpu_baseline"] = serve_cpu_baseline(min(args.ref_budget, 10.0))
 
     # pair-parallel reference variant: worker processes, after every GPU phase
