@@ -453,8 +453,10 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
         progress = true;
     }
     if (progress) s->cv_done.notify_all();
-    // 2. the launch: notice its end (and any error), relaunch for work in flight
-    if (s->running && cudaEventQuery(s->kev) == cudaSuccess) {
+    // 2. the launch: notice its end (and any error), relaunch for work in flight.
+    // One query: the launch may end between two of them.
+    const cudaError_t kq = s->running ? cudaEventQuery(s->kev) : cudaErrorNotReady;
+    if (s->running && kq == cudaSuccess) {
         s->running = false;
         int32_t err = 0;
         if (cudaMemcpy(&err, s->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess) err = XTED_ECUDA;
@@ -466,7 +468,7 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
             s->cv_done.notify_all();
             progress = true;
         }
-    } else if (s->running && cudaEventQuery(s->kev) != cudaErrorNotReady) {
+    } else if (s->running && kq != cudaErrorNotReady) {
         cudaGetLastError();
         s->running = false;
         s->error = XTED_ECUDA;
