@@ -2,8 +2,8 @@
 
 Every query's top-k is checked against the oracle's distances (exact, ties by
 lower corpus index), and each query's result must be the same when it runs
-alone as when it runs in a mix with others (north-star requirement for the
-serving loop). All through the C ABI.
+alone as when it runs in a mix with others (continuous batching must not change
+an answer). All through the C ABI.
 """
 import time
 

@@ -29,7 +29,7 @@ def test_restatement_matches_reference_goldens_synthetic(golden_synthetic):
         assert oracle.distance(a, b) == d, name
 
 
-def test_goldens_cover_survey_table(golden_datasets):
+def test_goldens_match_reference_cli_values(golden_datasets):
     got = {name: d for name, _, _, d in golden_datasets}
     # tree pair (0,1) of the sampled datasets, as the reference CLI reports them
     assert got["Sampled_Dataset/1_Swissport/swissport_nodes_1000.txt"] == 767
