@@ -216,3 +216,19 @@ def test_adjacency_parser_rejects_bad_text():
     for bad in ["[[1, 2], [3", "[[1,, 2]]", "[[a]]", "no brackets"]:
         with pytest.raises(xted.XtedError):
             trees.parse_adjacency(bad)
+
+
+def test_bench_cpu_baselines_small_sample():
+    """The benchmark's two CPU baselines of the reference code (its own
+    sequential mode with all cores per pair, and one thread per pair on
+    spawned worker processes) on a small sample: rates and labels."""
+    import bench
+    from xted import gen
+    pairs = [(gen.tree("random", 30 + i, i, "uniform", 8), gen.tree("deep", 25 + i, 100 + i, "uniform", 8))
+             for i in range(12)]
+    v1, i1 = bench.cpu_reference(pairs, 5.0, 1)
+    v2, i2 = bench.cpu_reference_pair_parallel(pairs, 5.0, 1)
+    assert v1 > 0 and v2 > 0
+    assert i1["pairs"] == 12 and i2["pairs"] == 12
+    assert "in sequence" in i1["sample"] and "pair-parallel" in i2["sample"]
+    assert i2["cores"] == (os.cpu_count() or 1)
