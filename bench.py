@@ -122,29 +122,40 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(name: str, rank: int):
-    from xted import gen
-    if name == "batched":
-        return gen.mixed_batch(4096, seed=4 + 1000 * rank), {
-            "workload": "4096 mixed pairs, sizes log-uniform 50-2000, 4 shapes, Zipf(1.1) over 1000 labels",
-            "npairs": 4096, "seed": 4 + 1000 * rank}
-    if name == "batched256":
-        return gen.mixed_batch(256, seed=4 + 1000 * rank), {
-            "workload": "256 mixed pairs (same distribution as the 4096-pair batch; profiling size)",
-            "npairs": 256, "seed": 4 + 1000 * rank}
-    if name == "batched1024":
-        return gen.mixed_batch(1024, seed=4 + 1000 * rank), {
-            "workload": "1024 mixed pairs (same distribution as the 4096-pair batch; profiling size)",
-            "npairs": 1024, "seed": 4 + 1000 * rank}
+def make_workload_config(name: str, rank: int):
+    """(generator call, config) of a named workload; nothing is built here."""
+    seed = 4 + 1000 * rank
+    if name in ("batched", "batched256", "batched1024"):
+        npairs = {"batched": 4096, "batched256": 256, "batched1024": 1024}[name]
+        desc = ("4096 mixed pairs, sizes log-uniform 50-2000, 4 shapes, Zipf(1.1) over 1000 labels" if npairs == 4096
+                else f"{npairs} mixed pairs (same distribution as the 4096-pair batch; profiling size)")
+        return ("mixed_batch", npairs, seed), {"workload": desc, "npairs": npairs, "seed": seed}
     if name == "single100":
-        return [gen.single_pair_100()], {"workload": "one pair, 100 vs 100 random recursive, 26 labels"}
+        return ("single100",), {"workload": "one pair, 100 vs 100 random recursive, 26 labels"}
     if name == "single1000":
-        return [gen.single_pair_1000()], {"workload": "one pair, 1000 wide-shallow vs 1000 deep-narrow, "
-                                                       "Zipf(1.1) over 10000 labels"}
+        return ("single1000",), {"workload": "one pair, 1000 wide-shallow vs 1000 deep-narrow, "
+                                              "Zipf(1.1) over 10000 labels"}
     if name == "single20000":
-        return [gen.single_pair_20000(shape="random"), gen.single_pair_20000(shape="caterpillar")], {
+        return ("single20000",), {
             "workload": "20000 vs 20000 random recursive + 20000 vs 20000 caterpillar, 64 labels"}
     raise SystemExit(f"unknown workload {name}")
+
+
+def arm_config(cfg: dict, world: int) -> dict:
+    """The `config` object of the bench line, the same for both arms."""
+    return dict(cfg, l2="distance tables exceed L2 (no flush)", parallelism=f"pairs sharded, dp{world}")
+
+
+def make_workload(name: str, rank: int):
+    from xted import gen
+    call, cfg = make_workload_config(name, rank)
+    if call[0] == "mixed_batch":
+        return gen.mixed_batch(call[1], seed=call[2]), cfg
+    if call[0] == "single100":
+        return [gen.single_pair_100()], cfg
+    if call[0] == "single1000":
+        return [gen.single_pair_1000()], cfg
+    return [gen.single_pair_20000(shape="random"), gen.single_pair_20000(shape="caterpillar")], cfg
 
 
 def dist_setup(args):
@@ -202,32 +213,43 @@ def aggregate(npairs: int, steps: int, dev_ms: float, cells: int, world: int):
     return value, gcups, dev_ms_max
 
 
-def cpu_reference(pairs, budget_s: float, stride: int):
+def cpu_reference(pairs, budget_s: float, stride: int, index=None):
     """The reference X-TED_CPU on a strided sample, all host cores per pair
-    (pairs in sequence, the reference's own mode). Returns (pairs/s, info)."""
+    (pairs in sequence, the reference's own mode). `pairs` is the whole
+    workload, or (with `index`) only the pairs at those workload positions.
+    Returns (pairs/s, info); info["distances"] maps workload index ->
+    reference distance, info["level_ms"] sums the reference's own timer
+    ("Total Time for Parallel Computing", X-TED_CPU/parallel_computing.cpp:184)."""
     import oracle
     ncpu = os.cpu_count() or 1
-    sample = pairs[::stride]
+    if index is None:
+        index = list(range(len(pairs)))[::stride]
+        sample = pairs[::stride]
+    else:
+        sample = pairs
     if oracle.ref_available():
         kind = "reference"
 
         def run(a, b):
-            return oracle.ref_distance(a, b, num_threads=ncpu)[0]
+            return oracle.ref_distance(a, b, num_threads=ncpu)
     else:
         kind = "port"
         ncpu = 1
 
         def run(a, b):
-            return oracle.distance(a, b)
-    done = 0
+            return oracle.distance(a, b), -1.0
+    done, level_ms, dist = 0, 0.0, {}
     t0 = time.perf_counter()
-    for a, b in sample:
-        run(a, b)
+    for p, (a, b) in zip(index, sample):
+        d, ms = run(a, b)
+        dist[int(p)] = d
+        level_ms += max(ms, 0.0)
         done += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
     return done / dt, {"kind": kind, "cores": ncpu, "pairs": done, "seconds": round(dt, 3),
+                       "level_ms": round(level_ms, 2), "distances": dist,
                        "sample": f"every {stride}th pair of the workload, first {done} "
                                  f"(time budget {budget_s:.0f} s), pairs in sequence, "
                                  f"{ncpu} threads per pair"}
@@ -285,13 +307,18 @@ def serve_bench(ctx, budget_s: float = 30.0, seed: int = 6):
     # computed, then with exact top-k pruning (the default, kept for the sweep)
     burst = 32
     sat = {}
+    answers = {}  # pool index -> every (ids, dists) answer given for it
+
+    def note(qi, r):
+        answers.setdefault(qi, []).append((r[0].tolist(), r[1].tolist()))
+
     for prune in (0, 2):
         ctx.serve_options(prune=prune)
         st0 = ctx.serve_stats()
         t0 = time.perf_counter()
-        tickets = [ctx.query_submit(pool[i % len(pool)], 10) for i in range(burst)]
-        for t in tickets:
-            ctx.query_wait(t)
+        tickets = [(i % len(pool), ctx.query_submit(pool[i % len(pool)], 10)) for i in range(burst)]
+        for qi, t in tickets:
+            note(qi, ctx.query_wait(t))
         sat_s = time.perf_counter() - t0
         st1 = ctx.serve_stats()
         sat[prune] = (burst / sat_s, (st1["cells"] - st0["cells"]) / sat_s / 1e9,
@@ -314,13 +341,14 @@ def serve_bench(ctx, budget_s: float = 30.0, seed: int = 6):
         while i < nq or pending:
             now = time.perf_counter() - start
             while i < nq and arrivals[i] <= now:
-                pending[ctx.query_submit(pool[rng.randrange(len(pool))], 10)] = True
+                qi = rng.randrange(len(pool))
+                pending[ctx.query_submit(pool[qi], 10)] = qi
                 i += 1
             for tk in list(pending):
                 r = ctx.query_poll(tk)
                 if r is not None:
                     lat.append(r[3])
-                    del pending[tk]
+                    note(pending.pop(tk), r)
                     last_done = time.perf_counter()
             time.sleep(0.0002)
         span = last_done - start
@@ -332,13 +360,111 @@ def serve_bench(ctx, budget_s: float = 30.0, seed: int = 6):
     for r in sweep:
         if r["achieved_qps"] >= 0.9 * r["offered_qps"]:
             sustained = r
-    return {"workload": "corpus 1000 trees U[100,1000] mixed shapes, Zipf(1.1)/1000 labels; Poisson queries "
+    check = serve_check(ctx, corpus, pool, answers)
+    return {"check": check, "workload": "corpus 1000 trees U[100,1000] mixed shapes, Zipf(1.1)/1000 labels; Poisson queries "
                         "U[100,1000], exact top-10", "saturation_qps": round(qps_sat, 2),
             "saturation_gcups": round(gcups_sat, 1), "pruning": "preorder-sequence bound, 2 rounds",
             "pairs_pruned_frac": round(pruned_frac, 3), "saturation_qps_unpruned": round(sat[0][0], 2),
             "sustained_qps": sustained["achieved_qps"],
             "p50_ms": sustained["p50_ms"], "p99_ms": sustained["p99_ms"], "sweep": sweep,
             "launches": ctx.serve_stats()["launches"]}
+
+
+def serve_check(ctx, corpus, pool, answers, nbatch: int = 4):
+    """Checks the serving answers given during the sweep. Queries 0-7 of the
+    pool: every answer against the reference top-10 of the golden fixture
+    (reference X-TED_CPU distances to all 1,000 corpus trees). The first
+    `nbatch` other pool queries that were answered: every answer against the
+    top-10 of the batch path (xted_distance_batch over the query and the whole
+    corpus)."""
+    gold = golden_configs()
+    checked = mism = 0
+    via_gold = via_batch = 0
+    extra = [qi for qi in sorted(answers) if qi >= 8][:nbatch]
+    for qi in sorted(answers):
+        if gold is not None and qi < gold["serve"]["nqueries"]:
+            want = topk(gold["serve"]["distances"][qi], 10)
+            via_gold += len(answers[qi])
+        elif qi in extra:
+            want = topk(ctx.distance_batch([(pool[qi], t) for t in corpus]).tolist(), 10)
+            via_batch += len(answers[qi])
+        else:
+            continue
+        for got in answers[qi]:
+            checked += 1
+            mism += got != want
+    return {"answers_checked": checked, "mismatches": mism, "vs_reference_fixture": via_gold,
+            "vs_batch_path": via_batch}
+
+
+def topk(dist, k):
+    """Exact top-k: ascending distance, ties by lower corpus index."""
+    order = sorted(range(len(dist)), key=lambda i: (dist[i], i))[:k]
+    return ([int(i) for i in order], [int(dist[i]) for i in order])
+
+
+_GOLD = []
+
+
+def golden_configs():
+    """Reference distances of the benchmark workloads (tests/golden/configs.json.gz,
+    made from the reference X-TED_CPU by tests/golden/make_golden.py), or None."""
+    if not _GOLD:
+        import gzip
+        try:
+            with gzip.open(os.path.join(REPO, "tests", "golden", "configs.json.gz"), "rt") as f:
+                _GOLD.append(json.load(f))
+        except OSError:
+            _GOLD.append(None)
+    return _GOLD[0]
+
+
+def golden_parity(workload: str, rank: int, out):
+    """Distances of the timed run against the golden fixture's reference
+    distances for the same workload (rank 0's seed), or None when the fixture
+    has none for it."""
+    import numpy as np
+    gold = golden_configs()
+    if gold is None or rank != 0:
+        return None
+    if workload == "batched":
+        want = np.array(gold["batch4096"]["distances"], np.int32)
+    elif workload in ("single1000", "single20000"):
+        d = {c["name"]: c["distance"] for c in gold["singles"]}
+        want = np.array([d["single1000"]] if workload == "single1000" else
+                        [d["single20000_random"], d["single20000_caterpillar"]], np.int32)
+    else:
+        return None
+    return {"checked": int(want.size), "mismatches": int((np.asarray(out) != want).sum()),
+            "against": "reference X-TED_CPU distances, tests/golden/configs.json.gz"}
+
+
+def singles(ctx):
+    """The single-pair workloads, one xted_distance call per pair (two timed
+    calls after one warm-up; best device time): ms per pair and GCUPS, with
+    each distance checked against the golden fixture."""
+    from xted import gen
+    gold = golden_configs()
+    want = {c["name"]: c["distance"] for c in gold["singles"]} if gold else {}
+    want["single100"] = None
+    out = {}
+    for name, (a, b) in (("single100", gen.single_pair_100()), ("single1000", gen.single_pair_1000()),
+                         ("single20000_random", gen.single_pair_20000(shape="random")),
+                         ("single20000_caterpillar", gen.single_pair_20000(shape="caterpillar"))):
+        d = ctx.distance(a, b)
+        best_dev, best_wall = 1e30, 1e30
+        for _ in range(2):
+            t0 = time.perf_counter()
+            d2 = ctx.distance(a, b)
+            best_wall = min(best_wall, (time.perf_counter() - t0) * 1e3)
+            st = ctx.stats()
+            best_dev = min(best_dev, st["device_ms"])
+            assert d2 == d
+        out[name] = {"m": a.n, "n": b.n, "device_ms": round(best_dev, 3), "wall_ms": round(best_wall, 3),
+                     "cells": st["cells"], "gcups": round(st["cells"] / (best_dev / 1e3) / 1e9, 2),
+                     "distance": d, "reference_distance": want.get(name),
+                     "match": None if want.get(name) is None else d == want[name]}
+    return out
 
 
 def serve_cpu_baseline(budget_s: float, seed: int = 6):
@@ -366,27 +492,55 @@ def serve_cpu_baseline(budget_s: float, seed: int = 6):
                                     f"({dt:.1f} s), scaled to 1,000 corpus trees"}
 
 
+def reference_workload(name: str):
+    """The workload of `name` for the reference arm, built without the CUDA
+    library (xted.synth reproduces the C generator's trees exactly): the
+    reference arm loads only the reference X-TED_CPU. For the mixed batch only
+    the sampled pairs are built. Returns (pairs, workload indices, config, stride)."""
+    from xted import synth
+    _, cfg = make_workload_config(name, 0)
+    if name.startswith("batched"):
+        npairs = cfg["npairs"]
+        stride = 32 if npairs > 256 else 1
+        which = list(range(0, npairs, stride))
+        return synth.mixed_pairs(npairs, cfg["seed"], which), which, cfg, stride
+    pairs = []
+    if name == "single100":
+        pairs = [(synth.tree("random", 100, synth.mix(1, 1), "uniform", 26),
+                  synth.tree("random", 100, synth.mix(1, 2), "uniform", 26))]
+    elif name == "single1000":
+        pairs = [(synth.tree("wide", 1000, synth.mix(2, 1), "zipf", 10000),
+                  synth.tree("deep", 1000, synth.mix(2, 2), "zipf", 10000))]
+    elif name == "single20000":
+        pairs = [tuple(synth.tree(sh, 20000, synth.mix(3, k), "uniform", 64) for k in (1, 2))
+                 for sh in ("random", "caterpillar")]
+    return pairs, list(range(len(pairs))), cfg, 1
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
-    pairs, cfg = make_workload(args.workload, 0)
-    stride = 32 if len(pairs) > 256 else 1
+    pairs, which, cfg, stride = reference_workload(args.workload)
     for _ in range(args.warmup):
-        cpu_reference(pairs[:1], 30.0, 1)
-    vals = []
+        cpu_reference(pairs[:1], 30.0, 1, index=which[:1])
+    vals, lvl = [], []
     info = None
     t_all = time.perf_counter()
     for _ in range(args.steps):
-        v, info = cpu_reference(pairs, args.ref_budget, stride)
+        v, info = cpu_reference(pairs, args.ref_budget, stride, index=which)
         vals.append(v)
+        lvl.append(info["pairs"] / (info["level_ms"] / 1e3) if info["level_ms"] > 0 else None)
     wall = time.perf_counter() - t_all
     value = statistics.mean(vals)
+    lv = [x for x in lvl if x]
     out = {"metric": METRIC, "value": round(value, 3), "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * wall / args.steps, 3),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-           "data": "synthetic", "config": cfg,
+           "data": "synthetic", "config": arm_config(cfg, world),
            "cpu_baseline": {"value": round(value, 3), "unit": "pairs/s", "cores": info["cores"],
-                            "kind": info["kind"], "sample": info["sample"]},
+                            "kind": info["kind"], "sample": info["sample"],
+                            # the same pairs timed by the reference's own level-loop timer
+                            "ref_timer_pairs_per_s": round(statistics.mean(lv), 3) if lv else None},
            "e2e": {"value": round(value, 3), "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -402,6 +556,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving sweep")
+    ap.add_argument("--no-singles", action="store_true", help="skip the single-pair workloads")
     ap.add_argument("--serve-budget", type=float, default=20.0, help="seconds for the serving sweep")
     ap.add_argument("--wait-timeout", type=float, default=20.0,
                     help="bound of the DP kernel's idle waits, seconds (raise it under a profiler's replay)")
@@ -436,6 +591,7 @@ def main():
     barrier(world)
     cells = st["cells"]
     value, gcups, dev_ms_max = aggregate(npairs, args.steps, dev_ms, cells, world)
+    parity = golden_parity(args.workload, rank, ref_out)
 
     # ---- end to end through the public batch call ----
     ctx.distance_batch(pairs)
@@ -474,7 +630,22 @@ def main():
         stride = 32 if npairs > 256 else 1
         v, info = cpu_reference(pairs, args.ref_budget, stride)
         cpu = {"value": round(v, 3), "unit": "pairs/s", "cores": info["cores"], "kind": info["kind"],
-               "sample": info["sample"]}
+               "sample": info["sample"],
+               "ref_timer_pairs_per_s": round(info["pairs"] / (info["level_ms"] / 1e3), 3)
+               if info["level_ms"] > 0 else None}
+        # the reference's distances of the sampled pairs against this run's
+        dd = info["distances"]
+        live = {"checked": len(dd), "mismatches": sum(int(ref_out[p]) != d for p, d in dd.items()),
+                "against": f"reference X-TED_CPU computed in this run ({info['kind']})"}
+        parity = dict(parity or {}, live_reference=live)
+
+    # ---- single pairs (configs 1-3), 1 GPU ----
+    single = None
+    if world == 1 and args.workload == "batched" and not args.no_singles:
+        try:
+            single = singles(ctx)
+        except Exception as ex:
+            single = {"error": f"{type(ex).__name__}: {ex}"[:300]}
 
 
     # ---- serving (1 GPU) ----
@@ -507,11 +678,13 @@ def main():
         "metric": METRIC, "value": round(value, 2), "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": dict(cfg, l2="distance tables exceed L2 (no flush)", parallelism=f"pairs sharded, dp{world}"),
+        "config": arm_config(cfg, world),
         "gcups": round(gcups, 2), "cells_per_step": cells, "cells_right_path": st["cells_right"],
         "e2e": {"value": round(e2e_value, 2), "unit": "pairs/s", "h2d_bytes_per_step": st_e2e["h2d_bytes"],
                 "d2h_bytes_per_step": st_e2e["d2h_bytes"], "host_plan_ms": round(st_e2e["host_plan_ms"], 2)},
+        "parity": parity,
         "plain_per_pair": plain,
+        "singles": single,
         "batched_vs_plain": round(value / plain["device_pairs_per_s"], 2) if plain else None,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_src,

@@ -6,6 +6,7 @@ after ``make -C oracle all ref``:
     python tests/golden/make_golden.py datasets    # -> datasets.json.gz
     python tests/golden/make_golden.py synthetic   # -> synthetic.json.gz
     python tests/golden/make_golden.py bracket     # -> bracket.json.gz
+    python tests/golden/make_golden.py configs     # -> configs.json.gz
 
 datasets: tree pair (0, 1) of every file of the reference's sampled datasets
   (Sampled_Dataset/*, Sampled_Dataset_Extra_Large_Trees/*), which is the pair the
@@ -19,7 +20,19 @@ synthetic: seeded trees from the product generator (all four shapes, sizes
   1..400, both label alphabets), expected distances from the reference
   ``standard_ted`` on decimal-string labels.
 
-Every tree is stored as {"labels": [...], "parent": [...]} in preorder.
+configs: the benchmark workloads themselves, regenerated from their seeds by
+  the product generator (xted.gen): the 1,000-node wide-shallow vs deep-narrow
+  pair, both 20,000-node pairs (random recursive and caterpillar), every pair
+  of the 4,096-pair mixed batch (seed 4), and the first 8 queries of the
+  serving pool (seed 6) against the whole 1,000-tree serving corpus (seed 5).
+  Expected distances from the reference ``standard_ted`` (all 8 threads for a
+  single pair; one thread per pair, one spawned worker per core, for the
+  batches). Trees are stored as a short SHA-256 of their CSR arrays, so a
+  change of the generator fails loudly instead of silently changing the
+  workload.
+
+Every tree of datasets/synthetic is stored as {"labels": [...], "parent": [...]}
+in preorder.
 """
 from __future__ import annotations
 
@@ -136,7 +149,64 @@ def bracket():
                              "from its standard_ted", "cases": cases}, f)
 
 
+def tree_hash(t):
+    """First 16 hex digits of the SHA-256 of a tree's labels | off | idx (int32)."""
+    import hashlib
+
+    import numpy as np
+    h = hashlib.sha256()
+    for arr in (t.labels, t.off, t.idx):
+        h.update(np.ascontiguousarray(arr, dtype=np.int32).tobytes())
+    return h.hexdigest()[:16]
+
+
+def _ref_pair(pair):
+    a, b = pair
+    return oracle.ref_distance(a, b, num_threads=1)
+
+
+def _ref_parallel(pairs):
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        return [d for d, _ in pool.map(_ref_pair, pairs, chunksize=1)]
+
+
+def configs():
+    import time
+
+    from xted import gen
+    out = {"source": "reference X-TED_CPU standard_ted on the benchmark workloads (xted.gen seeds)"}
+    singles = []
+    for name, pair in (("single1000", gen.single_pair_1000()),
+                       ("single20000_caterpillar", gen.single_pair_20000(shape="caterpillar")),
+                       ("single20000_random", gen.single_pair_20000(shape="random"))):
+        a, b = pair
+        t0 = time.perf_counter()
+        d, level_ms = oracle.ref_distance(a, b, num_threads=8)
+        wall = time.perf_counter() - t0
+        singles.append({"name": name, "a": tree_hash(a), "b": tree_hash(b), "m": a.n, "n": b.n, "distance": d,
+                        "ref_level_ms_8_threads": round(level_ms, 1), "ref_wall_s_8_threads": round(wall, 2)})
+        print(f"{name}: d={d} ({wall:.1f} s)", flush=True)
+    out["singles"] = singles
+    pairs = gen.mixed_batch(4096, seed=4)
+    t0 = time.perf_counter()
+    dist = _ref_parallel(pairs)
+    print(f"batch4096: {len(dist)} pairs ({time.perf_counter() - t0:.1f} s)", flush=True)
+    out["batch4096"] = {"seed": 4, "npairs": 4096, "hashes": [[tree_hash(a), tree_hash(b)] for a, b in pairs],
+                        "distances": dist}
+    corpus = gen.corpus(1000, seed=5)
+    queries = gen.corpus(64, seed=6)[:8]
+    t0 = time.perf_counter()
+    flat = _ref_parallel([(q, t) for q in queries for t in corpus])
+    print(f"serve: {len(flat)} pairs ({time.perf_counter() - t0:.1f} s)", flush=True)
+    out["serve"] = {"corpus_seed": 5, "ntrees": 1000, "query_seed": 6, "nqueries": len(queries),
+                    "corpus_hashes": [tree_hash(t) for t in corpus], "query_hashes": [tree_hash(q) for q in queries],
+                    "distances": [flat[k * len(corpus):(k + 1) * len(corpus)] for k in range(len(queries))]}
+    with gzip.open(os.path.join(HERE, "configs.json.gz"), "wt") as f:
+        json.dump(out, f)
+
+
 if __name__ == "__main__":
-    what = sys.argv[1:] or ["datasets", "synthetic", "bracket"]
+    what = sys.argv[1:] or ["datasets", "synthetic", "bracket", "configs"]
     for w in what:
-        {"datasets": datasets, "synthetic": synthetic, "bracket": bracket}[w]()
+        {"datasets": datasets, "synthetic": synthetic, "bracket": bracket, "configs": configs}[w]()

@@ -6,16 +6,13 @@ sizes and label distributions stand in for them.
 """
 from __future__ import annotations
 
-import math
 from typing import List, Tuple
 
 import numpy as np
 
 from . import _lib
+from .synth import LABELS, SHAPES, mix as _mix, mixed_specs
 from .trees import Tree
-
-SHAPES = {"random": 0, "wide": 1, "deep": 2, "caterpillar": 3}
-LABELS = {"uniform": 0, "zipf": 1}
 
 
 def tree(shape: str, n: int, seed: int, labels: str = "uniform", alphabet: int = 26) -> Tree:
@@ -26,14 +23,6 @@ def tree(shape: str, n: int, seed: int, labels: str = "uniform", alphabet: int =
                                         lab.ctypes.data_as(_lib._i32p), off.ctypes.data_as(_lib._i32p),
                                         idx.ctypes.data_as(_lib._i32p)), "xted_gen_tree")
     return Tree(lab[:n].copy(), off, idx[:max(n - 1, 0)].copy())
-
-
-def _mix(*xs: int) -> int:
-    h = 0x243F6A8885A308D3
-    for x in xs:
-        h = (h ^ (x & (2**64 - 1))) * 0x100000001B3 & (2**64 - 1)
-        h ^= h >> 29
-    return h
 
 
 def single_pair_100(seed: int = 1) -> Tuple[Tree, Tree]:
@@ -58,17 +47,8 @@ def mixed_batch(npairs: int = 4096, seed: int = 4, lo: int = 50, hi: int = 2000,
                 alphabet: int = 1000) -> List[Tuple[Tree, Tree]]:
     """Pairs with log-uniform sizes in [lo, hi], shapes uniform over the four
     kinds, labels Zipf(1.1) over `alphabet` ids, every tree drawn independently."""
-    rng = np.random.default_rng(_mix(seed, 99) % (2**63))
-    names = list(SHAPES)
-    out = []
-    for p in range(npairs):
-        ts = []
-        for s in range(2):
-            n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
-            shape = names[int(rng.integers(0, 4))]
-            ts.append(tree(shape, n, _mix(seed, p, s), "zipf", alphabet))
-        out.append((ts[0], ts[1]))
-    return out
+    return [tuple(tree(sh, n, sd, "zipf", alphabet) for sh, n, sd in spec)
+            for spec in mixed_specs(npairs, seed, lo, hi)]
 
 
 def corpus(ntrees: int = 1000, seed: int = 5, lo: int = 100, hi: int = 1000,
