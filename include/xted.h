@@ -1,5 +1,6 @@
 /*
- * xted.h -- C ABI of the B200-native unit-cost tree edit distance library.
+ * xted.h -- C ABI of the B200-native tree edit distance library (the
+ * reference's unit cost by default, general edit costs as an option).
  *
  * Drop-in for the reference X-TED entry point
  *   int standard_ted(vector<string>& x_node, vector<vector<int>>& x_adj,
@@ -84,7 +85,22 @@ typedef struct xted_opts {
                                2,048 and whose unit has at least this many
                                cells runs in 2,048-column stripes on up to 16
                                blocks at once (0 = 2^20; < 0: one block)    */
+    int32_t cost_del;       /* edit costs (integers >= 0): deleting a node of */
+    int32_t cost_ins;       /* the first tree, inserting a node of the second */
+    int32_t cost_ren;       /* tree, and mapping two nodes whose labels differ
+                               (equal labels map at 0). 1, 1, 1 (the default,
+                               and what 0, 0, 0 means) is the reference's unit
+                               cost (X-TED_CPU/parallel_computing.cpp:17-39),
+                               bit-exact with it. A pair of m and n nodes is
+                               accepted while cost_del*m + cost_ins*n <
+                               XTED_COST_BOUND (the row scan's key range),
+                               else the call returns XTED_EINVAL. The
+                               allocation-free entry point is unit-cost only. */
+    int32_t pad_;
 } xted_opts;
+
+/* Bound on cost_del * m + cost_ins * n for a pair of m and n nodes. */
+#define XTED_COST_BOUND (1 << 17)
 
 typedef struct xted_ctx xted_ctx;
 
@@ -133,7 +149,8 @@ int xted_last_stats(const xted_ctx *ctx, xted_stats *out);
 /* All pairs of ntrees trees: out[i*ntrees + j] = TED(trees[i], trees[j]),
  * symmetric with a zero diagonal. The reference harness allocates this
  * matrix but fills only pair (0, 1) (X-TED_CPU/TED_test.cpp:26-47); here the
- * ntrees(ntrees-1)/2 pairs run through the batch path in chunks whose
+ * ntrees(ntrees-1)/2 pairs (every ordered pair when cost_del != cost_ins,
+ * which makes TED asymmetric) run through the batch path in chunks whose
  * distance tables fit in pair_budget int32 elements (0: 2^30, or a quarter of
  * the context's mem_limit). Synchronous. */
 int xted_distance_matrix(xted_ctx *ctx, const xted_tree *trees, int32_t ntrees, int64_t pair_budget, int32_t *out);
@@ -186,8 +203,15 @@ int xted_parse_bracket(const char *s, int64_t len, int32_t cap_nodes, int32_t *c
  * it reads): calls that overlap on the GPU (two host threads at once) race,
  * so serialise them. The first call on a device does the set-up: it checks
  * the device and looks up the arena's device address with that device
- * current; make that first call before any stream capture. Same results and
- * empty-tree rules as xted_distance. */
+ * current; make that first call before any stream capture. CUDA loads
+ * modules lazily by default (since CUDA 12.2), so that first lookup is also
+ * what loads the library's module onto the device and commits the arena's
+ * XTED_NOALLOC_ARENA_BYTES of device memory: "allocates nothing" holds from
+ * the second call on. Make one warm-up call (any small pair) at start-up,
+ * before handing device memory to another allocator's pool. The call makes
+ * `device` current while it works and restores the calling thread's current
+ * device before it returns. Same results and empty-tree rules as
+ * xted_distance. */
 #define XTED_NOALLOC_ARENA_BYTES (16 << 20)
 int xted_distance_noalloc(const xted_tree *a, const xted_tree *b, int32_t device, int32_t *out);
 
@@ -246,6 +270,26 @@ int xted_serve_stats(xted_ctx *ctx, int64_t *out, int32_t n);
  * still beats the k-th (distance, index) found. The answer equals the
  * unpruned one. Applies to queries admitted later. */
 int xted_serve_options(xted_ctx *ctx, int32_t prune, int32_t first_round);
+
+/* ---- failure injection for tests ----
+ *
+ * No counterpart in the reference, whose error handling prints CUDA errors and
+ * carries on or exits the process (X-TED_GPU/utils/cuda_utils.h:35-41,
+ * X-TED_GPU/help.h:6-14) and whose spin barriers wait without bound
+ * (X-TED_GPU/parallel_X_TED.cu:68-91, 128-157). This hook lets a test check
+ * that a failure here is bounded, reported and survivable, without faulting
+ * or hanging anything: it arms one host-side fault for the next
+ * xted_distance_batch / xted_distance call or the next serving query posted
+ * to the device, then disarms itself.
+ *   XTED_FAULT_HOLD_PAIR: level 0 of one computed pair (the batch's pair 0,
+ *     or the query's first computed corpus tree) is never published into the
+ *     ready queue, so its tables never become ready. A batch then ends when
+ *     the persistent launch's bounded idle wait (wait_timeout_s) runs out and
+ *     returns XTED_ETIMEOUT; a serving launch goes idle and ends, and the
+ *     query fails with XTED_ETIMEOUT. The context stays usable. */
+#define XTED_FAULT_NONE 0
+#define XTED_FAULT_HOLD_PAIR 1
+int xted_test_fault(xted_ctx *ctx, int32_t kind);
 
 #ifdef __cplusplus
 }

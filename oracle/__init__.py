@@ -51,6 +51,9 @@ def _lib():
         lib = ctypes.CDLL(path)
         lib.xo_distance.restype = ctypes.c_int
         lib.xo_distance.argtypes = [ctypes.c_int, _i32p, _i32p, _i32p, ctypes.c_int, _i32p, _i32p, _i32p]
+        lib.xo_distance_cost.restype = ctypes.c_int
+        lib.xo_distance_cost.argtypes = [ctypes.c_int, _i32p, _i32p, _i32p, ctypes.c_int, _i32p, _i32p, _i32p,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.xo_tree_stats.restype = None
         lib.xo_tree_stats.argtypes = [ctypes.c_int, _i32p, _i32p, _i64p]
         lib.xo_distance_batch.restype = ctypes.c_int
@@ -94,12 +97,14 @@ def _arrs(t):
     return lab, off, idx
 
 
-def distance(a, b) -> int:
-    """Unit-cost TED by the C restatement of X-TED_CPU."""
+def distance(a, b, costs=None) -> int:
+    """TED by the C restatement of X-TED_CPU: unit cost (the reference's), or
+    with costs = (delete, insert, rename)."""
     la, ao, ai = _arrs(a)
     lb, bo, bi = _arrs(b)
-    d = _lib().xo_distance(len(a.labels), _p32(la), _p32(ao), _p32(ai),
-                           len(b.labels), _p32(lb), _p32(bo), _p32(bi))
+    cd, ci, cr = costs if costs is not None else (1, 1, 1)
+    d = _lib().xo_distance_cost(len(a.labels), _p32(la), _p32(ao), _p32(ai),
+                                len(b.labels), _p32(lb), _p32(bo), _p32(bi), int(cd), int(ci), int(cr))
     if d < 0:
         raise MemoryError("oracle allocation failed")
     return int(d)

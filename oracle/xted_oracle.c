@@ -82,26 +82,29 @@ static void xo_kr_depth(int K, const int32_t *kr, const int32_t *orl, int32_t *d
 
 /* X-TED_CPU/parallel_computing.cpp:4-45 compute: the forest table of the
  * keyroot pair (k,l), filled from high indices to low. D is (m+1)x(n+1),
- * Dt is m x n, both row-major. */
+ * Dt is m x n, both row-major. The reference's unit costs (its literal 1s
+ * at :17-25 and :31-39, and the label test) are the parameters cd (delete
+ * a node of the first tree), ci (insert a node of the second) and cr
+ * (label change); cd = ci = cr = 1 is the reference exactly. */
 static void xo_table(int i0, int j0, const int32_t *xorl, const int32_t *yorl,
                      const int32_t *la, const int32_t *lb, int n,
-                     int32_t *D, int32_t *Dt) {
+                     int32_t *D, int32_t *Dt, int cd, int ci, int cr) {
     const size_t ld = (size_t)n + 1;
     int imax = xorl[i0] + 1, jmax = yorl[j0] + 1;
     D[imax * ld + jmax] = 0;
-    for (int i = imax - 1; i > i0 - 1; i--) D[i * ld + jmax] = 1 + D[(i + 1) * ld + jmax];
-    for (int j = jmax - 1; j > j0 - 1; j--) D[imax * ld + j] = 1 + D[imax * ld + j + 1];
+    for (int i = imax - 1; i > i0 - 1; i--) D[i * ld + jmax] = cd + D[(i + 1) * ld + jmax];
+    for (int j = jmax - 1; j > j0 - 1; j--) D[imax * ld + j] = ci + D[imax * ld + j + 1];
     for (int i = imax - 1; i > i0 - 1; i--) {
         for (int j = jmax - 1; j > j0 - 1; j--) {
             if ((xorl[i] == xorl[i0]) & (yorl[j] == yorl[j0])) {
-                int cost = la[i] != lb[j];
-                int v = xo_min3(cost + D[(i + 1) * ld + j + 1], 1 + D[(i + 1) * ld + j],
-                                1 + D[i * ld + j + 1]);
+                int cost = la[i] != lb[j] ? cr : 0;
+                int v = xo_min3(cost + D[(i + 1) * ld + j + 1], cd + D[(i + 1) * ld + j],
+                                ci + D[i * ld + j + 1]);
                 D[i * ld + j] = v;
                 Dt[(size_t)i * n + j] = v;
             } else {
                 D[i * ld + j] = xo_min3(Dt[(size_t)i * n + j] + D[(xorl[i] + 1) * ld + yorl[j] + 1],
-                                        1 + D[(i + 1) * ld + j], 1 + D[i * ld + j + 1]);
+                                        cd + D[(i + 1) * ld + j], ci + D[i * ld + j + 1]);
             }
         }
     }
@@ -127,12 +130,15 @@ static void xo_prep_free(xo_prep *p) { free(p->orl); free(p->kr); free(p->dep); 
  * X-TED_CPU/TED.cpp:177-190 standard_ted (+ standard_ted_1 :145-174 and the
  * level loop of parallel_computing.cpp:121-182, run sequentially here: any
  * order that finishes every lower level first gives the same table values).
- * Returns the distance, or -1 on allocation failure.
+ * Returns the distance, or -1 on allocation failure. With edit costs cd
+ * (delete), ci (insert), cr (rename); the empty-tree rules become n * ci and
+ * m * cd.
  */
-int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx,
-                int n, const int32_t *lb, const int32_t *boff, const int32_t *bidx) {
-    if (m == 0) return n;
-    if (n == 0) return m;
+int xo_distance_cost(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx,
+                     int n, const int32_t *lb, const int32_t *boff, const int32_t *bidx,
+                     int cd, int ci, int cr) {
+    if (m == 0) return n * ci;
+    if (n == 0) return m * cd;
     xo_prep A, B;
     xo_prep_tree(m, aoff, aidx, &A);
     xo_prep_tree(n, boff, bidx, &B);
@@ -147,7 +153,7 @@ int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *ai
                 if (dl < 0 || dl > B.maxd) continue;
                 for (int l = 0; l < B.K; l++)
                     if (B.dep[l] == dl)
-                        xo_table(A.kr[k], B.kr[l], A.orl, B.orl, la, lb, n, D, Dt);
+                        xo_table(A.kr[k], B.kr[l], A.orl, B.orl, la, lb, n, D, Dt, cd, ci, cr);
             }
         result = Dt[0];
     }
@@ -156,6 +162,12 @@ int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *ai
     xo_prep_free(&A);
     xo_prep_free(&B);
     return result;
+}
+
+/* The reference's unit-cost distance (X-TED_CPU/TED.cpp:177-190). */
+int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx,
+                int n, const int32_t *lb, const int32_t *boff, const int32_t *bidx) {
+    return xo_distance_cost(m, la, aoff, aidx, n, lb, boff, bidx, 1, 1, 1);
 }
 
 /* Keyroot statistics used by tests: K, max keyroot depth and the sum of

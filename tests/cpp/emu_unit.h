@@ -31,6 +31,9 @@ struct Pools {
 };
 
 inline int g_cache = 8;  // shared-memory window of the far-row stack (the kernels use 8)
+// edit costs of the emulated launch: delete a row-tree node, insert a
+// column-tree node, change a label (the reference's unit costs by default)
+inline int g_cd = 1, g_ci = 1, g_cr = 1;
 
 // Unit u of pair pr; the pair's m x n tree-distance table is dtv[pr.dt_off ...].
 inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vector<int32_t> &dtv, int narrow_width,
@@ -63,7 +66,7 @@ inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vecto
         foff[c] = (cn[j].y & XTED_ROW_ORL_MASK) + 1 - j;
         dend[c] = je - j;
         far[c] = j > j0 && (cn[j].y & XTED_ROW_PREVLEAF);
-        key[c] = c + XTED_KEY_BIG * seg;
+        key[c] = c * g_ci + XTED_KEY_BIG * seg;
         if (dend[c] == 1) seg++;
         j++;
     }
@@ -76,7 +79,7 @@ inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vecto
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = H.krd[(size_t)kr];
         const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
-        for (int c = 0; c < W; c++) prev[c] = dend[c];
+        for (int c = 0; c < W; c++) prev[c] = dend[c] * g_ci;
         int sp = 0, lo = 0;
         for (auto &row : cache) std::fill(row.begin(), row.end(), -777);
         for (auto &row : stk) std::fill(row.begin(), row.end(), -777);
@@ -84,18 +87,18 @@ inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vecto
             const int2 ri = rn[i];
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
-            const int bord = imax - i, rowfar = imax - ro - 1;
+            const int bord = (imax - i) * g_cd, rowfar = (imax - ro - 1) * g_cd;
             int runmin = XTED_INF;
             for (int c = W - 1; c >= 0; c--) {
                 const bool se = dend[c] == 1;
-                const int diag = se ? bord - 1 : prev[(size_t)c + 1];
+                const int diag = se ? bord - g_cd : prev[(size_t)c + 1];
                 const bool tcol = foff[c] == dend[c];
                 int a;
                 if (trow && tcol) {
-                    a = diag + (ri.x != lab[c]);
+                    a = diag + (ri.x != lab[c] ? g_cr : 0);
                 } else {
                     int fv;
-                    if (trow) fv = dend[c] - foff[c];
+                    if (trow) fv = (dend[c] - foff[c]) * g_ci;
                     else if (tcol) fv = rowfar;
                     else {
                         if (sp < 1) FAIL("far-row stack underflow");
@@ -107,8 +110,8 @@ inline void run_unit(const Pools &H, const XPair &pr, const XUnit &u, std::vecto
                     if (dv < 0) FAIL("tree distance (%d,%d) read before it was written", i, node[c]);
                     a = dv + fv;
                 }
-                int Av = std::min(a, prev[c] + 1);
-                if (se) Av = std::min(Av, bord + 1);
+                int Av = std::min(a, prev[c] + g_cd);
+                if (se) Av = std::min(Av, bord + g_ci);
                 runmin = std::min(runmin, Av + key[c]);
                 loc[c] = runmin;
             }
@@ -188,26 +191,26 @@ inline void run_unit_striped(const Pools &H, const XPair &pr, const XUnit &u, st
             const int i0 = H.krd[(size_t)kr];
             const int imax = (rn[i0].y & XTED_ROW_ORL_MASK) + 1;
             const int tbase = tflat;
-            for (int c = 0; c < w; c++) prev[c] = dend[C0 + c];
-            int edge = right ? dend[C1] : 0;  // D[i+1][C1]: the bottom border first
+            for (int c = 0; c < w; c++) prev[c] = dend[C0 + c] * g_ci;
+            int edge = right ? dend[C1] * g_ci : 0;  // D[i+1][C1]: the bottom border first
             std::vector<std::vector<int>> stk;
             for (int i = imax - 1; i >= i0; i--, tflat++) {
                 const int2 ri = rn[i];
                 const int ro = ri.y & XTED_ROW_ORL_MASK;
                 const bool trow = ro == imax - 1;
-                const int bord = imax - i, rowfar = imax - ro - 1;
+                const int bord = (imax - i) * g_cd, rowfar = (imax - ro - 1) * g_cd;
                 int runmin = XTED_INF;
                 for (int lc = w - 1; lc >= 0; lc--) {
                     const int c = C0 + lc;
                     const bool se = dend[c] == 1;
-                    const int diag = se ? bord - 1 : (lc + 1 < w ? prev[lc + 1] : edge);
+                    const int diag = se ? bord - g_cd : (lc + 1 < w ? prev[lc + 1] : edge);
                     const bool tcol = foff[c] == dend[c];
                     int a;
                     if (trow && tcol) {
-                        a = diag + (ri.x != lab[c]);
+                        a = diag + (ri.x != lab[c] ? g_cr : 0);
                     } else {
                         int fv;
-                        if (trow) fv = dend[c] - foff[c];
+                        if (trow) fv = (dend[c] - foff[c]) * g_ci;
                         else if (tcol) fv = rowfar;
                         else {
                             const int f = c + foff[c];
@@ -224,9 +227,9 @@ inline void run_unit_striped(const Pools &H, const XPair &pr, const XUnit &u, st
                         if (dv < 0) FAIL("tree distance (%d,%d) read before it was written", i, node[c]);
                         a = dv + fv;
                     }
-                    int Av = std::min(a, prev[lc] + 1);
-                    if (se) Av = std::min(Av, bord + 1);
-                    runmin = std::min(runmin, Av + c);
+                    int Av = std::min(a, prev[lc] + g_cd);
+                    if (se) Av = std::min(Av, bord + g_ci);
+                    runmin = std::min(runmin, Av + c * g_ci);
                     loc[lc] = runmin;
                 }
                 int carry = XTED_INF;
@@ -236,14 +239,14 @@ inline void run_unit_striped(const Pools &H, const XPair &pr, const XUnit &u, st
                 }
                 for (int lc = 0; lc < w; lc++) {
                     const int c = C0 + lc;
-                    prev[lc] = std::min(loc[lc], carry) - c;
+                    prev[lc] = std::min(loc[lc], carry) - c * g_ci;
                     if (trow && foff[c] == dend[c]) {
                         int32_t &slot = dt[(size_t)i * n + node[c]];
                         if (slot >= 0) FAIL("tree distance (%d,%d) written twice", i, node[c]);
                         slot = prev[lc];
                     }
                 }
-                CR[(size_t)st][(size_t)tflat] = prev[0] + C0;
+                CR[(size_t)st][(size_t)tflat] = prev[0] + C0 * g_ci;
                 FC[(size_t)st][(size_t)tflat] = prev[0];
                 if (right) edge = FC[(size_t)st + 1][(size_t)tflat];
                 if (i != i0 && (ri.y & XTED_ROW_ISKR)) stk.pop_back();

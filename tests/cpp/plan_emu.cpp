@@ -20,8 +20,8 @@
 #include "../../x-ted_b200/csrc/plan_core.h"
 #include "emu_unit.h"
 
-extern "C" int xo_distance(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx, int n,
-                           const int32_t *lb, const int32_t *boff, const int32_t *bidx);
+extern "C" int xo_distance_cost(int m, const int32_t *la, const int32_t *aoff, const int32_t *aidx, int n,
+                                const int32_t *lb, const int32_t *boff, const int32_t *bidx, int cd, int ci, int cr);
 using namespace xted;
 
 struct HostPlan {
@@ -219,6 +219,15 @@ int main(int argc, char **argv) {
         const int hws[3] = {XTED_HALF_MAX, -1, 100};
         const int hw = hws[(it / 16) % 3];
         g_table = it % 5 == 4;
+        // edit costs: the reference's unit costs on two iterations of three,
+        // else random delete / insert / rename costs (0 to 4)
+        if (it % 3 == 2) {
+            emu::g_cd = (int)(g() % 5);
+            emu::g_ci = (int)(g() % 5);
+            emu::g_cr = (int)(g() % 5);
+        } else {
+            emu::g_cd = emu::g_ci = emu::g_cr = 1;
+        }
         HostPlan H;
         plan(L, O, I, nn, pt, orient, nw, rr, wr, hw, H);
         int64_t dts = 0;
@@ -295,13 +304,16 @@ int main(int argc, char **argv) {
             if (v != 1) FAIL("unit covered %d times", v);
         for (int p = 0; p < npairs; p++) {
             const DPair &q = H.pairs[(size_t)p];
-            const int got = q.trivial >= 0 ? q.trivial : dt[(size_t)q.dt_off];
             const int a = pt[2 * (size_t)p], b = pt[2 * (size_t)p + 1];
+            // an empty-tree pair: the gather kernel's rule (insert or delete the other tree)
+            const int got = q.trivial >= 0 ? (nn[(size_t)a] == 0 ? nn[(size_t)b] * emu::g_ci : nn[(size_t)a] * emu::g_cd)
+                                           : dt[(size_t)q.dt_off];
             const int32_t z = 0;
-            const int want = xo_distance(nn[(size_t)a], nn[(size_t)a] ? L[(size_t)a].data() : &z, O[(size_t)a].data(),
-                                         I[(size_t)a].empty() ? &z : I[(size_t)a].data(), nn[(size_t)b],
-                                         nn[(size_t)b] ? L[(size_t)b].data() : &z, O[(size_t)b].data(),
-                                         I[(size_t)b].empty() ? &z : I[(size_t)b].data());
+            const int want = xo_distance_cost(nn[(size_t)a], nn[(size_t)a] ? L[(size_t)a].data() : &z,
+                                              O[(size_t)a].data(), I[(size_t)a].empty() ? &z : I[(size_t)a].data(),
+                                              nn[(size_t)b], nn[(size_t)b] ? L[(size_t)b].data() : &z,
+                                              O[(size_t)b].data(), I[(size_t)b].empty() ? &z : I[(size_t)b].data(),
+                                              emu::g_cd, emu::g_ci, emu::g_cr);
             if (got != want)
                 FAIL("distance mismatch it=%d pair=%d m=%d n=%d got=%d want=%d", it, p, nn[(size_t)a],
                      nn[(size_t)b], got, want);

@@ -232,3 +232,30 @@ def test_bench_cpu_baselines_small_sample():
     assert i1["pairs"] == 12 and i2["pairs"] == 12
     assert "in sequence" in i1["sample"] and "pair-parallel" in i2["sample"]
     assert i2["cores"] == (os.cpu_count() or 1)
+
+
+def test_bench_reference_arm_builds_its_workload_without_the_cuda_library():
+    """The benchmark's reference arm times the reference X-TED_CPU alone: its
+    workload (the sampled pairs of the 4,096-pair batch) comes from the
+    pure-Python generator and the process never maps lib/libxted.so."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.argv = ['bench.py']\n"
+            "import bench\n"
+            "pairs, which, cfg, stride = bench.reference_workload('batched')\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(len(pairs), which[1], stride, 'libxted.so' in maps)\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=REPO, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.split() == ["128", "32", "32", "False"]
+
+
+def test_cpp_wrapper_compiles_and_converts():
+    """include/xted.hpp (the reference-signature C++ wrapper) compiled by
+    tests/cpp/Makefile; its string interning and adjacency-to-CSR conversion
+    checked on the host (tests/cpp/hpp_check.cpp)."""
+    import subprocess
+    subprocess.run(["make", "-C", os.path.join(REPO, "tests", "cpp")], check=True, capture_output=True)
+    r = subprocess.run([os.path.join(REPO, "tests", "cpp", "_build", "hpp_check")], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr

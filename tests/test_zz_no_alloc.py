@@ -62,6 +62,25 @@ def test_noalloc_matches_batched_entry_twice_in_a_row():
 
 
 @pytest.mark.gpu
+def test_noalloc_later_calls_take_no_device_memory_and_keep_the_device():
+    """After the first (warm-up) call, which loads the module and commits the
+    arena, further calls leave the device's free memory unchanged; every call
+    restores the caller's current device."""
+    import torch
+    torch.cuda.init()
+    a, b = _pairs()[1]
+    assert _noalloc(a, b)[0] == 0  # warm-up: module load and arena commit happen here (or earlier)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for a, b in _pairs():
+        assert _noalloc(a, b)[0] == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+    assert torch.cuda.current_device() == 0
+
+
+@pytest.mark.gpu
 def test_noalloc_edge_cases():
     t = gen.tree("random", 30, 9)
     empty = trees.Tree(np.zeros(0, np.int32), np.zeros(1, np.int32), np.zeros(0, np.int32))

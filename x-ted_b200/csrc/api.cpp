@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -28,7 +29,7 @@ int dp_occupancy(int *blocks_per_sm);
 cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s);
 cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s);
 cudaError_t launch_gather(const XPair *pairs, const int32_t *trivial, const int32_t *dt, int npairs,
-                          int32_t *out, cudaStream_t s);
+                          int32_t *out, int c_del, int c_ins, cudaStream_t s);
 }  // namespace xted
 
 using namespace xted;
@@ -45,6 +46,10 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 }  // namespace
 
 namespace xted {
+
+bool costs_fit(const xted_opts &o, int64_t m, int64_t n) {
+    return (int64_t)o.cost_del * m + (int64_t)o.cost_ins * n < XTED_COST_BOUND;
+}
 
 int ctx_dev_reserve(xted_ctx *c, DevBuf &b, size_t bytes) {
     if (b.cap >= bytes) return XTED_OK;
@@ -92,9 +97,14 @@ int ctx_host_reserve(HostBuf &b, size_t bytes) {
 int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs) {
     c->prepared = false;
     ctx_drop_graph(c);  // the graph holds the previous plan's buffers and sizes
+    for (int32_t p = 0; p < npairs; p++)
+        if (!costs_fit(c->opts, a[p].n, b[p].n)) return XTED_EINVAL;
     XKernelParams &K = c->kp;
     int rc = dev_plan(c, a, b, npairs, K);
     if (rc) return rc;
+    K.c_del = c->opts.cost_del;
+    K.c_ins = c->opts.cost_ins;
+    K.c_ren = c->opts.cost_ren;
     rc = ctx_dev_reserve(c, c->dt, (size_t)std::max<int64_t>(c->plan_dt_elems, 1) * sizeof(int32_t));
     if (rc) return rc;
     const int64_t stack_rows = c->plan_stack_rows, max_wide = c->plan_max_wide;
@@ -172,7 +182,7 @@ static int enqueue_step(xted_ctx *c, bool events) {
     if (events && cudaEventRecord(c->evk0, c->stream) != cudaSuccess) return XTED_ECUDA;
     if (K.ntasks > 0 && launch_dp(K, c->grid, c->stream) != cudaSuccess) return XTED_ECUDA;
     if (events && cudaEventRecord(c->evk1, c->stream) != cudaSuccess) return XTED_ECUDA;
-    if (launch_gather(K.pairs, c->d_trivial, K.dt, npairs, d_out, c->stream) != cudaSuccess)
+    if (launch_gather(K.pairs, c->d_trivial, K.dt, npairs, d_out, K.c_del, K.c_ins, c->stream) != cudaSuccess)
         return XTED_ECUDA;
     if ((events && cudaEventRecord(c->ev1, c->stream) != cudaSuccess) ||
         cudaMemcpyAsync(hres, cnt, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
@@ -311,6 +321,7 @@ void xted_opts_default(xted_opts *o) {
     o->wait_timeout_s = 20.0;
     o->mem_limit = 0;
     o->stripe_min_cells = 0;
+    o->cost_del = o->cost_ins = o->cost_ren = 1;
 }
 
 const char *xted_strerror(int code) {
@@ -335,8 +346,11 @@ int xted_create(xted_ctx **out, const xted_opts *opts) {
     if (opts) o = *opts;
     else xted_opts_default(&o);
     if (o.narrow_width < 0 || o.narrow_width > XTED_NARROW_MAX || o.run_rows < 1 ||
-        o.orientation < 0 || o.orientation > 2 || o.wait_timeout_s <= 0 || o.ctas_per_sm < 0)
+        o.orientation < 0 || o.orientation > 2 || o.wait_timeout_s <= 0 || o.ctas_per_sm < 0 ||
+        o.cost_del < 0 || o.cost_ins < 0 || o.cost_ren < 0 || o.cost_del >= XTED_COST_BOUND ||
+        o.cost_ins >= XTED_COST_BOUND || o.cost_ren >= XTED_COST_BOUND)
         return XTED_EINVAL;
+    if (o.cost_del == 0 && o.cost_ins == 0 && o.cost_ren == 0) o.cost_del = o.cost_ins = o.cost_ren = 1;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || o.device < 0 || o.device >= ndev) {
         cudaGetLastError();
@@ -392,7 +406,13 @@ int xted_distance_batch(xted_ctx *c, const xted_tree *a, const xted_tree *b, int
     const double t1 = now_ms();
     std::memset(&c->stats, 0, sizeof(c->stats));
     if (rc) return rc;
+    const bool hold = c->fault == XTED_FAULT_HOLD_PAIR && npairs > 0;
+    if (hold) {  // test hook: pair 0's level 0 is never published
+        c->fault = 0;
+        c->kp.hold_pair = 0;
+    }
     rc = ctx_run(c, out, false);
+    c->kp.hold_pair = -1;
     fill_stats(c, t1 - t0);
     c->stats.total_ms = now_ms() - t0;
     return rc;
@@ -427,6 +447,9 @@ int xted_distance_matrix(xted_ctx *c, const xted_tree *trees, int32_t ntrees, in
     int64_t budget = pair_budget > 0 ? pair_budget
                                      : (c->opts.mem_limit > 0 ? c->opts.mem_limit / 16 : (int64_t)1 << 30);
     const int64_t max_pairs = (int64_t)1 << 20;
+    // TED is symmetric when deleting and inserting cost the same: each
+    // unordered pair once, mirrored; else both orders
+    const bool sym = c->opts.cost_del == c->opts.cost_ins;
     std::vector<xted_tree> A, B;
     std::vector<int64_t> at;  // i * ntrees + j of each pair in the chunk
     std::vector<int32_t> res;
@@ -438,7 +461,7 @@ int xted_distance_matrix(xted_ctx *c, const xted_tree *trees, int32_t ntrees, in
         for (size_t k = 0; k < A.size(); k++) {
             const int64_t i = at[k] / ntrees, j = at[k] % ntrees;
             out[i * ntrees + j] = res[k];
-            out[j * ntrees + i] = res[k];
+            if (sym) out[j * ntrees + i] = res[k];
         }
         A.clear();
         B.clear();
@@ -448,7 +471,8 @@ int xted_distance_matrix(xted_ctx *c, const xted_tree *trees, int32_t ntrees, in
     int64_t cells = 0;
     for (int32_t i = 0; i < ntrees; i++) {
         out[(int64_t)i * ntrees + i] = 0;
-        for (int32_t j = i + 1; j < ntrees; j++) {
+        for (int32_t j = sym ? i + 1 : 0; j < ntrees; j++) {
+            if (j == i) continue;
             const int64_t c2 = (int64_t)std::max(trees[i].n, 1) * std::max(trees[j].n, 1);
             if (!A.empty() && (cells + c2 > budget || (int64_t)A.size() >= max_pairs)) {
                 const int rc = flush();
@@ -462,6 +486,17 @@ int xted_distance_matrix(xted_ctx *c, const xted_tree *trees, int32_t ntrees, in
         }
     }
     return flush();
+}
+
+int xted_test_fault(xted_ctx *c, int32_t kind) {
+    if (!c || kind < 0 || kind > XTED_FAULT_HOLD_PAIR) return XTED_EINVAL;
+    if (c->serve) {
+        std::lock_guard<std::mutex> g(serve_mutex(c));
+        c->fault = kind;
+    } else {
+        c->fault = kind;
+    }
+    return XTED_OK;
 }
 
 int xted_last_stats(const xted_ctx *c, xted_stats *out) {

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -41,6 +42,7 @@ struct xted_ctx {
     int64_t held = 0;  // device bytes held by this context
     xted_stats stats{};
     int32_t err_info[4] = {0, 0, 0, 0};
+    int32_t fault = 0;  // armed test fault (xted_test_fault), taken by the next batch or posted query
     xted::ServeState *serve = nullptr;  // owned; released by serve_shutdown
     // device planning: host-side bookkeeping of the current batch
     std::unordered_map<xted::TreeKey, int, xted::TreeKeyHash> tree_ids;
@@ -64,6 +66,8 @@ struct xted_ctx {
 namespace xted {
 
 int ctx_dev_reserve(xted_ctx *c, DevBuf &b, size_t bytes);
+// A pair of m and n nodes fits the row scan's key range under the context's costs.
+bool costs_fit(const xted_opts &o, int64_t m, int64_t n);
 int ctx_host_reserve(HostBuf &b, size_t bytes);
 int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs);
 int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs, XKernelParams &K);
@@ -71,5 +75,6 @@ int ctx_run(xted_ctx *c, int32_t *out, bool allow_graph);
 void ctx_drop_graph(xted_ctx *c);
 void fill_stats(xted_ctx *c, double plan_ms);
 void serve_shutdown(xted_ctx *c);
+std::mutex &serve_mutex(xted_ctx *c);  // the serving state's lock (c->serve must be set)
 
 }  // namespace xted

@@ -5,17 +5,22 @@
 // narrow units, one per warp. A unit computes the forest tables of a run of
 // A-keyroots against a chunk of B-segments, row by row from the bottom:
 //
-//   reference recurrence (X-TED_CPU/parallel_computing.cpp:17-43):
-//     tree cell   D[i][j] = min(D[i+1][j+1] + cost(i,j), D[i+1][j] + 1, D[i][j+1] + 1),
-//                 Dtree[i][j] = D[i][j]
-//     forest cell D[i][j] = min(Dtree[i][j] + D[orl(i)+1][orl(j)+1], D[i+1][j] + 1,
-//                               D[i][j+1] + 1)
+//   reference recurrence (X-TED_CPU/parallel_computing.cpp:17-43), with the
+//   unit costs there generalised to del (a row-tree node), ins (a column-tree
+//   node) and ren (a label change); the reference's costs are 1, 1, 1:
+//     tree cell   D[i][j] = min(D[i+1][j+1] + ren*(l(i) != l(j)), D[i+1][j] + del,
+//                               D[i][j+1] + ins),  Dtree[i][j] = D[i][j]
+//     forest cell D[i][j] = min(Dtree[i][j] + D[orl(i)+1][orl(j)+1], D[i+1][j] + del,
+//                               D[i][j+1] + ins)
+//   with borders D[i][je] = (imax - i) del and D[imax][j] = (je - j) ins.
 //
-// Row formulation: with A[j] = min(first term, D[i+1][j] + 1), row i is the
-// min-plus suffix scan D[i][j] = min_{k >= j} (A[k] + (k - j)) closed by the
-// border D[i][je] = imax - i. Every column carries a key c + BIG*seg, so one
+// Row formulation: with A[j] = min(first term, D[i+1][j] + del), row i is the
+// min-plus suffix scan D[i][j] = min_{k >= j} (A[k] + (k - j) ins) closed by
+// the border D[i][je]. Every column carries a key ins*c + BIG*seg, so one
 // unsegmented suffix-min of A + key over a whole chunk yields every segment
-// (table) at once: values from a later segment are at least BIG too large.
+// (table) at once: values from a later segment are at least BIG too large
+// (the host admits a pair only while del*m + ins*n, a bound of every table
+// value, stays below BIG).
 // The row above (D[i+1][*]) lives in registers; rows that later rows will use
 // as D[orl(i)+1][*] are pushed on a per-warp stack in global scratch (its
 // depth is the number of keyroots on a root path). Dtree is read with
@@ -48,6 +53,17 @@ __device__ __forceinline__ void set_error(const XKernelParams &P, int code, int 
         P.error_info[1] = b;
         P.error_info[2] = c;
     }
+}
+
+// Edit costs of a launch (XKernelParams c_del, c_ins, c_ren). The DP kernel
+// is compiled twice more for them: UC (unit cost, the reference's) makes them
+// compile-time ones, so the default path carries no cost registers.
+struct Costs {
+    int del, ins, ren;
+};
+template <bool UC>
+__device__ __forceinline__ Costs costs_of(const XKernelParams &P) {
+    return UC ? Costs{1, 1, 1} : Costs{P.c_del, P.c_ins, P.c_ren};
 }
 
 // Inclusive suffix minimum over the warp (lane l: min over lanes >= l). A lane
@@ -160,12 +176,12 @@ __device__ __forceinline__ int count_ends(const Cols<W> &C) {
 }
 
 template <int W>
-__device__ __forceinline__ void set_keys(Cols<W> &C, int c0, int before) {
+__device__ __forceinline__ void set_keys(Cols<W> &C, int c0, int before, int ins) {
     int seg = before;
 #pragma unroll
     for (int k = 0; k < W; k++) {
         const bool v = (C.valid >> k) & 1u;
-        C.key[k] = v ? (c0 + k) + XTED_KEY_BIG * seg : KEY_INVALID;
+        C.key[k] = v ? (c0 + k) * ins + XTED_KEY_BIG * seg : KEY_INVALID;
         if (v && C.segor[k] == 0) seg++;
     }
 }
@@ -176,7 +192,7 @@ __device__ __forceinline__ void set_keys(Cols<W> &C, int c0, int before) {
 // Returns the thread's suffix minimum; loc[k] = minimum over its columns >= k.
 template <int W>
 __device__ __forceinline__ int row_forest(const Cols<W> &C, const int (&prev)[W], const int32_t *slot,
-                                          const int32_t *top, int bord1, int rowfar, int (&loc)[W]) {
+                                          const int32_t *top, int bord1, int rowfar, int del, int (&loc)[W]) {
     int cur[W], farv[W];
 #pragma unroll
     for (int k = 0; k < W; k++) {
@@ -187,8 +203,8 @@ __device__ __forceinline__ int row_forest(const Cols<W> &C, const int (&prev)[W]
 #pragma unroll
     for (int k = W - 1; k >= 0; k--) {
         const int far = ((C.tcol >> k) & 1u) ? rowfar : farv[k];
-        int A = __viaddmin_s32(prev[k], 1, cur[k] + far);  // min(up + 1, forest term)
-        A = min(A, bord1 | C.segor[k]);                     // a segment's last column meets the border
+        int A = __viaddmin_s32(prev[k], del, cur[k] + far);  // min(up + del, forest term)
+        A = min(A, bord1 | C.segor[k]);                       // a segment's last column meets the border
         run = __viaddmin_s32(A, C.key[k], run);             // min(A + key, run)
         loc[k] = run;
     }
@@ -197,20 +213,20 @@ __device__ __forceinline__ int row_forest(const Cols<W> &C, const int (&prev)[W]
 
 // Row step, tree-path rows (row i on its table's right path): tree cells on
 // the segments' right paths, forest cells elsewhere with the far value of the
-// table's bottom border.
+// table's bottom border. bord = D[i][je] = (imax - i) del.
 template <int W>
 __device__ __forceinline__ int row_tree(const Cols<W> &C, const int (&prev)[W], const int32_t *slot, int dnext,
-                                        int rl, int bord, int (&loc)[W]) {
+                                        int rl, int bord, Costs K, int (&loc)[W]) {
     int cur[W];
 #pragma unroll
     for (int k = 0; k < W; k++) cur[k] = slot[k];
-    const int bord1 = bord + 1;
+    const int bord1 = bord + K.ins;
     int run = XTED_INF;
 #pragma unroll
     for (int k = W - 1; k >= 0; k--) {
-        const int diag = C.segor[k] == 0 ? bord - 1 : ((k == W - 1) ? dnext : prev[k + 1]);
-        const int a = ((C.tcol >> k) & 1u) ? diag + (rl != C.lab[k] ? 1 : 0) : cur[k] + C.fb[k];
-        int A = __viaddmin_s32(prev[k], 1, a);
+        const int diag = C.segor[k] == 0 ? bord - K.del : ((k == W - 1) ? dnext : prev[k + 1]);
+        const int a = ((C.tcol >> k) & 1u) ? diag + (rl != C.lab[k] ? K.ren : 0) : cur[k] + C.fb[k] * K.ins;
+        int A = __viaddmin_s32(prev[k], K.del, a);
         A = min(A, bord1 | C.segor[k]);
         run = __viaddmin_s32(A, C.key[k], run);
         loc[k] = run;
@@ -277,13 +293,14 @@ __device__ __forceinline__ void issue_row(const int32_t *cnode, int width, const
 // ---------------------------------------------------------------------------
 // Narrow unit: one warp, chunk width <= 32*W.
 // ---------------------------------------------------------------------------
-template <int W>
+template <int W, bool UC>
 __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
                            int32_t *ring, int32_t *cache, int32_t *cnode) {
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = lane * W;
     const int width = ch.width;
+    const Costs K = costs_of<UC>(P);
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, XTED_NARROW_MAX - 1);
     __syncwarp();  // the previous unit's copies have drained (cp_async_wait<0> at its end)
@@ -294,7 +311,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
-        set_keys<W>(C, c0, incl - e);
+        set_keys<W>(C, c0, incl - e, K.ins);
     }
     const int n = pr.n;
     const int32_t *dt_in = P.dt + pr.dt_off;
@@ -313,7 +330,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
         int prev[W];
 #pragma unroll
-        for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        for (int k = 0; k < W; k++) prev[k] = C.dend[k] * K.ins;
         int sp = 0, lo = 0;  // stack depth; lowest position held in the shared window
         __syncwarp();  // the ring's previous readers are done
 #pragma unroll
@@ -338,15 +355,15 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
             const int2 ri = *(const int2 *)(slot + NARROW_ROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
-            const int bord = imax - i;
+            const int bord = (imax - i) * K.del;
             int loc[W];
             int mine;
             if (!trow) {
                 const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
-                mine = row_forest<W>(C, prev, slot + pbase, top, bord + 1, imax - ro - 1, loc);
+                mine = row_forest<W>(C, prev, slot + pbase, top, bord + K.ins, (imax - ro - 1) * K.del, K.del, loc);
             } else {
                 const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
-                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, loc);
+                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, K, loc);
             }
             const int incl = warp_suffix_min(mine, lane);
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
@@ -419,7 +436,7 @@ __device__ __forceinline__ void group_sync(int gid) {
     }
 }
 
-template <int W, int G>
+template <int W, int G, bool UC>
 __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                           int32_t *ring, int32_t *cache, int32_t *cnode, int gtid, int gid) {
     constexpr int GROW = 256 * G + 8 * G;  // padded row of 256*G columns
@@ -434,6 +451,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
     constexpr int PF = XTED_PREFETCH;
     const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
     const int stack_rows = P.stack_rows;
+    const Costs K = costs_of<UC>(P);
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, 256 * G - 1);
     group_sync<G>(gid);  // the group's previous unit is done with cnode and S
@@ -447,7 +465,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
         group_sync<G>(gid);
         int before = incl - e;
         for (int w = 0; w < warp; w++) before += S.ends[w];
-        set_keys<W>(C, c0, before);
+        set_keys<W>(C, c0, before, K.ins);
     }
     const int n = pr.n;
     const int32_t *dt_in = P.dt + pr.dt_off;
@@ -459,7 +477,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
         int prev[W];
 #pragma unroll
-        for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        for (int k = 0; k < W; k++) prev[k] = C.dend[k] * K.ins;
         int sp = 0, lo = 0;  // stack depth; lowest position held in the shared window
         group_sync<G>(gid);  // the ring's and S.first's previous readers are done
         if (lane == 0) S.first[warp] = prev[0];
@@ -486,16 +504,16 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
             const int2 ri = *(const int2 *)(slot + GROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
-            const int bord = imax - i;
+            const int bord = (imax - i) * K.del;
             int loc[W];
             int mine;
             if (!trow) {
                 const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
-                mine = row_forest<W>(C, prev, slot + pbase, top, bord + 1, imax - ro - 1, loc);
+                mine = row_forest<W>(C, prev, slot + pbase, top, bord + K.ins, (imax - ro - 1) * K.del, K.del, loc);
             } else {
                 int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
                 if (lane == 31) dnext = S.first[warp + 1];
-                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, loc);
+                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, K, loc);
             }
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
@@ -593,6 +611,7 @@ __device__ __forceinline__ bool wait_progress(const XKernelParams &P, volatile i
     return false;
 }
 
+template <bool UC>
 __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                            int32_t *ring, int32_t *cache, int32_t *cnode, int s, int K, int X, int R,
                            const int32_t *expmap, int32_t *prog, int32_t *CR, int32_t *FC, int32_t *E) {
@@ -610,6 +629,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const int pbase = pad(lc0);
     const bool deep = run.depth > XTED_STACK_CACHE;
     const int stack_rows = P.stack_rows;
+    const Costs KC = costs_of<UC>(P);
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, w - 1);
     unsigned expm = 0;  // this thread's columns that stripes to the left read as far columns
@@ -638,7 +658,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
 #pragma unroll
     for (int k = 0; k < W; k++)
         if ((C.valid >> k) & 1u) cnode[lc0 + k] = C.node[k];
-    set_keys<W>(C, c0, 0);  // one segment: key = segment column
+    set_keys<W>(C, c0, 0, KC.ins);  // one segment: key = ins * segment column
     const int n = pr.n;
     const int32_t *dt_in = P.dt + pr.dt_off;
     int32_t *dt_out = P.dt + pr.dt_off;
@@ -655,11 +675,11 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
         const int tbase = tflat;
         int prev[W];
 #pragma unroll
-        for (int k = 0; k < W; k++) prev[k] = C.dend[k];
+        for (int k = 0; k < W; k++) prev[k] = C.dend[k] * KC.ins;
         int sp = 0, lo = 0;
         __syncthreads();  // the ring's and S's previous readers are done
         if (lane == 0) S.first[warp] = prev[0];
-        if (gtid == 0) S.first[G] = right ? w - C1 : 0;  // D[imax][C1]: the bottom border
+        if (gtid == 0) S.first[G] = right ? (w - C1) * KC.ins : 0;  // D[imax][C1]: the bottom border
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
@@ -687,7 +707,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             const int2 ri = *(const int2 *)(slot + GROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
-            const int bord = imax - i;
+            const int bord = (imax - i) * KC.del;
             int loc[W];
             int mine;
             if (!trow) {
@@ -695,7 +715,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                 const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
                 const int32_t *erow = E + (int64_t)(tbase + (imax - 1 - (ro + 1))) * X;
                 const int32_t *cur = slot + pbase;
-                const int rowfar = imax - ro - 1, bord1 = bord + 1;
+                const int rowfar = (imax - ro - 1) * KC.del, bord1 = bord + KC.ins;
                 int run_min = XTED_INF;
 #pragma unroll
                 for (int k = W - 1; k >= 0; k--) {
@@ -703,7 +723,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                     if ((C.tcol >> k) & 1u) far = rowfar;
                     else if (C.fidx[k] >= 0) far = top[C.fidx[k]];
                     else far = __ldcg(erow + (-1 - C.fidx[k]));
-                    int A = __viaddmin_s32(prev[k], 1, cur[k] + far);
+                    int A = __viaddmin_s32(prev[k], KC.del, cur[k] + far);
                     A = min(A, bord1 | C.segor[k]);
                     run_min = __viaddmin_s32(A, C.key[k], run_min);
                     loc[k] = run_min;
@@ -712,7 +732,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             } else {
                 int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
                 if (lane == 31) dnext = S.first[warp + 1];
-                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, loc);
+                mine = row_tree<W>(C, prev, slot + pbase, dnext, ri.x, bord, KC, loc);
             }
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
@@ -795,13 +815,14 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     cp_async_wait<0>();
 }
 
+template <bool UC>
 __device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
                                 int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 32) run_narrow<1>(P, pr, u, lane, stk, ring, cache, cnode);
-    else if (width <= 64) run_narrow<2>(P, pr, u, lane, stk, ring, cache, cnode);
-    else if (width <= 128) run_narrow<4>(P, pr, u, lane, stk, ring, cache, cnode);
-    else run_narrow<8>(P, pr, u, lane, stk, ring, cache, cnode);
+    if (width <= 32) run_narrow<1, UC>(P, pr, u, lane, stk, ring, cache, cnode);
+    else if (width <= 64) run_narrow<2, UC>(P, pr, u, lane, stk, ring, cache, cnode);
+    else if (width <= 128) run_narrow<4, UC>(P, pr, u, lane, stk, ring, cache, cnode);
+    else run_narrow<8, UC>(P, pr, u, lane, stk, ring, cache, cnode);
 }
 
 // ---------------------------------------------------------------------------
@@ -819,11 +840,13 @@ __device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const X
 // is computed when two rows fit, else row by row; wider segments read them
 // straight from global memory.
 // ---------------------------------------------------------------------------
+template <bool UC>
 __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *scr,
                              WideShared &S, int32_t *smem) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
+    const Costs K = costs_of<UC>(P);
     const int width = ch.width;
     const int per = (width + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS;
     const int64_t Wp = (int64_t)per * XTED_CTA_THREADS;
@@ -871,7 +894,8 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
-        for (int k = 0; k < nk; k++) prevb[(int64_t)k * XTED_CTA_THREADS + tid] = cols[(int64_t)k * XTED_CTA_THREADS + tid].w;
+        for (int k = 0; k < nk; k++)
+            prevb[(int64_t)k * XTED_CTA_THREADS + tid] = cols[(int64_t)k * XTED_CTA_THREADS + tid].w * K.ins;
         if (tid == 0) prevb[Wp] = 0;
         int sp = 0;
         __syncthreads();
@@ -897,8 +921,8 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
             const int2 ri = __ldg(&rows[i]);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
-            const int bord = imax - i;
-            const int rowfar = imax - ro - 1;
+            const int bord = (imax - i) * K.del;
+            const int rowfar = (imax - ro - 1) * K.del;
             const int32_t *top = stk + (int64_t)(sp > 0 ? sp - 1 : 0) * Wp;
             const int32_t *drow = dt_in + (int64_t)i * n;
             int run_min = XTED_INF;
@@ -912,14 +936,14 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
                 int diag = diag_next;
                 diag_next = up;
                 const bool segend = dend == 1;
-                if (segend) diag = bord - 1;
+                if (segend) diag = bord - K.del;
                 const bool tcol = foff == dend;
                 int a;
                 if (trow && tcol) {
-                    a = diag + (ri.x != ci.y);
+                    a = diag + (ri.x != ci.y ? K.ren : 0);
                 } else {
                     int far;
-                    if (trow) far = dend - foff;
+                    if (trow) far = (dend - foff) * K.ins;
                     else if (tcol) far = rowfar;
                     else {
                         const int f = c + foff;
@@ -927,9 +951,9 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
                     }
                     a = (staged ? srow[c] : __ldcg(drow + ci.x)) + far;
                 }
-                int A = min(a, up + 1);
-                if (segend) A = min(A, bord + 1);
-                run_min = min(run_min, A + c);
+                int A = min(a, up + K.del);
+                if (segend) A = min(A, bord + K.ins);
+                run_min = min(run_min, A + c * K.ins);
                 locb[at] = run_min;
             }
             const int incl = warp_suffix_min(run_min, lane);
@@ -947,7 +971,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
                 const int c = c0 + k;
                 const int64_t at = (int64_t)k * XTED_CTA_THREADS + tid;
                 const int4 ci = cols[at];
-                const int d = min(locb[at], carry) - c;
+                const int d = min(locb[at], carry) - c * K.ins;
                 prevb[at] = d;
                 if (trow && (ci.z & XTED_COL_FOFF_MASK) == ci.w) orow[ci.x] = d;
                 if (push && spush < stack_rows && (ci.z & XTED_COL_FARCOL)) stk[(int64_t)spush * Wp + at] = d;
@@ -958,26 +982,28 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     }
 }
 
+template <bool UC>
 __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk,
                               WideShared &S, int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int width = P.chunks[u.chunk].width;
     const int tid = threadIdx.x;
-    if (width <= 256) run_group<1, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
-    else if (width <= 512) run_group<2, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
-    else if (width <= 1024) run_group<4, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
-    else if (width <= XTED_WIDE_REG_MAX) run_group<8, XTED_WARPS>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
-    else if (P.chunks[u.chunk].nseg == 1) run_wide_big(P, pr, u, stk, S, ring);
+    if (width <= 256) run_group<1, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (width <= 512) run_group<2, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (width <= 1024) run_group<4, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (width <= XTED_WIDE_REG_MAX) run_group<8, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    else if (P.chunks[u.chunk].nseg == 1) run_wide_big<UC>(P, pr, u, stk, S, ring);
     else if (tid == 0) set_error(P, XTED_EINVAL, 4, width, P.chunks[u.chunk].nseg);
 }
 
 // Half-block unit: group gid (warps 4*gid .. 4*gid+3), chunk width <= XTED_HALF_MAX.
+template <bool UC>
 __device__ void dispatch_half(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                               int32_t *ring, int32_t *cache, int32_t *cnode, int gtid, int gid) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 128) run_group<1, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
-    else if (width <= 256) run_group<2, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
-    else if (width <= 512) run_group<4, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
-    else if (width <= XTED_HALF_MAX) run_group<8, 4>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    if (width <= 128) run_group<1, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (width <= 256) run_group<2, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (width <= 512) run_group<4, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    else if (width <= XTED_HALF_MAX) run_group<8, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
     else if (gtid == 0) set_error(P, XTED_EINVAL, 6, width, 0);
 }
 
@@ -1072,8 +1098,10 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
                 // admit posted queries first: their level-0 entries go to the new
                 // query's own (least urgent) bucket, and a busy launch would
                 // otherwise only look at the mailbox once it ran out of work
+                // a record is claimed only while the launch is open (no CLOSED
+                // bit): the claim and the closing are CAS on the same word
                 int cons = mbox[XTED_MBOX_CONSUMED];
-                while (cons < mbox[XTED_MBOX_POSTED]) {
+                while (!(cons & XTED_MBOX_CLOSED) && cons < mbox[XTED_MBOX_POSTED]) {
                     if (atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons + 1) == cons) {
                         __threadfence();  // acquire: the record and its query's plan are visible from here on
                         if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
@@ -1129,7 +1157,9 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
                         atomicAdd(&P.rq_ctl[CTL_IDLE], 1);
                         idle_counted = true;
                     }
-                    if (mbox[XTED_MBOX_STOP] != 0 || ctl[CTL_LEAVING] != 0) res = CLAIM_EXIT;
+                    if (mbox[XTED_MBOX_STOP] != 0 || ctl[CTL_LEAVING] != 0 ||
+                        (mbox[XTED_MBOX_CONSUMED] & XTED_MBOX_CLOSED))
+                        res = CLAIM_EXIT;
                 } else if (ld_acquire(P.done_total) >= P.ntasks) {
                     res = CLAIM_EXIT;
                 }
@@ -1138,9 +1168,19 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
                     if (t0 == 0) {
                         t0 = now;
                     } else if (P.serve) {
+                        // Idle everywhere: close the launch to new records and
+                        // leave (the host relaunches on new work). Closing is a
+                        // CAS on the claim word, so no block can claim a record
+                        // after it and then run that query alone while the
+                        // others leave; a record posted meanwhile stays for
+                        // the next launch.
                         if (now - t0 > P.idle_exit_ns && ctl[CTL_IDLE] >= (int)gridDim.x) {
-                            atomicExch(&P.rq_ctl[CTL_LEAVING], 1);
-                            res = CLAIM_EXIT;  // idle everywhere: the host relaunches on new work
+                            const int cons = mbox[XTED_MBOX_CONSUMED];
+                            if (!(cons & XTED_MBOX_CLOSED) && cons >= mbox[XTED_MBOX_POSTED] &&
+                                atomicCAS(&P.mbox[XTED_MBOX_CONSUMED], cons, cons | XTED_MBOX_CLOSED) == cons) {
+                                atomicExch(&P.rq_ctl[CTL_LEAVING], 1);
+                                res = CLAIM_EXIT;
+                            }
                         }
                     } else if (now - t0 > P.timeout_ns) {
                         set_error(P, XTED_ETIMEOUT, 0, 0, 0);
@@ -1216,14 +1256,14 @@ __device__ void publish_record(const XKernelParams &P, int r, int lane) {
     __threadfence();
     for (int p = lo + lane; p < lo + n; p += 32) {
         const int e = __ldcg(&P.first[p]);
-        if (e >= 0) rq_publish(P, e);
+        if (e >= 0 && p != P.hold_pair && !rq_publish(P, e)) finish_served_pair(P, p, P.entries[e].bucket);
     }
     __syncwarp();
 }
 
 __global__ void xted_rq_init_kernel(XKernelParams P) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < P.npairs && P.first[p] >= 0) rq_publish(P, P.first[p]);
+    if (p < P.npairs && P.first[p] >= 0 && p != P.hold_pair) rq_publish(P, P.first[p]);
 }
 
 // Trace record of a finished task (XTED_TRACE): end time and
@@ -1301,6 +1341,7 @@ __device__ bool gang_barrier(const XKernelParams &P, int *s_phase, int *s_ok) {
 }
 
 // One striped unit, run by every gang block (all threads).
+template <bool UC>
 __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S, int32_t *ring, int32_t *cache,
                          int32_t *cnode, int *s_g) {
     // s_g: [0] phase, [1] ok, [2] task, [3] entry, [4] stripes, [5] exports, [6] feasible, [7] scan scratch
@@ -1405,10 +1446,10 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
                 int32_t *CR = prog + 32;
                 int32_t *FC = CR + (int64_t)K * R;
                 int32_t *E = FC + (int64_t)K * R;
-                run_stripe(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
+                run_stripe<UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
             }
         } else if (b == 0) {
-            dispatch_wide(P, pr, u, scratch, S, ring, cache, cnode);  // too wide or too many exports: one block
+            dispatch_wide<UC>(P, pr, u, scratch, S, ring, cache, cnode);  // too wide or too many exports: one block
         }
         __threadfence();
     }
@@ -1448,7 +1489,7 @@ static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot")
 // The persistent DP kernel. Two instantiations: without striped units (every
 // batch whose column segments fit the register paths: the gang code is left
 // out of the hot loop entirely), and with them.
-template <bool STRIPES>
+template <bool STRIPES, bool UC>
 __device__ __forceinline__ void dp_main(const XKernelParams &P) {
     __shared__ int s_next, s_k[2];
     __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch;
@@ -1505,7 +1546,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
             __syncwarp();
             __syncthreads();  // every warp is between units
             if (STRIPES && s_gtask == CLAIM_GANG) {  // this gang block's part in a striped unit
-                run_gang(P, scratch, S[0], s_ring, s_cache, s_cnode, s_gang);
+                run_gang<UC>(P, scratch, S[0], s_ring, s_cache, s_cnode, s_gang);
                 __syncthreads();
                 if (tid == 0) {
                     s_progress++;
@@ -1519,7 +1560,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
             const XPair pr = P.pairs[T.pair];
             if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
             if (T.kind_n & XTED_TASK_WIDE) {
-                dispatch_wide(P, pr, P.units[T.unit_lo], scratch, S[0], s_ring, s_cache, s_cnode);
+                dispatch_wide<UC>(P, pr, P.units[T.unit_lo], scratch, S[0], s_ring, s_cache, s_cnode);
             } else {
                 // the block's two halves take the task's units one at a time
                 const int nu = (int)(T.kind_n & 0xffff);
@@ -1534,7 +1575,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                     const int k = s_k[gid];
                     group_sync<4>(gid);  // every thread of the half has read s_k before its next claim
                     if (k >= nu) break;
-                    dispatch_half(P, pr, P.units[T.unit_lo + k], stk, S[gid], ring, cache, cnode, gtid, gid);
+                    dispatch_half<UC>(P, pr, P.units[T.unit_lo + k], stk, S[gid], ring, cache, cnode, gtid, gid);
                 }
             }
             __threadfence();
@@ -1573,7 +1614,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
             ulo = __shfl_sync(FULLMASK, ulo, 0);
             __threadfence();  // acquire: the task's inputs, seen by the claimer, are visible here too
             const XPair pr = P.pairs[pair];
-            dispatch_narrow(P, pr, P.units[ulo], lane, n_stk, n_ring, n_cache, n_cnode);
+            dispatch_narrow<UC>(P, pr, P.units[ulo], lane, n_stk, n_ring, n_cache, n_cnode);
             __threadfence();  // release this unit's writes before it is counted done
             __syncwarp();
             if (lane == 0) {
@@ -1708,29 +1749,44 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
     cp_async_wait<0>();
 }
 
-__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) { dp_main<false>(P); }
-__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel_striped(XKernelParams P) { dp_main<true>(P); }
+// Four instantiations: with or without striped units, unit or general costs.
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel(XKernelParams P) { dp_main<false, true>(P); }
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel_striped(XKernelParams P) {
+    dp_main<true, true>(P);
+}
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel_costs(XKernelParams P) {
+    dp_main<false, false>(P);
+}
+__global__ void __launch_bounds__(XTED_CTA_THREADS, 2) xted_dp_kernel_striped_costs(XKernelParams P) {
+    dp_main<true, false>(P);
+}
 
-// Result of pair p: Dtree[0][0] of its table (X-TED_CPU/TED.cpp:188).
+// Result of pair p: Dtree[0][0] of its table (X-TED_CPU/TED.cpp:188), or for
+// a pair with an empty tree the cost of inserting (m = 0) or deleting (n = 0)
+// the other one (TED.cpp:181-186, with unit costs there).
 __global__ void xted_gather_kernel(const XPair *pairs, const int32_t *trivial, const int32_t *dt,
-                                   int npairs, int32_t *out) {
+                                   int npairs, int32_t *out, int c_del, int c_ins) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npairs) return;
     const int tv = trivial[p];
-    out[p] = tv >= 0 ? tv : __ldcg(dt + pairs[p].dt_off);
+    out[p] = tv >= 0 ? (pairs[p].m == 0 ? pairs[p].n * c_ins : pairs[p].m * c_del) : __ldcg(dt + pairs[p].dt_off);
 }
 
 // ---- host-side launch helpers ----
 int dp_occupancy(int *blocks_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(xted_dp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_BYTES);
     if (e != cudaSuccess) return (int)e;
-    e = cudaFuncSetAttribute(xted_dp_kernel_striped, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_BYTES);
-    if (e != cudaSuccess) return (int)e;
-    int other = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&other, xted_dp_kernel_striped, XTED_CTA_THREADS, DP_SMEM_BYTES);
-    if (e != cudaSuccess) return (int)e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, xted_dp_kernel, XTED_CTA_THREADS, DP_SMEM_BYTES);
-    if (e == cudaSuccess && other < *blocks_per_sm) *blocks_per_sm = other;  // one grid size for both
+    int least = 1 << 30;
+    for (const void *k : {(const void *)xted_dp_kernel_striped, (const void *)xted_dp_kernel_costs,
+                          (const void *)xted_dp_kernel_striped_costs, (const void *)xted_dp_kernel}) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, DP_SMEM_BYTES);
+        if (e != cudaSuccess) return (int)e;
+        int occ = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, XTED_CTA_THREADS, DP_SMEM_BYTES);
+        if (e != cudaSuccess) return (int)e;
+        least = occ < least ? occ : least;  // one grid size for every instantiation
+    }
+    *blocks_per_sm = least;
     return (int)e;
 }
 
@@ -1749,8 +1805,10 @@ cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, P.gang_blocks > 0 ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel,
-                               args);
+    const bool unit = P.c_del == 1 && P.c_ins == 1 && P.c_ren == 1;
+    const void *k = P.gang_blocks > 0 ? (unit ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel_striped_costs)
+                                      : (unit ? (const void *)xted_dp_kernel : (const void *)xted_dp_kernel_costs);
+    return cudaLaunchKernelExC(&cfg, k, args);
 }
 
 cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s) {
@@ -1760,9 +1818,9 @@ cudaError_t launch_rq_init(const XKernelParams &P, cudaStream_t s) {
 }
 
 cudaError_t launch_gather(const XPair *pairs, const int32_t *trivial, const int32_t *dt, int npairs,
-                          int32_t *out, cudaStream_t s) {
+                          int32_t *out, int c_del, int c_ins, cudaStream_t s) {
     if (npairs <= 0) return cudaSuccess;
-    xted_gather_kernel<<<(npairs + 255) / 256, 256, 0, s>>>(pairs, trivial, dt, npairs, out);
+    xted_gather_kernel<<<(npairs + 255) / 256, 256, 0, s>>>(pairs, trivial, dt, npairs, out, c_del, c_ins);
     return cudaGetLastError();
 }
 

@@ -16,7 +16,12 @@
 // GPU (two host threads at once) race on the arena and must be serialised by
 // the caller. The first call on a device checks the device and looks up the
 // arena's device address (the array's name is only a stand-in in host code),
-// so that first call belongs before any stream capture.
+// so that first call belongs before any stream capture. With CUDA's lazy
+// module loading (the default since CUDA 12.2) that lookup is also what loads
+// this module onto the device and commits the arena's 16 MiB, so "allocates
+// nothing" holds from the second call on: a caller that hands its memory to a
+// pool makes one warm-up call at start-up, before it does so. The caller's
+// current device is restored before every return.
 //
 // Algorithm: the same right-path keyroot decomposition as the batched path
 // (orl(v) = v + size(v) - 1 in preorder; keyroots = root and every child that
@@ -268,6 +273,21 @@ int copy_tree(int32_t *A, const TreeRegs &r, const xted_tree &t, cudaStream_t s)
     return ok ? XTED_OK : XTED_ECUDA;
 }
 
+// Restores the calling thread's current device on scope exit (the entry
+// point makes `device` current for its work, and must not leave it so).
+struct DeviceRestore {
+    int prev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
+    }
+    ~DeviceRestore() {
+        if (prev >= 0 && cudaSetDevice(prev) != cudaSuccess) cudaGetLastError();
+    }
+};
+
 }  // namespace
 
 extern "C" int xted_distance_noalloc(const xted_tree *a, const xted_tree *b, int32_t device, int32_t *out) {
@@ -283,6 +303,7 @@ extern "C" int xted_distance_noalloc(const xted_tree *a, const xted_tree *b, int
         cudaGetLastError();
         return XTED_ENODEV;
     }
+    const DeviceRestore restore;
     int32_t *A = nullptr;
     int rc = arena_for(device, &A);
     if (rc) return rc;

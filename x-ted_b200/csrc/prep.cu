@@ -432,6 +432,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.rq_ctl = d_ctl;
     K.done_total = d_ctl + 2 * XTED_BUCKETS;
     K.gang_ctl = d_gctl;
+    K.hold_pair = -1;
     c->d_trivial = d_trivial;
     c->plan_dt_elems = hs->dt_elems;
     c->plan_stack_rows = std::max(hs->stack_rows, 1);

@@ -109,8 +109,9 @@ public:
             }
         return false;
     }
+    // n = 0: nothing is held (a slot whose extents were already released)
     void release(int64_t off, int64_t n) {
-        n = std::max<int64_t>(n, 1);
+        if (n <= 0) return;
         auto it = free_.emplace(off, n).first;
         auto nx = std::next(it);
         if (nx != free_.end() && it->first + it->second == nx->first) {
@@ -150,6 +151,7 @@ struct Slot {
     uint64_t ticket = 0;
     int64_t seq = 0;
     int32_t gen = 0;
+    int32_t rec = -1;            // mailbox record of the posted round
     int64_t dt_off = 0, dt_n = 0, u_off = 0, u_n = 0, t_off = 0, t_n = 0, e_off = 0, e_n = 0;
     QPlan plan;
 };
@@ -159,6 +161,7 @@ struct Slot {
 struct ServeState {
     xted_ctx *c = nullptr;
     int T = 0, S = XTED_SERVE_SLOTS, Qmax = XTED_SERVE_MAX_QUERY;  // XTED_SERVE_SLOTS == XTED_SERVE_SLOTS_MAX
+    int32_t max_tree = 0;  // largest corpus tree
     int64_t Nc_nonempty = 0;
     ServePools pools;  // host planning pools: the corpus, then one region per slot
     // device
@@ -300,6 +303,17 @@ int post(ServeState *s, int slot, Slot &sl) {
     const size_t nb = 2 * (size_t)Q.nbase, n2 = 2 * (size_t)Q.n;
     cudaStream_t st = s->cs;
     const std::vector<int32_t> zeros(2 * p.entries.size(), 0);
+    std::vector<int32_t> first_held;  // test hook: one computed pair's level 0 is never published
+    if (s->c->fault == XTED_FAULT_HOLD_PAIR) {
+        first_held = p.first;
+        for (int32_t &f : first_held)
+            if (f >= 0) {
+                f = -1;
+                break;
+            }
+        s->c->fault = 0;
+    }
+    const std::vector<int32_t> &first = first_held.empty() ? p.first : first_held;
     const int32_t words[2] = {p.need, sl.gen};
     const int32_t rec[4] = {slot, (int32_t)pair_base, T, 0};
     const int32_t posted = s->posted + 1;
@@ -310,7 +324,7 @@ int post(ServeState *s, int slot, Slot &sl) {
     rc |= upload(s->d_runs + nb, H.runs.data() + nb, n2 * sizeof(XRun), st);
     rc |= upload(s->d_chunks + nb, H.chunks.data() + nb, n2 * sizeof(XChunk), st);
     rc |= upload(s->d_pairs + pair_base, p.pairs.data(), p.pairs.size() * sizeof(XPair), st);
-    rc |= upload(s->d_first + pair_base, p.first.data(), p.first.size() * 4, st);
+    rc |= upload(s->d_first + pair_base, first.data(), first.size() * 4, st);
     rc |= upload(s->d_entries + sl.e_off, p.entries.data(), p.entries.size() * sizeof(XEntry), st);
     rc |= upload(s->d_state + 2 * sl.e_off, zeros.data(), zeros.size() * 4, st);
     rc |= upload(s->d_units + sl.u_off, p.units.data(), p.units.size() * sizeof(XUnit), st);
@@ -320,6 +334,7 @@ int post(ServeState *s, int slot, Slot &sl) {
     rc |= upload(s->d_mbox + XTED_MBOX_REC + 4 * (s->posted & (XTED_SERVE_RECS - 1)), rec, sizeof(rec), st);
     rc |= upload(s->d_mbox + XTED_MBOX_POSTED, &posted, 4, st);
     if (rc) return XTED_ECUDA;
+    sl.rec = s->posted;
     s->posted = posted;
     return XTED_OK;
 }
@@ -340,12 +355,49 @@ void finish_query(ServeState *s, Query &q) {
 void first_round(ServeState *s, const Query &q, std::vector<int32_t> &lb, std::vector<int32_t> &dist,
                  std::vector<uint8_t> &inc) {
     const int T = s->T, level = s->prune;
+    // distances are TED(query, corpus tree): deleting a query node costs
+    // cost_del, inserting a corpus node cost_ins
+    const xted_opts &o = s->c->opts;
+    const bool unit = o.cost_del == 1 && o.cost_ins == 1 && o.cost_ren == 1;
     lb.assign((size_t)T, 0);
     dist.assign((size_t)T, -1);
-    for (int t = 0; t < T; t++)
-        if (q.n == 0 || s->sorted_labels[(size_t)t].empty())
-            dist[(size_t)t] = std::max<int32_t>(q.n, (int32_t)s->sorted_labels[(size_t)t].size());
-    if (level == 1) {
+    for (int t = 0; t < T; t++) {
+        const int32_t ct = (int32_t)s->sorted_labels[(size_t)t].size();
+        if (q.n == 0) dist[(size_t)t] = ct * o.cost_ins;  // X-TED_CPU/TED.cpp:181-186, with costs
+        else if (ct == 0) dist[(size_t)t] = q.n * o.cost_del;
+    }
+    if (!unit && level > 0) {
+        // weighted bounds: the label bound under the costs, and the unit
+        // Levenshtein bound times the cheapest operation (an alignment of
+        // distance L makes at least L operations)
+        std::vector<int32_t> ql(q.lab);
+        std::sort(ql.begin(), ql.end());
+        std::vector<int32_t> qd;
+        SeqBits P;
+        if (level >= 2 && q.n > 0) {
+            qd.resize((size_t)q.n);
+            for (int v = 0; v < q.n; v++) {
+                auto it = s->dense.find(q.lab[(size_t)v]);
+                qd[(size_t)v] = it == s->dense.end() ? -1 : it->second;
+            }
+            P.build(qd.data(), q.n, (int)s->dense.size());
+        }
+        const int cmin = std::min(o.cost_del, std::min(o.cost_ins, o.cost_ren));
+        parallel_for(T, 16, [&](int64_t lo, int64_t hi) {
+            std::vector<uint64_t> work;
+            for (int64_t t = lo; t < hi; t++) {
+                if (dist[(size_t)t] >= 0) continue;
+                const std::vector<int32_t> &tl = s->sorted_labels[(size_t)t];
+                int32_t b = label_lower_bound_cost(label_common(ql.data(), q.n, tl.data(), (int)tl.size()), q.n,
+                                                   (int)tl.size(), o.cost_del, o.cost_ins, o.cost_ren);
+                if (level >= 2) {
+                    const std::vector<int32_t> &sq = s->dense_seq[(size_t)t];
+                    b = std::max<int32_t>(b, cmin * P.distance(sq.data(), (int)sq.size(), work));
+                }
+                lb[(size_t)t] = b;
+            }
+        });
+    } else if (level == 1) {
         std::vector<int32_t> ql(q.lab);
         std::sort(ql.begin(), ql.end());
         parallel_for(T, 64, [&](int64_t lo, int64_t hi) {
@@ -429,8 +481,13 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
                 const double t2 = now_ms();
                 lk.lock();
                 s->plan_us += (int64_t)((t2 - t1) * 1e3);
-                sl.need_post = true;
                 s->second_rounds++;
+                if (never_fits(s, sl.plan)) {  // round 2 covers more trees than round 1 did
+                    q.state = XTED_ENOMEM;
+                    release(s, sl);
+                    continue;
+                }
+                sl.need_post = true;
                 continue;
             }
         }
@@ -458,15 +515,46 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
     const cudaError_t kq = s->running ? cudaEventQuery(s->kev) : cudaErrorNotReady;
     if (s->running && kq == cudaSuccess) {
         s->running = false;
-        int32_t err = 0;
-        if (cudaMemcpy(&err, s->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess) err = XTED_ECUDA;
+        int32_t err = 0, cons = 0;
+        if (cudaMemcpy(&err, s->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(&cons, s->d_mbox + XTED_MBOX_CONSUMED, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            err = XTED_ECUDA;
+        int32_t consumed = cons & ~XTED_MBOX_CLOSED;
         if (err != 0) {
             s->error = err;
             fail_inflight(s, err);
             cudaMemset(s->d_err, 0, 8 * sizeof(int32_t));
             cudaMemset(s->d_slot, 0, XTED_SERVE_SLOTS * sizeof(int32_t));
+            // records of the failed queries are void: the next launch starts after them
+            cudaStreamSynchronize(s->cs);
+            consumed = s->posted;
             s->cv_done.notify_all();
             progress = true;
+        } else {
+            // Every query whose record this launch claimed has finished: a
+            // launch leaves only when all of its blocks are idle. One that
+            // has not (its work was lost) fails instead of waiting forever.
+            for (int i = 0; i < s->S; i++) {
+                Slot &sl = s->slots[i];
+                if (!sl.busy || sl.gen == 0 || sl.rec < 0 || sl.rec >= consumed) continue;
+                if (((volatile int32_t *)s->h_flags)[i] == sl.gen) continue;  // done: step 1 takes it
+                auto it = s->queries.find(sl.ticket);
+                if (it != s->queries.end()) it->second.state = XTED_ETIMEOUT;
+                s->error = XTED_ETIMEOUT;
+                const int32_t zero = 0;  // the slot's finished-pair count restarts for its next query
+                if (cudaMemcpy(s->d_slot + i, &zero, 4, cudaMemcpyHostToDevice) != cudaSuccess) cudaGetLastError();
+                release(s, sl);
+                s->cv_done.notify_all();
+                progress = true;
+            }
+        }
+        // reopen the claim word for the next launch
+        if (cons != consumed &&
+            cudaMemcpy(s->d_mbox + XTED_MBOX_CONSUMED, &consumed, 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            s->error = XTED_ECUDA;
+            fail_inflight(s, XTED_ECUDA);
+            s->cv_done.notify_all();
         }
     } else if (s->running && kq != cudaErrorNotReady) {
         cudaGetLastError();
@@ -565,6 +653,19 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
     // 5. keep a launch running while queries are in flight
     bool inflight = false;
     for (const Slot &sl : s->slots) inflight |= sl.busy && sl.gen != 0;
+    if (inflight && !s->running && s->stop) {
+        // shutting down: a query whose record no launch claimed is not started again
+        for (int i = 0; i < s->S; i++) {
+            Slot &sl = s->slots[i];
+            if (!sl.busy || sl.gen == 0) continue;
+            if (((volatile int32_t *)s->h_flags)[i] == sl.gen) continue;  // done: step 1 takes it
+            auto it = s->queries.find(sl.ticket);
+            if (it != s->queries.end()) it->second.state = XTED_ETIMEOUT;
+            release(s, sl);
+        }
+        s->cv_done.notify_all();
+        return true;
+    }
     if (inflight && !s->running) {
         // every earlier launch ended with all of its work done: start from empty rings
         cudaStreamSynchronize(s->cs);
@@ -626,6 +727,7 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
         const int rc = validate_tree(tv);
         if (rc) return rc;
         N += tr[t].n;
+        s->max_tree = std::max(s->max_tree, tr[t].n);
         R += 3 * (int64_t)tr[t].n + 1;
         nonempty += tr[t].n;
     }
@@ -652,7 +754,9 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     int rq_log2 = 12;
     while (((int64_t)1 << rq_log2) < 4 * (int64_t)XTED_SERVE_SLOTS * std::max(T, 1)) rq_log2++;
     s->rq_log2 = rq_log2;
-    const int64_t dt_cap = std::min<int64_t>(kDtCapMax, (int64_t)S * Qm * std::max<int64_t>(nonempty, 1));
+    int64_t dt_cap = std::min<int64_t>(kDtCapMax, (int64_t)S * Qm * std::max<int64_t>(nonempty, 1));
+    if (c->opts.mem_limit > 0) dt_cap = std::min<int64_t>(dt_cap, c->opts.mem_limit / 8);  // half of the limit
+    dt_cap = std::max<int64_t>(dt_cap, 1);
     int rc = XTED_OK;
     rc |= dev_alloc(s, &s->d_node, n2);
     rc |= dev_alloc(s, &s->d_krd, n2);
@@ -747,11 +851,20 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     K.slot_gen = s->d_slot + 2 * XTED_SERVE_SLOTS;
     K.results = d_results;
     K.flags = d_flags;
+    K.hold_pair = -1;
+    // the kernel's row tree is the corpus tree and its column tree the query:
+    // TED(query, corpus tree) deletes query nodes and inserts corpus nodes,
+    // so the kernel's row deletions cost cost_ins and its column insertions cost_del
+    K.c_del = c->opts.cost_ins;
+    K.c_ins = c->opts.cost_del;
+    K.c_ren = c->opts.cost_ren;
     s->worker = std::thread(worker_main, s);
     return XTED_OK;
 }
 
 }  // namespace
+
+std::mutex &serve_mutex(xted_ctx *c) { return c->serve->mu; }
 
 void serve_shutdown(xted_ctx *c) {
     ServeState *s = c->serve;
@@ -792,6 +905,10 @@ int xted_query_submit(xted_ctx *c, const xted_tree *q, int32_t k, uint64_t *tick
     ServeState *s = c->serve;
     if (!s) return XTED_EINVAL;
     if (q->n > s->Qmax) return XTED_EINVAL;
+    // every pair must fit the row scan's key range: the corpus tree is the
+    // row tree (deleted at cost_ins), the query the column tree (cost_del)
+    if ((int64_t)c->opts.cost_ins * s->max_tree + (int64_t)c->opts.cost_del * q->n >= XTED_COST_BOUND)
+        return XTED_EINVAL;
     const int rc = validate_tree(TreeView{q->n, q->labels, q->child_off, q->child_idx});
     if (rc) return rc;
     Query Q;
@@ -850,10 +967,22 @@ int xted_serve_drain(xted_ctx *c) {
     if (!s) return XTED_EINVAL;
     std::unique_lock<std::mutex> lk(s->mu);
     s->cv_work.notify_all();
+    // bounded: XTED_ETIMEOUT once no query has finished, failed or been
+    // admitted for 4 x wait_timeout_s (at least 30 s)
+    const double limit_ms = 1e3 * std::max(30.0, 4.0 * s->c->opts.wait_timeout_s);
+    int64_t mark = -1;
+    double since = now_ms();
     for (;;) {
-        bool busy = !s->pending.empty();
-        for (const Slot &sl : s->slots) busy |= sl.busy;
-        if (!busy) break;
+        int64_t busy = (int64_t)s->pending.size();
+        for (const Slot &sl : s->slots) busy += sl.busy;
+        if (busy == 0) break;
+        const int64_t m = s->served + s->pairs_served + (int64_t)s->pending.size() + 1000003 * busy;
+        if (m != mark) {
+            mark = m;
+            since = now_ms();
+        } else if (now_ms() - since > limit_ms) {
+            return XTED_ETIMEOUT;
+        }
         s->cv_done.wait_for(lk, std::chrono::milliseconds(5));
     }
     const int e = s->error;

@@ -233,6 +233,31 @@ inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const 
 // intersection) of its pairs keep their label, so
 //   TED >= m + n - 2|M| + max(0, |M| - I),
 // which falls as |M| grows; at |M| = min(m, n) it is max(m, n) - min(m, n, I).
+// The same bound under edit costs cd (delete a node of the query, m nodes),
+// ci (insert a node of the corpus tree, n nodes) and cr (label change): a
+// mapping M costs cd (m - |M|) + ci (n - |M|) + cr max(0, |M| - I), piecewise
+// linear in |M|, so its minimum over 0 <= |M| <= min(m, n) is at 0, at
+// min(I, m, n) or at min(m, n).
+inline int64_t label_common(const int32_t *a, int m, const int32_t *b, int n) {
+    int i = 0, j = 0;
+    int64_t common = 0;
+    while (i < m && j < n) {
+        if (a[i] < b[j]) i++;
+        else if (b[j] < a[i]) j++;
+        else {
+            common++;
+            i++;
+            j++;
+        }
+    }
+    return common;
+}
+inline int32_t label_lower_bound_cost(int64_t common, int m, int n, int cd, int ci, int cr) {
+    const int64_t mn = std::min(m, n), I = std::min<int64_t>(common, mn);
+    auto cost = [&](int64_t M) { return (int64_t)cd * (m - M) + (int64_t)ci * (n - M) + (int64_t)cr * std::max<int64_t>(0, M - I); };
+    return (int32_t)std::min(cost(0), std::min(cost(I), cost(mn)));
+}
+
 inline int32_t label_lower_bound(const int32_t *a, int m, const int32_t *b, int n) {
     int i = 0, j = 0, common = 0;
     while (i < m && j < n) {

@@ -185,6 +185,10 @@ struct XKernelParams {
     const int32_t *slot_need, *slot_gen;  // pairs to finish, generation to report
     int32_t *results;       // [slots * serve_pairs] distances, mapped host memory
     int32_t *flags;         // [XTED_SERVE_SLOTS] generation of the last finished query, mapped host memory
+    // ---- test hook (xted_test_fault): level 0 of this pair is never published; -1: none ----
+    int32_t hold_pair;
+    // ---- edit costs: delete a row-tree node, insert a column-tree node, change a label ----
+    int32_t c_del, c_ins, c_ren;
 };
 
 // Serving mailbox in device memory. The host writes records and then the
@@ -194,7 +198,8 @@ struct XKernelParams {
 #define XTED_SERVE_RECS 64
 #define XTED_MBOX_POSTED 0    // records posted (host)
 #define XTED_MBOX_STOP 1      // nonzero: blocks leave when idle (host)
-#define XTED_MBOX_CONSUMED 2  // records claimed (device)
+#define XTED_MBOX_CONSUMED 2  // records claimed (device), | XTED_MBOX_CLOSED once the launch leaves
+#define XTED_MBOX_CLOSED (1 << 30)  // set by the block that ends the launch: no record is claimed after it
 #define XTED_MBOX_TOP 3       // bucket of the oldest query in flight (host)
 #define XTED_MBOX_REC 4       // records: 4 ints each {slot, pair_lo, npairs, 0}
 #define XTED_MBOX_INTS (XTED_MBOX_REC + 4 * XTED_SERVE_RECS)

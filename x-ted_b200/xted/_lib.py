@@ -26,6 +26,8 @@ XTED_ETOOBIG = -8
 XTED_NOALLOC_ARENA_BYTES = 16 << 20
 XTED_MAX_NODES = 65535
 XTED_SERVE_MAX_QUERY = 8192
+XTED_FAULT_NONE, XTED_FAULT_HOLD_PAIR = 0, 1
+XTED_COST_BOUND = 1 << 17
 
 ORIENT_AUTO, ORIENT_RIGHT, ORIENT_LEFT = 0, 1, 2
 
@@ -42,7 +44,8 @@ class COpts(ctypes.Structure):
                 ("narrow_width", ctypes.c_int32), ("run_rows", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("wide_rows", ctypes.c_int32), ("half_width", ctypes.c_int32), ("tuned", ctypes.c_int32),
                 ("wait_timeout_s", ctypes.c_double), ("mem_limit", ctypes.c_int64),
-                ("stripe_min_cells", ctypes.c_int64)]
+                ("stripe_min_cells", ctypes.c_int64), ("cost_del", ctypes.c_int32), ("cost_ins", ctypes.c_int32),
+                ("cost_ren", ctypes.c_int32), ("pad_", ctypes.c_int32)]
 
 
 class CStats(ctypes.Structure):
@@ -105,6 +108,7 @@ def lib():
                                                     _i32p, _i32p, _i32p, _i32p]),
             "xted_parse_bracket": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, _i32p, _i32p,
                                                   _i64p, _i32p, _i32p, _i64p]),
+            "xted_test_fault": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

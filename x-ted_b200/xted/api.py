@@ -30,7 +30,10 @@ class Context:
                  narrow_width: Optional[int] = None, run_rows: Optional[int] = None,
                  ctas_per_sm: int = 0, wait_timeout_s: float = 20.0, mem_limit: int = 0,
                  wide_rows: int = 0, half_width: int = 0, tuned: Optional[bool] = None,
-                 stripe_min_cells: int = 0):
+                 stripe_min_cells: int = 0, costs: Optional[Tuple[int, int, int]] = None):
+        """`costs` = (delete, insert, rename) edit costs, integers >= 0; None is
+        the reference's unit cost (1, 1, 1). Delete applies to nodes of the
+        first tree of a pair, insert to nodes of the second."""
         L = _lib.lib()
         o = _lib.COpts()
         L.xted_opts_default(ctypes.byref(o))
@@ -50,6 +53,8 @@ class Context:
         o.wait_timeout_s = wait_timeout_s
         o.mem_limit = mem_limit
         o.stripe_min_cells = stripe_min_cells
+        if costs is not None:
+            o.cost_del, o.cost_ins, o.cost_ren = (int(x) for x in costs)
         self.opts = o
         h = ctypes.c_void_p()
         _lib.check(L.xted_create(ctypes.byref(h), ctypes.byref(o)), "xted_create")
@@ -118,6 +123,13 @@ class Context:
         out = np.zeros(max(self._prepared_n, 1), np.int32)
         _lib.check(_lib.lib().xted_run_prepared(self._h, out.ctypes.data_as(_lib._i32p)), "xted_run_prepared")
         return out[:self._prepared_n]
+
+    def test_fault(self, kind: int = _lib.XTED_FAULT_HOLD_PAIR) -> None:
+        """Arms one host-side fault for the next batch call or posted serving
+        query (xted_test_fault): with XTED_FAULT_HOLD_PAIR one pair's first
+        level is never made ready, so the call fails with XTED_ETIMEOUT after
+        the context's bounded wait. For failure-handling tests."""
+        _lib.check(_lib.lib().xted_test_fault(self._h, int(kind)), "xted_test_fault")
 
     def stats(self) -> dict:
         s = _lib.CStats()
