@@ -259,3 +259,29 @@ def test_cpp_wrapper_compiles_and_converts():
     r = subprocess.run([os.path.join(REPO, "tests", "cpp", "_build", "hpp_check")], capture_output=True, text=True,
                        timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def test_shard_pairs_balances_and_covers():
+    """Pair-list sharding by estimated cells (longest first, to the least
+    loaded rank): every pair on exactly one rank, loads within one pair's
+    cells of each other; the exact top-k merge of per-shard lists; contiguous
+    corpus shards."""
+    import numpy as np
+    from xted import multi
+    rng = np.random.default_rng(3)
+    cells = rng.integers(1, 10 ** 6, 1000)
+    for world in (1, 2, 3, 8):
+        parts = multi.shard_pairs(cells, world)
+        allp = np.sort(np.concatenate(parts))
+        assert np.array_equal(allp, np.arange(1000))
+        loads = [int(cells[p].sum()) for p in parts]
+        assert max(loads) - min(loads) <= int(cells.max())
+    ids, ds = multi.topk_merge([([4, 9, -1], [2, 5, -1]), ([1, 7], [2, 3])], 3)
+    assert ids.tolist() == [1, 4, 7] and ds.tolist() == [2, 2, 3]
+    ids, ds = multi.topk_merge([([0], [1])], 3)
+    assert ids.tolist() == [0, -1, -1] and ds.tolist() == [1, -1, -1]
+    from xted import gen
+    corpus = gen.corpus(50, seed=2, lo=1, hi=300)
+    ranges = multi.shard_corpus(corpus, 4)
+    assert ranges[0][0] == 0 and ranges[-1][1] == 50
+    assert all(ranges[r][1] == ranges[r + 1][0] for r in range(3))

@@ -56,3 +56,75 @@ def test_two_gloo_ranks_shard_and_aggregate():
     assert t0 == t1 == 2000.0             # time is the slowest rank's
     assert v0 == v1 == pytest.approx(256 * 2 * 3 / 2.0)
     assert g0 == g1 == pytest.approx(30 * 3 / 2.0 / 1e9)
+
+
+def _shard_main(rank, world, port, q):
+    """Two gloo ranks run the library's sharded paths with the oracle standing
+    in for each rank's GPU (no GPU here): a pair list split by estimated cells
+    and gathered, and a corpus split in contiguous shards with the top-k merge."""
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "MASTER_ADDR": "127.0.0.1",
+                       "MASTER_PORT": str(port)})
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "x-ted_b200"))
+    try:
+        import datetime
+
+        import torch.distributed as dist
+
+        import oracle
+        from xted import gen, multi
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        pairs = gen.mixed_batch(40, seed=17, lo=5, hi=120)
+        seen = []
+
+        def compute(ps):
+            seen.append(len(ps))
+            return oracle.distance_batch(ps)
+
+        got = multi.distance_batch_sharded(pairs, compute)
+        corpus = gen.corpus(30, seed=18, lo=1, hi=80)
+        queries = gen.corpus(3, seed=19, lo=1, hi=80)
+        shard = {}
+
+        def load(trees_):
+            shard["trees"] = trees_
+
+        def local_topk(qt, k):
+            d = [oracle.distance(qt, t) for t in shard["trees"]]
+            order = sorted(range(len(d)), key=lambda i: (d[i], i))[:k]
+            return order, [d[i] for i in order]
+
+        sc = multi.ShardedCorpus(corpus, load, local_topk)
+        answers = [tuple(x.tolist() for x in sc.query(qt, 7)) for qt in queries]
+        dist.destroy_process_group()
+        q.put((rank, got.tolist(), seen, sc.lo, sc.hi, answers))
+    except Exception as e:  # reported to the parent
+        q.put((rank, "error", repr(e)))
+
+
+@pytest.mark.timeout(240)
+def test_two_gloo_ranks_shard_pairs_and_corpus():
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "x-ted_b200"))
+    import oracle
+    from xted import gen
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=200) for _ in procs], key=lambda o: o[0])
+    for p in procs:
+        p.join(timeout=30)
+    assert all(len(o) == 6 for o in out), out
+    pairs = gen.mixed_batch(40, seed=17, lo=5, hi=120)
+    want = oracle.distance_batch(pairs).tolist()
+    assert out[0][1] == want and out[1][1] == want           # every rank holds every distance
+    assert sum(out[0][2]) + sum(out[1][2]) == 40 and min(out[0][2][0], out[1][2][0]) > 0
+    assert out[0][3] == 0 and out[0][4] == out[1][3] and out[1][4] == 30  # contiguous corpus shards
+    corpus = gen.corpus(30, seed=18, lo=1, hi=80)
+    for qi, qt in enumerate(gen.corpus(3, seed=19, lo=1, hi=80)):
+        d = [oracle.distance(qt, t) for t in corpus]
+        order = sorted(range(30), key=lambda i: (d[i], i))[:7]
+        assert out[0][5][qi] == (order, [d[i] for i in order]) == out[1][5][qi]
