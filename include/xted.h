@@ -83,8 +83,9 @@ typedef struct xted_opts {
     int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
     int64_t stripe_min_cells; /* a table whose column segment is wider than
                                2,048 and whose unit has at least this many
-                               cells runs in 2,048-column stripes on up to 16
-                               blocks at once (0 = 2^20; < 0: one block)    */
+                               cells runs in column stripes (512 to 2,048
+                               columns) on up to 64 blocks at once
+                               (0 = 2^20; < 0: one block)                   */
     int32_t cost_del;       /* edit costs (integers >= 0): deleting a node of */
     int32_t cost_ins;       /* the first tree, inserting a node of the second */
     int32_t cost_ren;       /* tree, and mapping two nodes whose labels differ

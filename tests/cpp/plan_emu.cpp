@@ -154,6 +154,8 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
         X.ntasks = E.ntasks;
         X.bucket = level_bucket(chain[(size_t)E.pair] - E.key, chain_max);
         X.next = E.level + 1 < H.pairs[(size_t)E.pair].L ? (int32_t)e + 1 : -1;
+        X.nnarrow = E.nntasks;
+        X.pad = 0;
     }
     H.units.assign((size_t)uoff, XUnit{-1, -1});
     H.tasks.assign((size_t)toff, XTask{-1, -1, 0, -1});
@@ -258,12 +260,17 @@ int main(int argc, char **argv) {
                 if (t.pair != E.pair || t.entry != e) FAIL("task of another entry in the range");
                 const int nu = (int)(t.kind_n & 0xffff);
                 const bool full = (t.kind_n & XTED_TASK_WIDE) != 0, half = (t.kind_n & XTED_TASK_HALF) != 0;
+                // the narrow tasks of a level are the first X.nnarrow of its range (two claim rings)
+                if ((k < X.nnarrow) != !(full || half)) FAIL("task %d of a level out of its kind's range", k);
                 const bool wide = full || half;
                 if (nu < 1 || nu > XTED_TASK_UNITS || (full && nu != 1) || (half && nu > 8)) FAIL("bad unit count %d", nu);
                 for (int u = 0; u < nu && !g_table; u++) {
                     const int w = H.chunks[(size_t)H.units[(size_t)(t.unit_lo + u)].chunk].width;
                     if (half && (w <= nw || w > XTED_HALF_MAX || w > hw)) FAIL("half unit of width %d", w);
-                    if (full && w <= XTED_HALF_MAX && w > nw && hw >= w) FAIL("whole-block unit of width %d", w);
+                    // a level's last half-width unit, alone in its task, runs on the whole block
+                    const bool lone = E.nhalf % level_bundle_half(E.nhalf) == 1;
+                    if (full && w <= XTED_HALF_MAX && w > nw && hw >= w && !lone)
+                        FAIL("whole-block unit of width %d", w);
                 }
                 const DPair &q = H.pairs[(size_t)t.pair];
                 XPair x;

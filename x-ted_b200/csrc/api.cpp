@@ -172,10 +172,10 @@ static int enqueue_step(xted_ctx *c, bool events) {
     const size_t ne = (size_t)K.nentries;
     if (cudaMemsetAsync(cnt, 0, 8 * sizeof(int32_t), c->stream) != cudaSuccess ||
         (K.ntasks > 0 &&
-         (cudaMemsetAsync(K.entry_state, 0, 2 * ne * sizeof(int32_t), c->stream) != cudaSuccess ||
-          cudaMemsetAsync(K.rq, 0xff, ((size_t)XTED_BUCKETS << K.rq_log2) * sizeof(unsigned long long),
+         (cudaMemsetAsync(K.entry_state, 0, XTED_ESTATE * ne * sizeof(int32_t), c->stream) != cudaSuccess ||
+          cudaMemsetAsync(K.rq, 0xff, ((size_t)XTED_RINGS << K.rq_log2) * sizeof(unsigned long long),
                           c->stream) != cudaSuccess ||
-          cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_BUCKETS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
+          cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_RINGS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
           cudaMemsetAsync(K.gang_ctl, 0, XTED_GCTL_INTS * sizeof(int32_t), c->stream) != cudaSuccess ||
           launch_rq_init(K, c->stream) != cudaSuccess)))
         return XTED_ECUDA;

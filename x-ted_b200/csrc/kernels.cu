@@ -276,7 +276,9 @@ static_assert(CACHE_INTS == XTED_WARPS * XTED_STACK_CACHE * NARROW_ROW, "stack c
 // table), so consecutive lanes read consecutive tree distances; one thread
 // also copies the row's node record. The thread that computes a column is not
 // the one that copied it, so a row is read only after a barrier that follows
-// every copier's wait.
+// every copier's wait. (Each thread copying its own W columns, from node ids
+// in registers, issues fewer instructions but makes each warp-wide copy touch
+// W lines instead of one; it measured 4% slower on the mixed batch.)
 template <int W>
 __device__ __forceinline__ void issue_row(const int32_t *cnode, int width, const int32_t *dt, int n,
                                           const int2 *rows, int r, int32_t *slot, int rec_at, int me, int nthr,
@@ -293,9 +295,14 @@ __device__ __forceinline__ void issue_row(const int32_t *cnode, int width, const
 // ---------------------------------------------------------------------------
 // Narrow unit: one warp, chunk width <= 32*W.
 // ---------------------------------------------------------------------------
+// Keyroots [kr_start, run end) of the unit. With `yield` set, the warp stops
+// between two keyroot tables once *yield is no longer FLOW_RUN (its block is
+// gathering for a group task) and returns the next keyroot; the tables of a
+// run are independent, so the rest runs later from there. Returns -1 when
+// the unit is done.
 template <int W, bool UC>
-__device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
-                           int32_t *ring, int32_t *cache, int32_t *cnode) {
+__device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
+                          int32_t *ring, int32_t *cache, int32_t *cnode, int kr_start, const volatile int *yield) {
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int c0 = lane * W;
@@ -325,7 +332,15 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
     const bool deep = run.depth > XTED_STACK_CACHE;
     const int stack_rows = P.stack_rows;
 
-    for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
+    for (int kr = kr_start < 0 ? run.kr_lo : kr_start; kr < run.kr_hi; kr++) {
+        if (yield && kr > run.kr_lo && kr != kr_start) {
+            int y = 0;
+            if (lane == 0) y = *yield != 0;  // FLOW_RUN == 0
+            if (__shfl_sync(FULLMASK, y, 0)) {
+                cp_async_wait<0>();
+                return kr;
+            }
+        }
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
         int prev[W];
@@ -409,6 +424,7 @@ __device__ void run_narrow(const XKernelParams &P, const XPair &pr, const XUnit 
         }
     }
     cp_async_wait<0>();
+    return -1;
 }
 
 // ---------------------------------------------------------------------------
@@ -497,7 +513,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
                 const int r = i - (PF - 1);
                 if (r >= i0)
                     issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
-                                 gtid == 0);
+                             gtid == 0);
                 cp_async_commit();
             }
             const int32_t *slot = ring + (i & (PF - 1)) * GSLOT;
@@ -611,11 +627,11 @@ __device__ __forceinline__ bool wait_progress(const XKernelParams &P, volatile i
     return false;
 }
 
-template <bool UC>
+template <int W, bool UC>
 __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                            int32_t *ring, int32_t *cache, int32_t *cnode, int s, int K, int X, int R,
                            const int32_t *expmap, int32_t *prog, int32_t *CR, int32_t *FC, int32_t *E) {
-    constexpr int W = 8, G = XTED_WARPS;
+    constexpr int G = XTED_WARPS, SW = XTED_CTA_THREADS * W;  // stripe width: W columns per thread
     constexpr int GROW = 256 * G + 8 * G;
     constexpr int GSLOT = GROW + 8;
     constexpr int PF = XTED_PREFETCH;
@@ -623,7 +639,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
     const int w = ch.width;
-    const int C0 = s * XTED_STRIPE, C1 = min(C0 + XTED_STRIPE, w), tw = C1 - C0;
+    const int C0 = s * SW, C1 = min(C0 + SW, w);
     const bool right = s + 1 < K, left = s > 0;
     const int lc0 = gtid * W, c0 = C0 + lc0;  // this thread's first column: local, in the segment
     const int pbase = pad(lc0);
@@ -645,7 +661,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             C.dend[k] = 2;
             C.fb[k] = 1;
             C.segor[k] = NOSEG;
-            C.fidx[k] = pad(min(lc0 + k, XTED_STRIPE - 1));
+            C.fidx[k] = pad(min(lc0 + k, SW - 1));
         } else {
             const int f = c + (C.dend[k] - C.fb[k]);  // orl(j)+1 in segment columns
             if (f >= w) C.fidx[k] = pad(lc0 + k);     // the border: a tree-path column (rowfar)
@@ -684,7 +700,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
             if (r >= i0)
-                issue_row<W>(cnode, tw, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
                              gtid == 0);
             cp_async_commit();
         }
@@ -694,8 +710,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(cnode, tw, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
-                                 gtid == 0);
+                    issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                             gtid == 0);
                 cp_async_commit();
             }
             if (gtid == 0 && right && ld_acquire((const int32_t *)prog_right) >= tflat + 1) {
@@ -773,7 +789,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
-                    const int32_t *src = stk + (int64_t)(sp - 1) * XTED_STRIPE + lc0;
+                    const int32_t *src = stk + (int64_t)(sp - 1) * SW + lc0;
                     int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * GROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = src[k];
@@ -786,7 +802,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = prev[k];
                     if (deep) {
-                        int32_t *g = stk + (int64_t)sp * XTED_STRIPE + lc0;
+                        int32_t *g = stk + (int64_t)sp * SW + lc0;
 #pragma unroll
                         for (int k = 0; k < W; k++) g[k] = prev[k];
                     }
@@ -816,13 +832,14 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
 }
 
 template <bool UC>
-__device__ void dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
-                                int32_t *ring, int32_t *cache, int32_t *cnode) {
+__device__ int dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
+                               int32_t *ring, int32_t *cache, int32_t *cnode, int kr_start,
+                               const volatile int *yield) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 32) run_narrow<1, UC>(P, pr, u, lane, stk, ring, cache, cnode);
-    else if (width <= 64) run_narrow<2, UC>(P, pr, u, lane, stk, ring, cache, cnode);
-    else if (width <= 128) run_narrow<4, UC>(P, pr, u, lane, stk, ring, cache, cnode);
-    else run_narrow<8, UC>(P, pr, u, lane, stk, ring, cache, cnode);
+    if (width <= 32) return run_narrow<1, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
+    if (width <= 64) return run_narrow<2, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
+    if (width <= 128) return run_narrow<4, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
+    return run_narrow<8, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
 }
 
 // ---------------------------------------------------------------------------
@@ -1016,18 +1033,27 @@ __device__ void dispatch_half(const XKernelParams &P, const XPair &pr, const XUn
 // Publishes entry e (or, past levels without tasks, the first later level
 // that has some) into its bucket's ring. Returns false when the pair has no
 // level left, i.e. the pair is finished.
+__device__ __forceinline__ void ring_push(const XKernelParams &P, int g, int e) {
+    const unsigned pos = (unsigned)atomicAdd(&P.rq_ctl[2 * g + 1], 1);
+    const unsigned head = *(volatile unsigned *)&P.rq_ctl[2 * g];
+    if (pos - head >= (1u << P.rq_log2)) {  // ring full: never overwrite a live slot
+        set_error(P, XTED_ENOMEM, 5, g, (int)pos);
+        return;
+    }
+    const unsigned long long v = ((unsigned long long)pos << 32) | (unsigned)e;
+    ((volatile unsigned long long *)P.rq)[((int64_t)g << P.rq_log2) + (pos & ((1u << P.rq_log2) - 1))] = v;
+}
+
+// Publishes entry e (or, past levels without tasks, the first later level that
+// has some): its narrow tasks into its bucket's narrow ring, its group tasks
+// into its bucket's group ring. Returns false when the pair has no level
+// left, i.e. the pair is finished.
 __device__ bool rq_publish(const XKernelParams &P, int e) {
     while (e >= 0) {
         const XEntry X = P.entries[e];
         if (X.ntasks > 0) {
-            const unsigned pos = (unsigned)atomicAdd(&P.rq_ctl[2 * X.bucket + 1], 1);
-            const unsigned head = *(volatile unsigned *)&P.rq_ctl[2 * X.bucket];
-            if (pos - head >= (1u << P.rq_log2)) {  // ring full: never overwrite a live slot
-                set_error(P, XTED_ENOMEM, 5, X.bucket, (int)pos);
-                return true;
-            }
-            const unsigned long long v = ((unsigned long long)pos << 32) | (unsigned)e;
-            ((volatile unsigned long long *)P.rq)[((int64_t)X.bucket << P.rq_log2) + (pos & ((1u << P.rq_log2) - 1))] = v;
+            if (X.nnarrow > 0) ring_push(P, XTED_KIND_NARROW * XTED_BUCKETS + X.bucket, e);
+            if (X.ntasks > X.nnarrow) ring_push(P, XTED_KIND_GROUP * XTED_BUCKETS + X.bucket, e);
             return true;
         }
         e = X.next;  // a level without tasks: go on to the next one
@@ -1035,11 +1061,11 @@ __device__ bool rq_publish(const XKernelParams &P, int e) {
     return false;
 }
 
-// Entry held by ring position pos of bucket b, or -1 if that position is not
+// Entry held by ring position pos of ring g, or -1 if that position is not
 // written yet.
-__device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned pos) {
+__device__ __forceinline__ int rq_entry(const XKernelParams &P, int g, unsigned pos) {
     const unsigned long long v =
-        ((volatile const unsigned long long *)P.rq)[((int64_t)b << P.rq_log2) + (pos & ((1u << P.rq_log2) - 1))];
+        ((volatile const unsigned long long *)P.rq)[((int64_t)g << P.rq_log2) + (pos & ((1u << P.rq_log2) - 1))];
     return (unsigned)(v >> 32) == pos ? (int)(unsigned)v : -1;
 }
 
@@ -1069,12 +1095,18 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int b, unsigned 
 // completions may publish work) one pass is made and CLAIM_NONE returned if it
 // finds nothing; only a block with nothing in flight waits, counts as idle in
 // a serving session, or ends the launch.
+// Kinds: a bit mask of XTED_KIND_* rings the claim may take from, and the
+// kind preferred within a bucket; buckets keep their priority order across
+// kinds. A block that has narrow units in flight claims narrow tasks only (a
+// group task would stop its warps until every unit in flight had finished).
 // Serving: rq_ctl words after the done counter.
-#define CTL_IDLE (2 * XTED_BUCKETS + 1)     // blocks currently idle (or gone)
-#define CTL_LEAVING (2 * XTED_BUCKETS + 2)  // nonzero once blocks have started to leave
+#define CTL_IDLE (2 * XTED_RINGS + 1)     // blocks currently idle (or gone)
+#define CTL_LEAVING (2 * XTED_RINGS + 2)  // nonzero once blocks have started to leave
+#define KINDS_NARROW 1u
+#define KINDS_ANY 3u
 
 template <bool STRIPES>
-__device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lane) {
+__device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lane, unsigned kinds, int prefer) {
     // Called by a whole warp; lane 0 claims, the warp reads every bucket's
     // head and tail in one coalesced load so that only non-empty buckets are
     // probed. Returns the same result in every lane.
@@ -1084,7 +1116,7 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
     unsigned ns = 32;
     uint64_t t0 = 0;
     bool idle_counted = false;  // serving: this block is counted in CTL_IDLE
-    static_assert(2 * XTED_BUCKETS == 32, "one lane per bucket head or tail");
+    static_assert(2 * XTED_BUCKETS == 32, "one lane per bucket head or tail of each kind");
     for (long it = 0; it < (1L << 28); it++) {
         int res = CLAIM_NONE, e_out = -1, top = XTED_BUCKETS - 1;
         if (lane == 0) {
@@ -1120,31 +1152,39 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
             return res;
         }
         top = __shfl_sync(FULLMASK, top, 0);
-        // snapshot: lane 2b holds bucket b's head, lane 2b+1 its tail
-        const int v = ctl[lane];
-        const int tl = __shfl_down_sync(FULLMASK, v, 1);
-        const unsigned nonempty = __ballot_sync(FULLMASK, (lane & 1) == 0 && (int)((unsigned)tl - (unsigned)v) > 0);
+        // snapshot: lane 2b holds bucket b's narrow-ring head, lane 2b+1 its
+        // tail; the same lanes read the group rings' words 32 further on
+        const int v0 = ctl[lane], v1 = ctl[2 * XTED_BUCKETS + lane];
+        const int tl0 = __shfl_down_sync(FULLMASK, v0, 1), tl1 = __shfl_down_sync(FULLMASK, v1, 1);
+        const unsigned ne0 = __ballot_sync(FULLMASK, (lane & 1) == 0 && (int)((unsigned)tl0 - (unsigned)v0) > 0);
+        const unsigned ne1 = __ballot_sync(FULLMASK, (lane & 1) == 0 && (int)((unsigned)tl1 - (unsigned)v1) > 0);
         if (lane == 0) {
             for (int i = 0; i < XTED_BUCKETS && res == CLAIM_NONE; i++) {
                 const int b = (top - i) & (XTED_BUCKETS - 1);
-                if (!((nonempty >> (2 * b)) & 1u)) continue;  // empty when looked at
-                for (int guard = 0; guard < 256; guard++) {
-                    const unsigned h = (unsigned)ctl[2 * b];
-                    if ((int)((unsigned)ctl[2 * b + 1] - h) <= 0) break;  // empty
-                    const int e = rq_entry(P, b, h);
-                    if (e < 0) break;  // the head position is reserved but not yet written
-                    const XEntry X = P.entries[e];
-                    if (state[2 * e] < X.ntasks) {
-                        const int k = atomicAdd(&P.entry_state[2 * e], 1);
-                        if (k < X.ntasks) {
-                            __threadfence();  // acquire: the level's inputs are visible from here on
-                            if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
-                            e_out = e;
-                            res = X.task_off + k;
-                            break;
+                for (int pass = 0; pass < 2 && res == CLAIM_NONE; pass++) {
+                    const int kind = pass == 0 ? prefer : 1 - prefer;
+                    if (!((kinds >> kind) & 1u)) continue;
+                    if (!(((kind ? ne1 : ne0) >> (2 * b)) & 1u)) continue;  // empty when looked at
+                    const int g = kind * XTED_BUCKETS + b;
+                    for (int guard = 0; guard < 256; guard++) {
+                        const unsigned h = (unsigned)ctl[2 * g];
+                        if ((int)((unsigned)ctl[2 * g + 1] - h) <= 0) break;  // empty
+                        const int e = rq_entry(P, g, h);
+                        if (e < 0) break;  // the head position is reserved but not yet written
+                        const XEntry X = P.entries[e];
+                        const int lim = kind == XTED_KIND_NARROW ? X.nnarrow : X.ntasks - X.nnarrow;
+                        if (state[XTED_ESTATE * e + kind] < lim) {
+                            const int k = atomicAdd(&P.entry_state[XTED_ESTATE * e + kind], 1);
+                            if (k < lim) {
+                                __threadfence();  // acquire: the level's inputs are visible from here on
+                                if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
+                                e_out = e;
+                                res = X.task_off + (kind == XTED_KIND_NARROW ? 0 : X.nnarrow) + k;
+                                break;
+                            }
                         }
+                        atomicCAS((int32_t *)&ctl[2 * g], (int)h, (int)(h + 1));  // exhausted: next entry
                     }
-                    atomicCAS((int32_t *)&ctl[2 * b], (int)h, (int)(h + 1));  // exhausted: next entry
                 }
             }
             if (res == CLAIM_NONE && wait) {
@@ -1213,17 +1253,20 @@ __device__ void finish_served_pair(const XKernelParams &P, int pair, int bucket)
     const int n = atomicAdd(&P.slot_done[s], 1) + 1;
     if (n == __ldcg(&P.slot_need[s])) {
         P.slot_done[s] = 0;
-        // Every position left in the query's bucket names one of its own,
-        // now exhausted, entries (a bucket serves one query at a time). Move
-        // the head past them before the host may hand those entry ids to a
-        // new query: a claimer must never find an old position whose entry
-        // id has been reused.
-        volatile int32_t *ctl = P.rq_ctl + 2 * bucket;
-        const unsigned tl = (unsigned)ctl[1];
-        for (int g = 0; g < 1024; g++) {
-            const unsigned h = (unsigned)ctl[0];
-            if ((int)(tl - h) <= 0) break;
-            atomicCAS((int32_t *)&P.rq_ctl[2 * bucket], (int)h, (int)tl);
+        // Every position left in the query's bucket (both its rings) names
+        // one of its own, now exhausted, entries (a bucket serves one query at
+        // a time). Move the heads past them before the host may hand those
+        // entry ids to a new query: a claimer must never find an old position
+        // whose entry id has been reused.
+        for (int kind = 0; kind < 2; kind++) {
+            const int rg = kind * XTED_BUCKETS + bucket;
+            volatile int32_t *ctl = P.rq_ctl + 2 * rg;
+            const unsigned tl = (unsigned)ctl[1];
+            for (int g = 0; g < 1024; g++) {
+                const unsigned h = (unsigned)ctl[0];
+                if ((int)(tl - h) <= 0) break;
+                atomicCAS((int32_t *)&P.rq_ctl[2 * rg], (int)h, (int)tl);
+            }
         }
         __threadfence_system();
         ((volatile int32_t *)P.flags)[s] = __ldcg(&P.slot_gen[s]);
@@ -1233,7 +1276,7 @@ __device__ void finish_served_pair(const XKernelParams &P, int pair, int bucket)
 // After a task (all its writes fenced and the block synchronised).
 __device__ void complete_task(const XKernelParams &P, int e, int pair) {
     const XEntry X = P.entries[e];
-    const int done = atomicAdd(&P.entry_state[2 * e + 1], 1) + 1;
+    const int done = atomicAdd(&P.entry_state[XTED_ESTATE * e + 2], 1) + 1;
     if (done == X.ntasks) {
         __threadfence();  // acquire the level's other tasks, release to the next level's claimers
         if (!rq_publish(P, X.next) && P.serve) finish_served_pair(P, pair, X.bucket);
@@ -1344,7 +1387,7 @@ __device__ bool gang_barrier(const XKernelParams &P, int *s_phase, int *s_ok) {
 template <bool UC>
 __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S, int32_t *ring, int32_t *cache,
                          int32_t *cnode, int *s_g) {
-    // s_g: [0] phase, [1] ok, [2] task, [3] entry, [4] stripes, [5] exports, [6] feasible, [7] scan scratch
+    // s_g: [0] phase, [1] ok, [2] task, [3] entry, [4] stripes, [5] exports, [6] feasible, [7] columns per thread
     const int tid = threadIdx.x, b = blockIdx.x;
     volatile int32_t *g = P.gang_ctl;
     if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // A: every gang block is here
@@ -1369,14 +1412,19 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
         }
         __syncthreads();
         const int t = s_g[2];
-        int K = 0, X = 0, feasible = 0;
+        int K = 0, X = 0, feasible = 0, SWd = XTED_STRIPE;
         if (t >= 0) {
             const XTask T = P.tasks[t];
             const XUnit u = P.units[T.unit_lo];
             const XChunk ch = P.chunks[u.chunk];
             const XPair pr = P.pairs[T.pair];
             const int w = ch.width, R = P.runs[u.run].rows;
-            K = (w + XTED_STRIPE - 1) / XTED_STRIPE;
+            // the narrowest stripes (at least XTED_STRIPE_MIN_W columns per
+            // thread) that the gang's blocks cover: more stripes run a
+            // table's rows in parallel, each row passed right to left
+            SWd = XTED_CTA_THREADS * XTED_STRIPE_MIN_W;
+            while (SWd < XTED_STRIPE && (w + SWd - 1) / SWd > P.gang_blocks) SWd *= 2;
+            K = (w + SWd - 1) / SWd;
             int32_t *expmap = P.gang_buf;
             // mark the far columns that cross a stripe boundary, then number them
             for (int c = tid; c < w; c += XTED_CTA_THREADS) expmap[c] = 0;
@@ -1387,7 +1435,7 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
                 for (int c = tid; c < w; c += XTED_CTA_THREADS) {
                     const int j = j0 + c;
                     const int f = c + ((__ldg(&nodes[j]).y & XTED_ROW_ORL_MASK) + 1 - j);
-                    if (f < w && f / XTED_STRIPE != c / XTED_STRIPE) expmap[f] = 1;
+                    if (f < w && f / SWd != c / SWd) expmap[f] = 1;
                 }
             }
             __syncthreads();
@@ -1411,7 +1459,7 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
             }
             X = total;
             const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
-            const int64_t need = wal + 32 + 2 * (int64_t)K * R + (int64_t)R * X;
+            const int64_t need = wal + XTED_GANG_MAX + 2 * (int64_t)K * R + (int64_t)R * X;
             feasible = K <= P.gang_blocks && need <= P.gang_cap;
             if (tid < XTED_GANG_MAX) P.gang_buf[wal + tid] = 0;  // progress words
         }
@@ -1423,15 +1471,16 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
             g[XTED_GCTL_DESC + 2] = K;
             g[XTED_GCTL_DESC + 3] = X;
             g[XTED_GCTL_DESC + 4] = feasible;
+            g[XTED_GCTL_DESC + 5] = SWd / XTED_CTA_THREADS;
             __threadfence();
         }
     }
     if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // B: the layout is ready
     if (tid == 0) {
-        for (int q = 0; q < 5; q++) s_g[2 + q] = g[XTED_GCTL_DESC + q];
+        for (int q = 0; q < 6; q++) s_g[2 + q] = g[XTED_GCTL_DESC + q];
     }
     __syncthreads();
-    const int t = s_g[2], e = s_g[3], K = s_g[4], X = s_g[5], feasible = s_g[6];
+    const int t = s_g[2], e = s_g[3], K = s_g[4], X = s_g[5], feasible = s_g[6], SWW = s_g[7];
     if (t >= 0) {
         __threadfence();  // acquire: the unit's inputs (complete before it was published) and the layout
         const XTask T = P.tasks[t];
@@ -1443,10 +1492,15 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
                 const int w = P.chunks[u.chunk].width, R = P.runs[u.run].rows;
                 const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
                 int32_t *prog = P.gang_buf + wal;
-                int32_t *CR = prog + 32;
+                int32_t *CR = prog + XTED_GANG_MAX;
                 int32_t *FC = CR + (int64_t)K * R;
                 int32_t *E = FC + (int64_t)K * R;
-                run_stripe<UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
+                if (SWW == 2)
+                    run_stripe<2, UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
+                else if (SWW == 4)
+                    run_stripe<4, UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
+                else
+                    run_stripe<8, UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
             }
         } else if (b == 0) {
             dispatch_wide<UC>(P, pr, u, scratch, S, ring, cache, cnode);  // too wide or too many exports: one block
@@ -1471,7 +1525,7 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
 // claims the next task (one claimer at a time). A group task (half or whole
 // block) gathers every warp at a block barrier once they are between units.
 #define FLOW_SLOTS 16  // > warps + 1: every open task has a unit running or unclaimed
-#define FLOW_RUN 0
+#define FLOW_RUN 0  // zero: run_narrow's yield test reads "mode != 0"
 #define FLOW_GROUP 1
 #define FLOW_EXIT 2
 // A slot's units are handed out through one word, (units << 8) | handed out:
@@ -1485,6 +1539,8 @@ struct FlowSlot {
     int pad[2];
 };
 static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot");
+#define CHAIN_MAX 2  // group tasks run back to back while narrow units wait
+#define PARK_SLOTS 16  // parked narrow units (at most one per warp is ever in flight; spare room for races)
 
 // The persistent DP kernel. Two instantiations: without striped units (every
 // batch whose column segments fit the register paths: the gang code is left
@@ -1492,9 +1548,14 @@ static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot")
 template <bool STRIPES, bool UC>
 __device__ __forceinline__ void dp_main(const XKernelParams &P) {
     __shared__ int s_next, s_k[2];
-    __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch;
+    __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch, s_chain;
+    __shared__ int s_role;  // XTED_KIND_* the block last claimed: the kind it prefers when idle
     __shared__ int s_gang[8];  // gang protocol: barrier phase, status, descriptor
     __shared__ FlowSlot s_fs[FLOW_SLOTS];
+    // narrow units parked between two keyroot tables while the block ran a
+    // group task: x flow slot, y unit, z pair, w next keyroot
+    __shared__ int s_park[4 * PARK_SLOTS];
+    __shared__ unsigned s_park_full, s_park_held;
     __shared__ WideShared S[2];
     extern __shared__ __align__(16) int32_t s_dyn[];  // ring | stack cache | column nodes (DP_SMEM_BYTES)
     int32_t *s_ring = s_dyn;
@@ -1510,6 +1571,10 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
         s_fs[tid].task = -1;
     }
     if (tid == 0) {
+        s_park_full = 0;
+        s_park_held = 0;
+        s_chain = 0;
+        s_role = (blockIdx.x & 1) ? XTED_KIND_NARROW : XTED_KIND_GROUP;
         s_mode = FLOW_RUN;
         s_lock = -1;
         s_progress = 0;
@@ -1580,18 +1645,87 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
             }
             __threadfence();
             __syncthreads();
-            if (tid == 0) {
-                complete_task(P, s_gentry, T.pair);
-                if (P.trace) trace_task_end(P, t);
-                s_progress++;
-                *vmode = FLOW_RUN;
+            if (warp == 0) {
+                // Every warp waits at the barrier below, so the block looks for
+                // its next task now: another group task (or a striped unit for
+                // a gang block) then runs without gathering the warps again,
+                // which costs them the tail of whatever they were running. A
+                // narrow task found here is opened as usual. While parked or
+                // open narrow units wait, at most CHAIN_MAX group tasks chain.
+                int nt = CLAIM_NONE, ne = -1, allow = 0;
+                if (lane == 0) {
+                    complete_task(P, s_gentry, T.pair);
+                    if (P.trace) trace_task_end(P, t);
+                    s_progress++;
+                    bool waiting = *(volatile unsigned *)&s_park_full != 0, room = false;
+                    for (int q = 0; q < FLOW_SLOTS; q++) {
+                        const int w = vfs[q].word;
+                        if ((w & 255) < (w >> 8)) waiting = true;
+                        if ((w >> 8) == 0) room = true;
+                    }
+                    allow = room && (!waiting || s_chain < CHAIN_MAX);
+                }
+                if (__shfl_sync(FULLMASK, allow, 0))
+                    nt = claim_task<STRIPES>(P, &ne, false, lane, KINDS_ANY, XTED_KIND_GROUP);
+                if (lane == 0) {
+                    bool stay = false;
+                    if (nt == CLAIM_GANG) {
+                        s_gtask = CLAIM_GANG;
+                        stay = true;
+                    } else if (nt >= 0) {
+                        const XTask T2 = P.tasks[nt];
+                        if (P.trace) P.trace[4 * (int64_t)nt] = global_ns();
+                        if (STRIPES && (T2.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 &&
+                            gang_push(P, nt, ne, (int64_t)P.runs[P.units[T2.unit_lo].run].rows *
+                                                     P.chunks[P.units[T2.unit_lo].chunk].width < XTED_GANG_BIG_CELLS)) {
+                            // handed to the gang
+                        } else if (T2.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
+                            s_gtask = nt;
+                            s_gentry = ne;
+                            s_next = 0;
+                            stay = true;
+                        } else {
+                            s_role = XTED_KIND_NARROW;
+                            int q = 0;
+                            while (q < FLOW_SLOTS - 1 && (vfs[q].word >> 8) != 0) q++;  // room was seen
+                            vfs[q].task = nt;
+                            vfs[q].entry = ne;
+                            vfs[q].pair = T2.pair;
+                            vfs[q].unit_lo = T2.unit_lo;
+                            vfs[q].done = 0;
+                            __threadfence_block();
+                            atomicExch(&s_fs[q].word, (int)(T2.kind_n & 0xffff) << 8);
+                            if (P.trace) P.trace[4 * (int64_t)nt + 1] = global_ns();
+                        }
+                    }
+                    s_chain = stay ? s_chain + 1 : 0;
+                    __threadfence_block();
+                    *vmode = nt == CLAIM_EXIT ? FLOW_EXIT : (stay ? FLOW_GROUP : FLOW_RUN);
+                }
+                nt = __shfl_sync(FULLMASK, nt, 0);
+                ne = __shfl_sync(FULLMASK, ne, 0);
+                if (nt == CLAIM_RECORD) publish_record(P, ne, lane);
             }
             __syncthreads();
             continue;
         }
-        // a unit of an open narrow task
-        int slot = -1, k = 0;
+        // a parked unit first (it holds a slot's task open), else a new unit of an open narrow task
+        int slot = -1, k = 0, kr0 = -1, upark = 0, ppark = 0;
         if (lane == 0) {
+            for (unsigned f = *(volatile unsigned *)&s_park_full; f != 0 && slot < 0;
+                 f = *(volatile unsigned *)&s_park_full) {
+                const unsigned bit = f & (0u - f);
+                if (atomicAnd(&s_park_full, ~bit) & bit) {
+                    const int i = __ffs(bit) - 1;
+                    const volatile int *pk = s_park + 4 * i;
+                    slot = pk[0];
+                    upark = pk[1];
+                    ppark = pk[2];
+                    kr0 = pk[3];
+                    __threadfence_block();
+                    atomicAnd(&s_park_held, ~bit);  // the entry may be reused
+                }
+            }
             for (int q = 0; q < FLOW_SLOTS && slot < 0; q++) {
                 const int w = vfs[q].word;
                 if ((w & 255) < (w >> 8)) {
@@ -1607,14 +1741,47 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
         if (slot >= 0) {
             int pair = 0, ulo = 0;
             if (lane == 0) {
-                pair = vfs[slot].pair;
-                ulo = vfs[slot].unit_lo + k;
+                pair = kr0 >= 0 ? ppark : vfs[slot].pair;
+                ulo = kr0 >= 0 ? upark : vfs[slot].unit_lo + k;
             }
             pair = __shfl_sync(FULLMASK, pair, 0);
             ulo = __shfl_sync(FULLMASK, ulo, 0);
+            kr0 = __shfl_sync(FULLMASK, kr0, 0);
             __threadfence();  // acquire: the task's inputs, seen by the claimer, are visible here too
             const XPair pr = P.pairs[pair];
-            dispatch_narrow<UC>(P, pr, P.units[ulo], lane, n_stk, n_ring, n_cache, n_cnode);
+            // with no room to park (never expected), the unit runs on to its end
+            bool parked = false;
+            for (const volatile int *yield = vmode;; yield = nullptr) {
+                const int next = dispatch_narrow<UC>(P, pr, P.units[ulo], lane, n_stk, n_ring, n_cache, n_cnode, kr0,
+                                                     yield);
+                if (next < 0) break;
+                // the block gathers for a group task: park the rest of the unit
+                int ok = 0;
+                if (lane == 0) {
+                    for (int i = 0; i < PARK_SLOTS && !ok; i++) {
+                        const unsigned bit = 1u << i;
+                        if (!(atomicOr(&s_park_held, bit) & bit)) {
+                            volatile int *pk = s_park + 4 * i;
+                            pk[0] = slot;
+                            pk[1] = ulo;
+                            pk[2] = pair;
+                            pk[3] = next;
+                            __threadfence_block();
+                            atomicOr(&s_park_full, bit);
+                            ok = 1;
+                        }
+                    }
+                }
+                kr0 = next;
+                if (__shfl_sync(FULLMASK, ok, 0)) {
+                    parked = true;
+                    break;
+                }
+            }
+            if (parked) {
+                __syncwarp();
+                continue;
+            }
             __threadfence();  // release this unit's writes before it is counted done
             __syncwarp();
             if (lane == 0) {
@@ -1653,7 +1820,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                             room = true;
                         }
                     }
-                    stop = *vmode != FLOW_RUN || open || !room;
+                    stop = *vmode != FLOW_RUN || open || !room || *(volatile unsigned *)&s_park_full != 0;
                     if (!stop && busy && *vprog == pg0 && global_ns() - c0 > idle_limit) {
                         set_error(P, XTED_ETIMEOUT, 8, warp, pg0);
                         stop = 2;
@@ -1663,7 +1830,10 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                 busy = __shfl_sync(FULLMASK, busy, 0);
                 if (stop == 2) t = CLAIM_EXIT;
                 if (stop) break;
-                t = claim_task<STRIPES>(P, &e, !busy, lane);
+                // narrow units in flight: narrow tasks only; an idle block takes
+                // either kind, its role's first within a bucket
+                t = claim_task<STRIPES>(P, &e, !busy, lane, busy ? KINDS_NARROW : KINDS_ANY,
+                                        busy ? XTED_KIND_NARROW : *(volatile int *)&s_role);
                 if (t != CLAIM_NONE) break;
                 __nanosleep(ns);  // nothing ready while units of this block run: poll again soon
                 __syncwarp();
@@ -1686,9 +1856,11 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                         s_gtask = t;
                         s_gentry = e;
                         s_next = 0;
+                        s_role = XTED_KIND_GROUP;
                         __threadfence_block();
                         *vmode = FLOW_GROUP;
                     } else {
+                        s_role = XTED_KIND_NARROW;
                         int q = 0;
                         while (q < FLOW_SLOTS - 1 && (vfs[q].word >> 8) != 0) q++;  // room was seen; only the claimer fills
                         vfs[q].task = t;

@@ -65,6 +65,7 @@ struct DLevel {
     int32_t pair, level;
     int32_t nwide, nnarrow, nhalf;
     int32_t ntasks, entry;  // tasks at this level; this entry's index
+    int32_t nntasks;        // its narrow tasks (the first ones of its range)
     int32_t task_off, unit_off;
     int64_t key;            // estimate, then the earliest start of the level (see k_pair_rank)
 };
@@ -426,7 +427,8 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     E.nwide = (int32_t)wide;
     E.nnarrow = (int32_t)narrow;
     E.nhalf = (int32_t)half;
-    E.ntasks = (int32_t)(wide + (narrow + bundle - 1) / bundle + (half + bundle_h - 1) / bundle_h);
+    E.nntasks = (int32_t)((narrow + bundle - 1) / bundle);
+    E.ntasks = (int32_t)(wide + E.nntasks + (half + bundle_h - 1) / bundle_h);
     *est_out = est;
 }
 
@@ -487,7 +489,11 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
             }
         }
     }
-    if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_HALF | (uint32_t)bundle, bundle_lo};
+    // a last task of one half-block unit would leave the block's other half
+    // idle for the whole unit: it runs on the whole block instead
+    if (bundle > 0)
+        tasks[t++] = XTask{E.pair, E.entry, (bundle == 1 ? XTED_TASK_WIDE : XTED_TASK_HALF) | (uint32_t)bundle,
+                           bundle_lo};
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         const int32_t cw_lo = cb.chunk_lo + cb.nnarrow + cb.nhalf, cw_hi = cw_lo + cb.nwide;

@@ -163,6 +163,8 @@ __global__ void k_level_offsets(DLevel *lv, int64_t nent, const int64_t *task_sc
     X.ntasks = E.ntasks;
     X.bucket = level_bucket(chain[E.pair] - E.key, sum->chain_max);
     X.next = E.level + 1 < pairs[E.pair].L ? (int32_t)e + 1 : -1;
+    X.nnarrow = E.nntasks;
+    X.pad = 0;
     entries[e] = X;
 }
 
@@ -393,9 +395,9 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     // ---- buffer C: units, tasks and the ready queue's state ----
     int rq_log2 = 0;
     while (((int64_t)1 << rq_log2) < (int64_t)E1) rq_log2++;
-    const size_t rq_slots = (size_t)XTED_BUCKETS << rq_log2;
+    const size_t rq_slots = (size_t)XTED_RINGS << rq_log2;
     rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
-                                         8 * rq_slots + 4 * (2 * E1 + (size_t)npairs + 2 * XTED_BUCKETS + 8) +
+                                         8 * rq_slots + 4 * (XTED_ESTATE * E1 + (size_t)npairs + 2 * XTED_RINGS + 8) +
                                          4 * XTED_GCTL_INTS +
                                          8 * 256);
     if (rc) return rc;
@@ -403,9 +405,9 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     XUnit *d_units_out = cw.take<XUnit>((size_t)nunits);
     XTask *d_tasks_out = cw.take<XTask>((size_t)ntasks);
     int32_t *d_first = cw.take<int32_t>((size_t)npairs);
-    int32_t *d_state = cw.take<int32_t>(2 * E1);  // claimed, done per entry
+    int32_t *d_state = cw.take<int32_t>(XTED_ESTATE * E1);  // narrow claimed, group claimed, done per entry
     unsigned long long *d_rq = cw.take<unsigned long long>(rq_slots);
-    int32_t *d_ctl = cw.take<int32_t>(2 * XTED_BUCKETS + 8);  // heads/tails, then the done counter
+    int32_t *d_ctl = cw.take<int32_t>(2 * XTED_RINGS + 8);  // heads/tails, then the done counter
     int32_t *d_gctl = cw.take<int32_t>(XTED_GCTL_INTS);       // striped units: ring, barrier, descriptor
     if (nent > 0) k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out);
     k_pair_finalize<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_xpairs,
@@ -430,7 +432,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.rq = d_rq;
     K.rq_log2 = rq_log2;
     K.rq_ctl = d_ctl;
-    K.done_total = d_ctl + 2 * XTED_BUCKETS;
+    K.done_total = d_ctl + 2 * XTED_RINGS;
     K.gang_ctl = d_gctl;
     K.hold_pair = -1;
     c->d_trivial = d_trivial;

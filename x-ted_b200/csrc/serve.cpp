@@ -302,7 +302,7 @@ int post(ServeState *s, int slot, Slot &sl) {
     const DTree &Q = H.trees[(size_t)(T + slot)];
     const size_t nb = 2 * (size_t)Q.nbase, n2 = 2 * (size_t)Q.n;
     cudaStream_t st = s->cs;
-    const std::vector<int32_t> zeros(2 * p.entries.size(), 0);
+    const std::vector<int32_t> zeros(XTED_ESTATE * p.entries.size(), 0);
     std::vector<int32_t> first_held;  // test hook: one computed pair's level 0 is never published
     if (s->c->fault == XTED_FAULT_HOLD_PAIR) {
         first_held = p.first;
@@ -326,7 +326,7 @@ int post(ServeState *s, int slot, Slot &sl) {
     rc |= upload(s->d_pairs + pair_base, p.pairs.data(), p.pairs.size() * sizeof(XPair), st);
     rc |= upload(s->d_first + pair_base, first.data(), first.size() * 4, st);
     rc |= upload(s->d_entries + sl.e_off, p.entries.data(), p.entries.size() * sizeof(XEntry), st);
-    rc |= upload(s->d_state + 2 * sl.e_off, zeros.data(), zeros.size() * 4, st);
+    rc |= upload(s->d_state + XTED_ESTATE * sl.e_off, zeros.data(), zeros.size() * 4, st);
     rc |= upload(s->d_units + sl.u_off, p.units.data(), p.units.size() * sizeof(XUnit), st);
     rc |= upload(s->d_tasks + sl.t_off, p.tasks.data(), p.tasks.size() * sizeof(XTask), st);
     rc |= upload(s->d_slot + XTED_SERVE_SLOTS + slot, &words[0], 4, st);      // slot_need
@@ -669,8 +669,8 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
     if (inflight && !s->running) {
         // every earlier launch ended with all of its work done: start from empty rings
         cudaStreamSynchronize(s->cs);
-        bool ok = cudaMemsetAsync(s->d_rq, 0xff, ((size_t)XTED_BUCKETS << s->rq_log2) * 8, s->ks) == cudaSuccess &&
-                  cudaMemsetAsync(s->d_ctl, 0, (2 * XTED_BUCKETS + 8) * 4, s->ks) == cudaSuccess &&
+        bool ok = cudaMemsetAsync(s->d_rq, 0xff, ((size_t)XTED_RINGS << s->rq_log2) * 8, s->ks) == cudaSuccess &&
+                  cudaMemsetAsync(s->d_ctl, 0, (2 * XTED_RINGS + 8) * 4, s->ks) == cudaSuccess &&
                   launch_dp(s->K, s->c->grid, s->ks) == cudaSuccess &&
                   cudaEventRecord(s->kev, s->ks) == cudaSuccess;
         if (!ok) {
@@ -766,11 +766,11 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     rc |= dev_alloc(s, &s->d_pairs, (size_t)S * T);
     rc |= dev_alloc(s, &s->d_first, (size_t)S * T);
     rc |= dev_alloc(s, &s->d_entries, (size_t)kEntryCap);
-    rc |= dev_alloc(s, &s->d_state, 2 * (size_t)kEntryCap);
+    rc |= dev_alloc(s, &s->d_state, XTED_ESTATE * (size_t)kEntryCap);
     rc |= dev_alloc(s, &s->d_units, (size_t)kUnitCap);
     rc |= dev_alloc(s, &s->d_tasks, (size_t)kTaskCap);
-    rc |= dev_alloc(s, &s->d_rq, (size_t)XTED_BUCKETS << rq_log2);
-    rc |= dev_alloc(s, &s->d_ctl, 2 * XTED_BUCKETS + 8);
+    rc |= dev_alloc(s, &s->d_rq, (size_t)XTED_RINGS << rq_log2);
+    rc |= dev_alloc(s, &s->d_ctl, 2 * XTED_RINGS + 8);
     rc |= dev_alloc(s, &s->d_mbox, XTED_MBOX_INTS);
     rc |= dev_alloc(s, &s->d_slot, 3 * XTED_SERVE_SLOTS);
     rc |= dev_alloc(s, &s->d_err, 8);
@@ -837,7 +837,7 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
     K.rq = s->d_rq;
     K.rq_log2 = rq_log2;
     K.rq_ctl = s->d_ctl;
-    K.done_total = s->d_ctl + 2 * XTED_BUCKETS;
+    K.done_total = s->d_ctl + 2 * XTED_RINGS;
     K.error = s->d_err;
     K.error_info = s->d_err + 1;
     K.timeout_ns = (uint64_t)(c->opts.wait_timeout_s * 1e9);

@@ -222,6 +222,8 @@ inline void serve_plan_query(ServePools &s, int slot, const int32_t *lab, const 
         X.ntasks = E.ntasks;
         X.bucket = 0;
         X.next = E.level + 1 < dp[(size_t)E.pair].L ? (int32_t)e + 1 : -1;
+        X.nnarrow = E.nntasks;
+        X.pad = 0;
     }
 }
 

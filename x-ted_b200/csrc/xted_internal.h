@@ -86,8 +86,9 @@ struct XUnit {
 // into XTED_STRIPE-column stripes, one per gang block (blocks 0 .. gang_blocks-1
 // of the launch), run concurrently with the stripes' row carries passed right
 // to left through the gang buffer.
-#define XTED_STRIPE 2048
-#define XTED_GANG_MAX 16
+#define XTED_STRIPE 2048        // widest stripe (8 columns per thread)
+#define XTED_STRIPE_MIN_W 2     // narrowest stripe: 2 columns per thread (512 columns)
+#define XTED_GANG_MAX 64
 #define XTED_GANG_RING 256
 #define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
 // Units under XTED_GANG_BIG_CELLS go to the gang only while fewer than
@@ -101,7 +102,7 @@ struct XUnit {
 #define XTED_GCTL_TAIL 0
 #define XTED_GCTL_HEAD 1
 #define XTED_GCTL_BAR 2
-#define XTED_GCTL_DESC 4   // task, entry, stripes, exports, feasible (5 ints)
+#define XTED_GCTL_DESC 4   // task, entry, stripes, exports, feasible, columns per thread (6 ints)
 #define XTED_GCTL_RING 16
 #define XTED_GCTL_INTS (XTED_GCTL_RING + 4 * XTED_GANG_RING)
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
@@ -134,12 +135,24 @@ struct XTask {
 // reference instead runs one host-synchronised level at a time
 // (X-TED_CPU/parallel_computing.cpp:155-182, X-TED_GPU/parallel_X_TED.cu:312-387).
 #define XTED_BUCKETS 16
+// Every bucket has two rings: one for the narrow tasks of its entries (run by
+// single warps, a block's warps independently) and one for their group tasks
+// (half- and whole-block units, striped units), so that a block busy with
+// narrow units can keep claiming narrow work instead of stopping all its
+// warps for a group task. Ring index = kind * XTED_BUCKETS + bucket.
+#define XTED_KIND_NARROW 0
+#define XTED_KIND_GROUP 1
+#define XTED_RINGS (2 * XTED_BUCKETS)
+// entry_state words per entry: narrow tasks claimed, group tasks claimed, tasks done
+#define XTED_ESTATE 3
 
 struct XEntry {
     int32_t task_off;  // first task
     int32_t ntasks;
     int32_t bucket;    // priority: larger = longer remaining critical path of the pair
     int32_t next;      // entry of the pair's next level, -1 after the last level
+    int32_t nnarrow;   // tasks [task_off, task_off + nnarrow) are narrow, the rest group tasks
+    int32_t pad;
 };
 
 struct XKernelParams {
@@ -159,13 +172,13 @@ struct XKernelParams {
     int32_t stack_rows;   // stack capacity in rows
     int32_t ntasks;
     int32_t nentries, npairs;
-    int32_t *entry_state; // [2 * nentries]: tasks claimed, tasks done
-    // Bucket b's ring is rq[b << rq_log2 ...]; queue position pos lives in
+    int32_t *entry_state; // [XTED_ESTATE * nentries]: narrow claimed, group claimed, done
+    // Ring g's slots are rq[g << rq_log2 ...]; queue position pos lives in
     // slot pos & (2^rq_log2 - 1) as (pos << 32 | entry), so a reader knows a
     // slot holds position pos and not an older or not-yet-written one.
     unsigned long long *rq;
     int32_t rq_log2;
-    int32_t *rq_ctl;      // [2 * XTED_BUCKETS]: head, tail of each bucket (unsigned positions)
+    int32_t *rq_ctl;      // [2 * XTED_RINGS]: head, tail of each ring (unsigned positions), then counters
     int32_t *done_total;  // finished tasks
     int32_t *error;       // 0 = ok; else an XTED error code
     int32_t *error_info;  // [4] diagnostics of the first error

@@ -36,7 +36,7 @@ BUCKETS = [  # (max_n, tree sizes drawn log-uniformly from [lo, hi), pairs in th
 ]
 RUN_ROWS = [16, 32, 64, 128]
 NARROW = [128, 256]
-HALF = [-1, 384, 512]
+HALF = [-1, 384, 512, 768, 1024]
 
 HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "csrc", "tune_table.h")
 
