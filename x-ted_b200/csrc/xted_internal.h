@@ -119,7 +119,8 @@ static inline int64_t xted_wide_big_scratch(int64_t w, int64_t sr) {
 #ifndef XTED_TASK_UNITS
 #define XTED_TASK_UNITS 32   // narrow units per task (claimed by the block's warps dynamically)
 #endif
-#define XTED_PREFETCH 4      // rows of tree distances in flight per unit (cp.async ring depth)
+#define XTED_PREFETCH 2      // rows of tree distances in flight per unit (cp.async ring depth; 2 measured
+                             // faster than 4 or 8 on the mixed batch: the smaller ring leaves more L1)
 
 struct XTask {
     int32_t pair;
