@@ -41,6 +41,10 @@ __device__ __forceinline__ int ld_acquire(const int32_t *p) {
     return v;
 }
 
+__device__ __forceinline__ void st_release(int32_t *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -438,6 +442,8 @@ struct __align__(16) WideShared {
     int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
     int ends[XTED_WARPS];
     int cin;                    // stripes: the right neighbour's carry for the current row
+    int cbuf[16], fbuf[16];     // stripes: the right neighbour's carries and first columns of rows
+                                // [pf_lo, pf_hi), read in one batch while it is ahead (thread 0)
 };
 static_assert(XTED_WARPS == 8, "carry combination reads the warp minima as two int4");
 
@@ -632,9 +638,12 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                            int32_t *ring, int32_t *cache, int32_t *cnode, int s, int K, int X, int R,
                            const int32_t *expmap, int32_t *prog, int32_t *CR, int32_t *FC, int32_t *E) {
     constexpr int G = XTED_WARPS, SW = XTED_CTA_THREADS * W;  // stripe width: W columns per thread
-    constexpr int GROW = 256 * G + 8 * G;
-    constexpr int GSLOT = GROW + 8;
-    constexpr int PF = XTED_PREFETCH;
+    constexpr int GROW = 256 * G + 8 * G;  // padded row of the stack cache
+    // the ring holds stripe rows only (SW columns): narrow stripes keep more
+    // rows in flight in the same shared memory (8 at 512 columns, 4 at 1,024)
+    constexpr int SROW = SW + SW / 32, SSLOT = SROW + 8;
+    constexpr int PF = 8 * SSLOT <= RING_INTS ? 8 : 4 * SSLOT <= RING_INTS ? 4 : 2;
+    static_assert(PF * SSLOT <= RING_INTS, "stripe ring");
     const int gtid = threadIdx.x, lane = gtid & 31, warp = gtid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
@@ -681,10 +690,20 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const int2 *rows = P.rowinfo + pr.row_base;
     volatile int32_t *prog_right = prog + s + 1;
     int tflat = 0;
-    // thread 0: the right neighbour's carry and first column of the current
-    // row, loaded at the row's start when that stripe is already past it
-    int cin_pf = XTED_INF, fc_pf = 0;
-    bool have_pf = false;
+    // thread 0: the right neighbour's carries and first columns, read in
+    // batches of up to 16 rows once that stripe is past them (one L2 round
+    // trip per batch instead of an acquire and two dependent loads per row)
+    int pf_lo = 0, pf_hi = 0, fc_pf = 0;
+    auto refill = [&](int avail) {
+        const int nb = min(min(avail - tflat, 16), R - tflat);
+        const int32_t *cr = CR + (int64_t)(s + 1) * R + tflat, *fc = FC + (int64_t)(s + 1) * R + tflat;
+        for (int q = 0; q < nb; q++) {
+            S.cbuf[q] = __ldcg(cr + q);
+            S.fbuf[q] = __ldcg(fc + q);
+        }
+        pf_lo = tflat;
+        pf_hi = tflat + nb;
+    };
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = __ldg(&P.krd[kr]);
         const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
@@ -700,7 +719,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
             if (r >= i0)
-                issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT, SROW, gtid, 32 * G,
                              gtid == 0);
             cp_async_commit();
         }
@@ -710,17 +729,16 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             {
                 const int r = i - (PF - 1);
                 if (r >= i0)
-                    issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                    issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT, SROW, gtid, 32 * G,
                              gtid == 0);
                 cp_async_commit();
             }
-            if (gtid == 0 && right && ld_acquire((const int32_t *)prog_right) >= tflat + 1) {
-                cin_pf = __ldcg(CR + (int64_t)(s + 1) * R + tflat);
-                fc_pf = __ldcg(FC + (int64_t)(s + 1) * R + tflat);
-                have_pf = true;
+            if (gtid == 0 && right && tflat >= pf_hi) {
+                const int avail = ld_acquire((const int32_t *)prog_right);
+                if (avail > tflat) refill(avail);
             }
-            const int32_t *slot = ring + (i & (PF - 1)) * GSLOT;
-            const int2 ri = *(const int2 *)(slot + GROW);
+            const int32_t *slot = ring + (i & (PF - 1)) * SSLOT;
+            const int2 ri = *(const int2 *)(slot + SROW);
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = (imax - i) * KC.del;
@@ -753,12 +771,16 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
             if (gtid == 0) {
-                if (right && !have_pf && wait_progress(P, prog_right, tflat + 1)) {
-                    cin_pf = __ldcg(CR + (int64_t)(s + 1) * R + tflat);
-                    fc_pf = __ldcg(FC + (int64_t)(s + 1) * R + tflat);
+                int cin = XTED_INF;
+                if (right) {
+                    if (tflat >= pf_hi && wait_progress(P, prog_right, tflat + 1))
+                        refill(ld_acquire((const int32_t *)prog_right));
+                    if (tflat < pf_hi) {
+                        cin = S.cbuf[tflat - pf_lo];
+                        fc_pf = S.fbuf[tflat - pf_lo];
+                    }
                 }
-                S.cin = right ? cin_pf : XTED_INF;
-                have_pf = false;
+                S.cin = cin;
             }
             __syncthreads();
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
@@ -822,10 +844,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             if (gtid == 0 && right) S.first[G] = fc_pf;
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
             __syncthreads();          // ... and everyone's, the record and the stack push; this row's outputs
-            if (gtid == 0 && left) {  // one fence after the barrier orders the whole block's outputs
-                __threadfence();
-                ((volatile int32_t *)prog)[s] = tflat + 1;
-            }
+            if (gtid == 0 && left)  // one release after the barrier orders the whole block's outputs
+                st_release(prog + s, tflat + 1);
         }
     }
     cp_async_wait<0>();
