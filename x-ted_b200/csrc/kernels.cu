@@ -1403,37 +1403,52 @@ __device__ bool gang_barrier(const XKernelParams &P, int *s_phase, int *s_ok) {
     return *s_ok != 0;
 }
 
-// One striped unit, run by every gang block (all threads).
+// One round of striped units, run by every gang block (all threads): block 0
+// takes the unit at the gang ring's head and, while they fit the gang's
+// blocks and buffer, the units queued behind it (independent tables, all
+// ready), lays each out in its own part of the gang buffer and gives it a
+// range of consecutive gang blocks; every block then runs its stripe of its
+// unit. Several narrow tables of one level then run side by side instead of
+// one after another.
 template <bool UC>
 __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S, int32_t *ring, int32_t *cache,
                          int32_t *cnode, int *s_g) {
-    // s_g: [0] phase, [1] ok, [2] task, [3] entry, [4] stripes, [5] exports, [6] feasible, [7] columns per thread
+    // s_g: [0] phase, [1] ok, [2] units in the round, [3..7] scratch, then
+    // XTED_GANG_UNITS descriptors of 8 ints: task, entry, stripes, exports,
+    // feasible, columns per thread, first block, buffer offset
+    int *desc = s_g + 8;
     const int tid = threadIdx.x, b = blockIdx.x;
     volatile int32_t *g = P.gang_ctl;
     if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // A: every gang block is here
     if (b == 0) {
-        if (tid == 0) {
-            const int hd = g[XTED_GCTL_HEAD];
-            volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (hd & (XTED_GANG_RING - 1));
-            const uint64_t t0 = global_ns();
-            bool ok = false;
-            for (long it = 0; it < (1L << 26); it++) {
-                if (slot[0] == hd + 1) {
-                    ok = true;
-                    break;
+        int nunits = 0, blocks_used = 0;
+        int64_t buf_used = 0;
+        for (int ui = 0; ui < XTED_GANG_UNITS; ui++) {
+            if (tid == 0) {
+                const int hd = g[XTED_GCTL_HEAD] + ui;
+                volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (hd & (XTED_GANG_RING - 1));
+                bool ok = false;
+                if (ui == 0) {  // the unit that called the gang: wait until its slot is written
+                    const uint64_t t0 = global_ns();
+                    for (long it = 0; it < (1L << 26); it++) {
+                        if (slot[0] == hd + 1) {
+                            ok = true;
+                            break;
+                        }
+                        if (global_ns() - t0 > P.timeout_ns) break;
+                        __nanosleep(32);
+                    }
+                    if (!ok) set_error(P, XTED_ETIMEOUT, 12, hd, 0);
+                } else {  // units behind it only if already queued
+                    ok = g[XTED_GCTL_TAIL] - hd > 0 && slot[0] == hd + 1;
                 }
-                if (global_ns() - t0 > P.timeout_ns) break;
-                __nanosleep(32);
+                __threadfence();
+                s_g[3] = ok ? slot[1] : -1;
+                s_g[4] = ok ? slot[2] : -1;
             }
-            if (!ok) set_error(P, XTED_ETIMEOUT, 12, hd, 0);
-            __threadfence();
-            s_g[2] = ok ? slot[1] : -1;
-            s_g[3] = ok ? slot[2] : -1;
-        }
-        __syncthreads();
-        const int t = s_g[2];
-        int K = 0, X = 0, feasible = 0, SWd = XTED_STRIPE;
-        if (t >= 0) {
+            __syncthreads();
+            const int t = s_g[3];
+            if (t < 0) break;
             const XTask T = P.tasks[t];
             const XUnit u = P.units[T.unit_lo];
             const XChunk ch = P.chunks[u.chunk];
@@ -1442,10 +1457,11 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
             // the narrowest stripes (at least XTED_STRIPE_MIN_W columns per
             // thread) that the gang's blocks cover: more stripes run a
             // table's rows in parallel, each row passed right to left
-            SWd = XTED_CTA_THREADS * XTED_STRIPE_MIN_W;
+            int SWd = XTED_CTA_THREADS * XTED_STRIPE_MIN_W;
             while (SWd < XTED_STRIPE && (w + SWd - 1) / SWd > P.gang_blocks) SWd *= 2;
-            K = (w + SWd - 1) / SWd;
-            int32_t *expmap = P.gang_buf;
+            const int K = (w + SWd - 1) / SWd;
+            if (ui > 0 && blocks_used + K > P.gang_blocks) break;  // the round is full
+            int32_t *expmap = P.gang_buf + buf_used;
             // mark the far columns that cross a stripe boundary, then number them
             for (int c = tid; c < w; c += XTED_CTA_THREADS) expmap[c] = 0;
             __syncthreads();
@@ -1477,64 +1493,84 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
                 expmap[c] = m ? before : -1;
                 before += m;
             }
-            X = total;
+            const int X = total;
             const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
-            const int64_t need = wal + XTED_GANG_MAX + 2 * (int64_t)K * R + (int64_t)R * X;
-            feasible = K <= P.gang_blocks && need <= P.gang_cap;
-            if (tid < XTED_GANG_MAX) P.gang_buf[wal + tid] = 0;  // progress words
+            const int64_t need = (wal + XTED_GANG_MAX + 2 * (int64_t)K * R + (int64_t)R * X + 31) & ~(int64_t)31;
+            const bool fits = buf_used + need <= P.gang_cap;
+            if (ui > 0 && !fits) break;  // the buffer is full: the next round takes it
+            const int feasible = K <= P.gang_blocks && fits;
+            if (feasible && tid < XTED_GANG_MAX) expmap[wal + tid] = 0;  // progress words
+            if (tid == 0) {
+                int *d = desc + 8 * ui;
+                d[0] = t;
+                d[1] = s_g[4];
+                d[2] = K;
+                d[3] = X;
+                d[4] = feasible;
+                d[5] = SWd / XTED_CTA_THREADS;
+                d[6] = blocks_used;
+                d[7] = (int)(buf_used >> 5);  // in units of 32 ints
+            }
+            blocks_used += feasible ? K : 1;  // an infeasible unit runs alone on its first block
+            if (feasible) buf_used += need;
+            nunits++;
+            __syncthreads();
         }
         __threadfence();
         __syncthreads();
         if (tid == 0) {
-            g[XTED_GCTL_DESC + 0] = t;
-            g[XTED_GCTL_DESC + 1] = s_g[3];
-            g[XTED_GCTL_DESC + 2] = K;
-            g[XTED_GCTL_DESC + 3] = X;
-            g[XTED_GCTL_DESC + 4] = feasible;
-            g[XTED_GCTL_DESC + 5] = SWd / XTED_CTA_THREADS;
+            g[XTED_GCTL_DESC] = nunits;
+            for (int q = 0; q < 8 * nunits; q++) g[XTED_GCTL_UDESC + q] = desc[q];
             __threadfence();
         }
     }
     if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // B: the layout is ready
     if (tid == 0) {
-        for (int q = 0; q < 6; q++) s_g[2 + q] = g[XTED_GCTL_DESC + q];
+        s_g[2] = g[XTED_GCTL_DESC];
+        for (int q = 0; q < 8 * s_g[2]; q++) desc[q] = g[XTED_GCTL_UDESC + q];
     }
     __syncthreads();
-    const int t = s_g[2], e = s_g[3], K = s_g[4], X = s_g[5], feasible = s_g[6], SWW = s_g[7];
-    if (t >= 0) {
+    const int nunits = s_g[2];
+    for (int ui = 0; ui < nunits; ui++) {
+        const int *d = desc + 8 * ui;
+        const int t = d[0], K = d[2], X = d[3], feasible = d[4], SWW = d[5], base = d[6];
+        if (b < base || b >= base + (feasible ? K : 1)) continue;
         __threadfence();  // acquire: the unit's inputs (complete before it was published) and the layout
         const XTask T = P.tasks[t];
         const XUnit u = P.units[T.unit_lo];
         const XPair pr = P.pairs[T.pair];
-        if (P.trace && b == 0 && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
+        if (P.trace && b == base && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
         if (feasible) {
-            if (b < K) {
-                const int w = P.chunks[u.chunk].width, R = P.runs[u.run].rows;
-                const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
-                int32_t *prog = P.gang_buf + wal;
-                int32_t *CR = prog + XTED_GANG_MAX;
-                int32_t *FC = CR + (int64_t)K * R;
-                int32_t *E = FC + (int64_t)K * R;
-                if (SWW == 2)
-                    run_stripe<2, UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
-                else if (SWW == 4)
-                    run_stripe<4, UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
-                else
-                    run_stripe<8, UC>(P, pr, u, scratch, S, ring, cache, cnode, b, K, X, R, P.gang_buf, prog, CR, FC, E);
-            }
-        } else if (b == 0) {
+            const int w = P.chunks[u.chunk].width, R = P.runs[u.run].rows;
+            const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
+            int32_t *expmap = P.gang_buf + ((int64_t)d[7] << 5);
+            int32_t *prog = expmap + wal;
+            int32_t *CR = prog + XTED_GANG_MAX;
+            int32_t *FC = CR + (int64_t)K * R;
+            int32_t *E = FC + (int64_t)K * R;
+            const int st = b - base;
+            if (SWW == 2)
+                run_stripe<2, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
+            else if (SWW == 4)
+                run_stripe<4, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
+            else
+                run_stripe<8, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
+        } else {
             dispatch_wide<UC>(P, pr, u, scratch, S, ring, cache, cnode);  // too wide or too many exports: one block
         }
         __threadfence();
     }
-    if (b == 0 && tid == 0) {  // the ring slot is consumed before anyone looks for the next unit
-        g[XTED_GCTL_HEAD] = g[XTED_GCTL_HEAD] + 1;
+    if (b == 0 && tid == 0) {  // the round's ring slots are consumed before anyone looks for the next unit
+        g[XTED_GCTL_HEAD] = g[XTED_GCTL_HEAD] + nunits;
         __threadfence();
     }
     if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // C: every stripe is done
-    if (b == 0 && tid == 0 && t >= 0) {
-        complete_task(P, e, P.tasks[t].pair);
-        if (P.trace) trace_task_end(P, t);
+    if (b == 0 && tid == 0) {
+        for (int ui = 0; ui < nunits; ui++) {
+            const int t = desc[8 * ui];
+            complete_task(P, desc[8 * ui + 1], P.tasks[t].pair);
+            if (P.trace) trace_task_end(P, t);
+        }
     }
     __syncthreads();
 }
@@ -1570,7 +1606,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
     __shared__ int s_next, s_k[2];
     __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch, s_chain;
     __shared__ int s_role;  // XTED_KIND_* the block last claimed: the kind it prefers when idle
-    __shared__ int s_gang[8];  // gang protocol: barrier phase, status, descriptor
+    __shared__ int s_gang[8 + 8 * XTED_GANG_UNITS];  // gang protocol: barrier phase, status, unit descriptors
     __shared__ FlowSlot s_fs[FLOW_SLOTS];
     // narrow units parked between two keyroot tables while the block ran a
     // group task: x flow slot, y unit, z pair, w next keyroot

@@ -92,18 +92,21 @@ struct XUnit {
 #define XTED_GANG_RING 256
 #define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
 // Units under XTED_GANG_BIG_CELLS go to the gang only while fewer than
-// XTED_GANG_SMALL_QUEUE units wait for it (the gang runs one unit at a time;
-// when many are ready, one block each in parallel is faster); bigger ones
-// always queue.
+// XTED_GANG_SMALL_QUEUE units wait for it (a gang round runs at most
+// XTED_GANG_UNITS units side by side; when many more are ready, one block
+// each in parallel is faster); bigger ones always queue.
 #define XTED_GANG_BIG_CELLS ((int64_t)1 << 24)
-#define XTED_GANG_SMALL_QUEUE 4
-// gang control words: ring tail, ring head, barrier count, descriptor, then
-// the ring (XTED_GANG_RING slots of 4 ints: tag, task, entry, 0)
+#define XTED_GANG_SMALL_QUEUE XTED_GANG_UNITS
+// gang control words: ring tail, ring head, barrier count, the round's unit
+// count and descriptors, then the ring (XTED_GANG_RING slots of 4 ints: tag,
+// task, entry, 0)
 #define XTED_GCTL_TAIL 0
 #define XTED_GCTL_HEAD 1
 #define XTED_GCTL_BAR 2
-#define XTED_GCTL_DESC 4   // task, entry, stripes, exports, feasible, columns per thread (6 ints)
-#define XTED_GCTL_RING 16
+#define XTED_GCTL_DESC 4   // units in the current round
+#define XTED_GANG_UNITS 8  // striped units one gang round may run side by side
+#define XTED_GCTL_UDESC 8  // their descriptors, 8 ints each
+#define XTED_GCTL_RING (XTED_GCTL_UDESC + 8 * XTED_GANG_UNITS)
 #define XTED_GCTL_INTS (XTED_GCTL_RING + 4 * XTED_GANG_RING)
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
 #define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
