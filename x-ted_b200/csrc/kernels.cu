@@ -1549,7 +1549,9 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
             int32_t *FC = CR + (int64_t)K * R;
             int32_t *E = FC + (int64_t)K * R;
             const int st = b - base;
-            if (SWW == 2)
+            if (SWW == 1)
+                run_stripe<1, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
+            else if (SWW == 2)
                 run_stripe<2, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
             else if (SWW == 4)
                 run_stripe<4, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);

@@ -88,7 +88,7 @@ struct XUnit {
 // to left through the gang buffer.
 #define XTED_STRIPE 2048        // widest stripe (8 columns per thread)
 #define XTED_STRIPE_MIN_W 2     // narrowest stripe: 2 columns per thread (512 columns)
-#define XTED_GANG_MAX 64
+#define XTED_GANG_MAX 128
 #define XTED_GANG_RING 256
 #define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
 // Units under XTED_GANG_BIG_CELLS go to the gang only while fewer than
@@ -104,7 +104,7 @@ struct XUnit {
 #define XTED_GCTL_HEAD 1
 #define XTED_GCTL_BAR 2
 #define XTED_GCTL_DESC 4   // units in the current round
-#define XTED_GANG_UNITS 8  // striped units one gang round may run side by side
+#define XTED_GANG_UNITS 16  // striped units one gang round may run side by side
 #define XTED_GCTL_UDESC 8  // their descriptors, 8 ints each
 #define XTED_GCTL_RING (XTED_GCTL_UDESC + 8 * XTED_GANG_UNITS)
 #define XTED_GCTL_INTS (XTED_GCTL_RING + 4 * XTED_GANG_RING)
