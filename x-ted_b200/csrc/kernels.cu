@@ -126,17 +126,17 @@ __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &p
     const int2 *nodes = P.rowinfo + pr.col_base;
     int s = ch.k_lo, j = 0, j0 = 0, je = 0;
     if (c0 < ch.width) {
-        const int32_t pos0 = __ldg(&P.cumw[ch.k_lo]) + c0;
+        const int32_t pos0 = P.cumw[ch.k_lo] + c0;
         int lo = ch.k_lo, hi = ch.k_lo + ch.nseg - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(&P.cumw[mid]) <= pos0) lo = mid;
+            if (P.cumw[mid] <= pos0) lo = mid;
             else hi = mid - 1;
         }
         s = lo;
-        j0 = __ldg(&P.krd[s]);
-        je = (__ldg(&nodes[j0]).y & XTED_ROW_ORL_MASK) + 1;
-        j = j0 + (pos0 - __ldg(&P.cumw[s]));
+        j0 = P.krd[s];
+        je = (nodes[j0].y & XTED_ROW_ORL_MASK) + 1;
+        j = j0 + (pos0 - P.cumw[s]);
     }
 #pragma unroll
     for (int k = 0; k < W; k++) {
@@ -144,11 +144,11 @@ __device__ __forceinline__ void load_cols(const XKernelParams &P, const XPair &p
         if (c < ch.width) {
             if (j >= je) {
                 s++;
-                j0 = __ldg(&P.krd[s]);
-                je = (__ldg(&nodes[j0]).y & XTED_ROW_ORL_MASK) + 1;
+                j0 = P.krd[s];
+                je = (nodes[j0].y & XTED_ROW_ORL_MASK) + 1;
                 j = j0;
             }
-            const int2 nd = __ldg(&nodes[j]);
+            const int2 nd = nodes[j];
             const int foff = (nd.y & XTED_ROW_ORL_MASK) + 1 - j;
             C.node[k] = j;
             C.lab[k] = nd.x;
@@ -345,8 +345,8 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
                 return kr;
             }
         }
-        const int i0 = __ldg(&P.krd[kr]);
-        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        const int i0 = P.krd[kr];
+        const int imax = (rows[i0].y & XTED_ROW_ORL_MASK) + 1;
         int prev[W];
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k] * K.ins;
@@ -495,8 +495,8 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
     const int2 *rows = P.rowinfo + pr.row_base;
 
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
-        const int i0 = __ldg(&P.krd[kr]);
-        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        const int i0 = P.krd[kr];
+        const int imax = (rows[i0].y & XTED_ROW_ORL_MASK) + 1;
         int prev[W];
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k] * K.ins;
@@ -705,8 +705,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
         pf_hi = tflat + nb;
     };
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
-        const int i0 = __ldg(&P.krd[kr]);
-        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        const int i0 = P.krd[kr];
+        const int imax = (rows[i0].y & XTED_ROW_ORL_MASK) + 1;
         const int tbase = tflat;
         int prev[W];
 #pragma unroll
@@ -901,12 +901,12 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     };
     {   // derive this thread's columns once per unit (single segment: keyroot k_lo)
         const int2 *nodes = P.rowinfo + pr.col_base;
-        const int j0 = __ldg(&P.krd[ch.k_lo]);
+        const int j0 = P.krd[ch.k_lo];
         const int je = j0 + width;
         for (int k = 0; k < nk; k++) {
             const int c = c0 + k;
             const int j = j0 + c;
-            const int2 nd = __ldg(&nodes[j]);
+            const int2 nd = nodes[j];
             uint32_t z = (uint32_t)((nd.y & XTED_ROW_ORL_MASK) + 1 - j);
             if (j > j0 && (nd.y & XTED_ROW_PREVLEAF)) z |= XTED_COL_FARCOL;
             cols[(int64_t)k * XTED_CTA_THREADS + tid] = make_int4(j, nd.x, (int)z, je - j);
@@ -919,7 +919,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     const int stack_rows = P.stack_rows;
     // the next thread's first column (the diagonal of this thread's last one)
     const int64_t next_ix = c1 < width ? (int64_t)tid + 1 : Wp;
-    const int j0s = __ldg(&P.krd[ch.k_lo]);  // the segment's first node: row slice drow[j0s, j0s + width)
+    const int j0s = P.krd[ch.k_lo];  // the segment's first node: row slice drow[j0s, j0s + width)
     constexpr int kStageInts = DP_SMEM_BYTES / 4;
     const bool staged = width <= kStageInts, dbl = 2 * width <= kStageInts;
     auto stage_row = [&](int r, int32_t *dst) {
@@ -929,8 +929,8 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
     };
     // single segment: key = column index
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
-        const int i0 = __ldg(&P.krd[kr]);
-        const int imax = (__ldg(&rows[i0]).y & XTED_ROW_ORL_MASK) + 1;
+        const int i0 = P.krd[kr];
+        const int imax = (rows[i0].y & XTED_ROW_ORL_MASK) + 1;
         for (int k = 0; k < nk; k++)
             prevb[(int64_t)k * XTED_CTA_THREADS + tid] = cols[(int64_t)k * XTED_CTA_THREADS + tid].w * K.ins;
         if (tid == 0) prevb[Wp] = 0;
@@ -955,7 +955,7 @@ __device__ void run_wide_big(const XKernelParams &P, const XPair &pr, const XUni
                 }
                 __syncthreads();  // every thread's copies of row i have landed
             }
-            const int2 ri = __ldg(&rows[i]);
+            const int2 ri = rows[i];
             const int ro = ri.y & XTED_ROW_ORL_MASK;
             const bool trow = ro == imax - 1;
             const int bord = (imax - i) * K.del;
@@ -1050,9 +1050,15 @@ __device__ void dispatch_half(const XKernelParams &P, const XPair &pr, const XUn
 // non-empty bucket. An entry is only published after every task of the
 // previous level of its pair has finished, so claimed tasks never wait.
 // ---------------------------------------------------------------------------
-// Publishes entry e (or, past levels without tasks, the first later level
-// that has some) into its bucket's ring. Returns false when the pair has no
-// level left, i.e. the pair is finished.
+// A field of a ready-queue entry, read through L2: P.entries[e].f. A serving
+// session hands the entry ids of a finished query (or of its first round) to
+// the next plan while the kernel runs, and a claimer reads the entry straight
+// after the ring slot that names it, before any acquire: a copy of the old
+// entry left in this SM's L1 would give the wrong task range and move the
+// ring's head past a live entry. Only the fields a caller uses are loaded.
+__device__ __forceinline__ int32_t entry_ld(const int32_t &f) { return __ldcg(&f); }
+
+// Appends entry e at the tail of ring g.
 __device__ __forceinline__ void ring_push(const XKernelParams &P, int g, int e) {
     const unsigned pos = (unsigned)atomicAdd(&P.rq_ctl[2 * g + 1], 1);
     const unsigned head = *(volatile unsigned *)&P.rq_ctl[2 * g];
@@ -1070,13 +1076,15 @@ __device__ __forceinline__ void ring_push(const XKernelParams &P, int g, int e) 
 // left, i.e. the pair is finished.
 __device__ bool rq_publish(const XKernelParams &P, int e) {
     while (e >= 0) {
-        const XEntry X = P.entries[e];
-        if (X.ntasks > 0) {
-            if (X.nnarrow > 0) ring_push(P, XTED_KIND_NARROW * XTED_BUCKETS + X.bucket, e);
-            if (X.ntasks > X.nnarrow) ring_push(P, XTED_KIND_GROUP * XTED_BUCKETS + X.bucket, e);
+        const XEntry &X = P.entries[e];
+        const int nt = entry_ld(X.ntasks);
+        if (nt > 0) {
+            const int nn = entry_ld(X.nnarrow), b = entry_ld(X.bucket);
+            if (nn > 0) ring_push(P, XTED_KIND_NARROW * XTED_BUCKETS + b, e);
+            if (nt > nn) ring_push(P, XTED_KIND_GROUP * XTED_BUCKETS + b, e);
             return true;
         }
-        e = X.next;  // a level without tasks: go on to the next one
+        e = entry_ld(X.next);  // a level without tasks: go on to the next one
     }
     return false;
 }
@@ -1191,15 +1199,16 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
                         if ((int)((unsigned)ctl[2 * g + 1] - h) <= 0) break;  // empty
                         const int e = rq_entry(P, g, h);
                         if (e < 0) break;  // the head position is reserved but not yet written
-                        const XEntry X = P.entries[e];
-                        const int lim = kind == XTED_KIND_NARROW ? X.nnarrow : X.ntasks - X.nnarrow;
+                        const XEntry &X = P.entries[e];
+                        const int nn = entry_ld(X.nnarrow);
+                        const int lim = kind == XTED_KIND_NARROW ? nn : entry_ld(X.ntasks) - nn;
                         if (state[XTED_ESTATE * e + kind] < lim) {
                             const int k = atomicAdd(&P.entry_state[XTED_ESTATE * e + kind], 1);
                             if (k < lim) {
                                 __threadfence();  // acquire: the level's inputs are visible from here on
                                 if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
                                 e_out = e;
-                                res = X.task_off + (kind == XTED_KIND_NARROW ? 0 : X.nnarrow) + k;
+                                res = entry_ld(X.task_off) + (kind == XTED_KIND_NARROW ? 0 : nn) + k;
                                 break;
                             }
                         }
@@ -1295,11 +1304,11 @@ __device__ void finish_served_pair(const XKernelParams &P, int pair, int bucket)
 
 // After a task (all its writes fenced and the block synchronised).
 __device__ void complete_task(const XKernelParams &P, int e, int pair) {
-    const XEntry X = P.entries[e];
+    const XEntry &X = P.entries[e];
     const int done = atomicAdd(&P.entry_state[XTED_ESTATE * e + 2], 1) + 1;
-    if (done == X.ntasks) {
+    if (done == entry_ld(X.ntasks)) {
         __threadfence();  // acquire the level's other tasks, release to the next level's claimers
-        if (!rq_publish(P, X.next) && P.serve) finish_served_pair(P, pair, X.bucket);
+        if (!rq_publish(P, entry_ld(X.next)) && P.serve) finish_served_pair(P, pair, entry_ld(X.bucket));
     }
     __threadfence();
     atomicAdd(P.done_total, 1);
@@ -1319,7 +1328,7 @@ __device__ void publish_record(const XKernelParams &P, int r, int lane) {
     __threadfence();
     for (int p = lo + lane; p < lo + n; p += 32) {
         const int e = __ldcg(&P.first[p]);
-        if (e >= 0 && p != P.hold_pair && !rq_publish(P, e)) finish_served_pair(P, p, P.entries[e].bucket);
+        if (e >= 0 && p != P.hold_pair && !rq_publish(P, e)) finish_served_pair(P, p, entry_ld(P.entries[e].bucket));
     }
     __syncwarp();
 }
@@ -1467,10 +1476,10 @@ __device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S
             __syncthreads();
             {
                 const int2 *nodes = P.rowinfo + pr.col_base;
-                const int j0 = __ldg(&P.krd[ch.k_lo]);
+                const int j0 = P.krd[ch.k_lo];
                 for (int c = tid; c < w; c += XTED_CTA_THREADS) {
                     const int j = j0 + c;
-                    const int f = c + ((__ldg(&nodes[j]).y & XTED_ROW_ORL_MASK) + 1 - j);
+                    const int f = c + ((nodes[j].y & XTED_ROW_ORL_MASK) + 1 - j);
                     if (f < w && f / SWd != c / SWd) expmap[f] = 1;
                 }
             }

@@ -6,7 +6,7 @@
 // 304-387). Here the raw trees go up once and everything else is built on the
 // device, one thread per tree / oriented tree / pair / (pair, level):
 //
-//   k_tree_basic   sizes, depths, parents, keyroot-size sums (both decompositions)
+//   k_tree_basic_warp  sizes, depths, parents, keyroot-size sums (both decompositions), a warp per tree
 //   k_orient       per orientation: node records, kdepth, keyroots by depth,
 //                  column-list positions, row runs, column chunks
 //   k_pair_setup   decomposition choice, level count
@@ -29,9 +29,90 @@ namespace xted {
 
 namespace {
 
-__global__ void k_tree_basic(PlanPools P, DTree *trees) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < P.ntrees) tree_basic(P, t, trees);
+// The outputs of tree_basic (plan_core.h: sizes, depths and parents of every
+// node, the keyroot-size sums of both decompositions) with a warp per tree
+// and the work spread over its lanes instead of one thread walking the tree:
+// parents straight from the child lists; each node's orl (rightmost leaf) by
+// pointer jumping along last children, its size orl - v + 1; depths as a
+// prefix sum of +1 at every node and -1 just past its subtree (u is an
+// ancestor of v exactly when u <= v <= orl(u)); the sums as lane sums. One
+// thread per tree waited on a dependent global load per node visited.
+__global__ void k_tree_basic_warp(PlanPools P, DTree *trees_out) {
+    const int lane = threadIdx.x & 31;
+    const int t = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (t >= P.ntrees) return;  // whole warps: t is the same in every lane
+    DTree T = P.trees[t];
+    const int n = T.n;
+    const int32_t *off = P.raw + T.raw + n, *idx = P.raw + T.raw + 2 * n + 1;
+    int32_t *size = P.size + T.nbase, *depth = P.depth + T.nbase, *par = P.parent + T.nbase;
+    int32_t *jump = P.opar + 2 * (int64_t)T.nbase;  // scratch: this tree's orientation pool, unused until k_orient
+    T.S[0] = T.S[1] = 0;
+    if (n > 0) {
+        for (int v = lane; v < n; v += 32) {
+            const int32_t lo = off[v], hi = off[v + 1];
+            for (int32_t e = lo; e < hi; e++) par[idx[e]] = v;
+            size[v] = hi > lo ? idx[hi - 1] : v;  // last child, or the node itself for a leaf
+        }
+        if (lane == 0) par[0] = -1;
+        __syncwarp();
+        int32_t *cur = size, *nxt = jump;
+        for (int round = 0; round < 32; round++) {
+            bool changed = false;
+            for (int v = lane; v < n; v += 32) {
+                const int32_t a = cur[v], b = cur[a];
+                nxt[v] = b;
+                changed |= b != a;
+            }
+            __syncwarp();
+            int32_t *tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+            if (!__any_sync(0xffffffffu, changed)) break;
+        }
+        // cur[v] = orl(v). Depth: +1 at every u, -1 at orl(u) + 1, then an inclusive prefix sum
+        for (int v = lane; v < n; v += 32) depth[v] = 0;
+        __syncwarp();
+        for (int u = lane; u < n; u += 32) {
+            atomicAdd(&depth[u], 1);
+            const int32_t o1 = cur[u] + 1;
+            if (o1 < n) atomicSub(&depth[o1], 1);
+        }
+        __syncwarp();
+        const int per = (n + 31) / 32, a0 = min(lane * per, n), a1 = min(a0 + per, n);
+        int32_t sum = 0;
+        for (int v = a0; v < a1; v++) sum += depth[v];
+        int32_t incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        int32_t run = incl - sum;
+        for (int v = a0; v < a1; v++) {
+            run += depth[v];
+            depth[v] = run - 1;
+        }
+        __syncwarp();
+        for (int v = lane; v < n; v += 32) size[v] = cur[v] - v + 1;
+        __syncwarp();
+        int64_t sr = 0, sl = 0;
+        for (int v = lane; v < n; v += 32) {
+            const int32_t lo = off[v], hi = off[v + 1];
+            for (int32_t e = lo; e < hi; e++) {
+                const int64_t z = size[idx[e]];
+                if (e != hi - 1) sr += z;
+                if (e != lo) sl += z;
+            }
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, d);
+            sl += __shfl_down_sync(0xffffffffu, sl, d);
+        }
+        T.S[0] = sr + size[0];
+        T.S[1] = sl + size[0];
+    }
+    if (lane == 0) trees_out[t] = T;
 }
 
 __global__ void k_orient(PlanPools P) {
@@ -338,7 +419,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
 
     const int BS = 128;
     cudaMemsetAsync(d_sum, 0, sizeof(Summary), s);
-    k_tree_basic<<<blocks_for(T, BS), BS, 0, s>>>(P, d_trees);
+    k_tree_basic_warp<<<blocks_for(32 * (int64_t)T, BS), BS, 0, s>>>(P, d_trees);
     k_orient<<<blocks_for(2 * (int64_t)T, BS), BS, 0, s>>>(P);
     k_pair_setup<<<blocks_for(npairs, BS), BS, 0, s>>>(d_trees, P.otrees, d_pt, c->opts.orientation, npairs,
                                                        d_pairs, d_L, d_cells);

@@ -31,6 +31,8 @@
 #include <chrono>
 #include <climits>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -538,6 +540,15 @@ bool step(ServeState *s, std::unique_lock<std::mutex> &lk) {
                 Slot &sl = s->slots[i];
                 if (!sl.busy || sl.gen == 0 || sl.rec < 0 || sl.rec >= consumed) continue;
                 if (((volatile int32_t *)s->h_flags)[i] == sl.gen) continue;  // done: step 1 takes it
+                if (std::getenv("XTED_SERVE_DEBUG")) {
+                    int32_t done = -1;
+                    cudaMemcpy(&done, s->d_slot + i, 4, cudaMemcpyDeviceToHost);
+                    std::fprintf(stderr,
+                                 "xted serve: launch %lld ended with slot %d unfinished: round %d gen %d rec %d "
+                                 "consumed %d posted %d need %d done %d flag %d\n",
+                                 (long long)s->launches, i, sl.round, sl.gen, sl.rec, consumed, s->posted,
+                                 sl.plan.need, done, ((volatile int32_t *)s->h_flags)[i]);
+                }
                 auto it = s->queries.find(sl.ticket);
                 if (it != s->queries.end()) it->second.state = XTED_ETIMEOUT;
                 s->error = XTED_ETIMEOUT;
