@@ -119,11 +119,15 @@ def test_planner_emulation_matches_oracle(tmp_path):
     obj = tmp_path / "xo.o"
     exe = tmp_path / "plan_emu"
     subprocess.run(["gcc", "-O2", "-c", os.path.join(REPO, "oracle", "xted_oracle.c"), "-o", str(obj)], check=True)
-    subprocess.run(["g++", "-O2", "-std=c++17", "-I/usr/local/cuda/include",
-                    os.path.join(REPO, "tests", "cpp", "plan_emu.cpp"), str(obj), "-o", str(exe), "-lpthread"],
-                   check=True)
-    for window in ("8", "2"):  # the kernels' shared stack window, and a tiny one that forces reloads
-        r = subprocess.run([str(exe), "100", "250", "99", window], capture_output=True, text=True, timeout=600)
+    # the second build makes runs of more than 30 rows "long" (single-unit
+    # narrow tasks), which the product reaches only on trees above 4,096 nodes
+    exe_long = tmp_path / "plan_emu_long"
+    for flags, out in (([], exe), (["-DXTED_LONG_RUN_ROWS=30"], exe_long)):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-I/usr/local/cuda/include", *flags,
+                        os.path.join(REPO, "tests", "cpp", "plan_emu.cpp"), str(obj), "-o", str(out), "-lpthread"],
+                       check=True)
+    for prog, window in ((exe, "8"), (exe, "2"), (exe_long, "8")):  # "2": a tiny stack window that forces reloads
+        r = subprocess.run([str(prog), "100", "250", "99", window], capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout + r.stderr
         assert r.stdout.startswith("ok")
 

@@ -621,6 +621,9 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 // columns on pushed rows, then its progress (rows done, flat over the unit's
 // keyroots). Waits are bounded by the launch's timeout.
 // ---------------------------------------------------------------------------
+#ifndef XTED_STRIPE_PUB
+#define XTED_STRIPE_PUB 4
+#endif
 __device__ __forceinline__ bool wait_progress(const XKernelParams &P, volatile int32_t *prog, int want) {
     const uint64_t t0 = global_ns();
     for (long it = 0; it < (1L << 26); it++) {
@@ -844,7 +847,9 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             if (gtid == 0 && right) S.first[G] = fc_pf;
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
             __syncthreads();          // ... and everyone's, the record and the stack push; this row's outputs
-            if (gtid == 0 && left)  // one release after the barrier orders the whole block's outputs
+            // one release after the barrier orders the whole block's outputs;
+            // published every XTED_STRIPE_PUB rows (and at the unit's end)
+            if (gtid == 0 && left && ((tflat + 1) % XTED_STRIPE_PUB == 0 || tflat + 1 == R))
                 st_release(prog + s, tflat + 1);
         }
     }

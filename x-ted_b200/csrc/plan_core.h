@@ -180,6 +180,16 @@ XT_HD inline int32_t level_bundle(int64_t nnarrow) {
     return (int32_t)b;
 }
 
+// Narrow units of a run longer than this many rows are tasks of one unit
+// each: a bundle of them would run its units a few at a time on one block's
+// warps (4 rounds for 32 units on 8 warps), while single-unit tasks spread
+// over the warps of several blocks. Such runs are the few big keyroots of
+// large trees, whose levels are short of parallel work.
+#ifndef XTED_LONG_RUN_ROWS
+#define XTED_LONG_RUN_ROWS 4096
+#endif
+XT_HD inline bool long_run_rows(int32_t rows) { return rows > XTED_LONG_RUN_ROWS; }
+
 // Builds oriented tree ot = 2 t + o: node records, keyroot depths, keyroots
 // grouped by depth, column-list positions, row runs and column chunks.
 XT_HD inline void orient_tree(const PlanPools &P, int ot) {
@@ -379,23 +389,35 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
-    int64_t wide = 0, narrow = 0, half = 0;
+    int64_t wide = 0, narrow = 0, half = 0, nlong = 0;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
-    int32_t small_max[64];  // longest non-big run per depth (the first 64 depths; more use maxrows)
+    int32_t small_max[64];  // longest bundled run per depth (the first 64 depths; more use maxrows)
+    int32_t long_max[64];   // longest run of single-unit narrow tasks per depth
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         const int64_t nr = ra.run_hi - ra.run_lo;
-        int64_t nbig = 0;
-        int32_t sm = 0;
+        int64_t nbig = 0, nl = 0;
+        int32_t sm = 0, lm = 0;
         if (cb.nnarrow > 0)
             for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
-                if (big_run(C, r)) nbig++;
-                else if (C.runs[r].rows > sm) sm = C.runs[r].rows;
+                const int32_t rows = C.runs[r].rows;
+                if (big_run(C, r)) {
+                    nbig++;
+                } else if (long_run_rows(rows)) {
+                    nl++;
+                    if (rows > lm) lm = rows;
+                } else if (rows > sm) {
+                    sm = rows;
+                }
             }
-        if (al - lo < 64) small_max[al - lo] = sm;
+        if (al - lo < 64) {
+            small_max[al - lo] = sm;
+            long_max[al - lo] = lm;
+        }
         wide += nr * cb.nwide + nbig * cb.nnarrow;
         half += nr * cb.nhalf;
         narrow += (nr - nbig) * cb.nnarrow;
+        nlong += nl * cb.nnarrow;
     }
     const int32_t bundle = level_bundle(narrow);
     const int rounds = (bundle + XTED_WARPS - 1) / XTED_WARPS;  // units a warp runs in one task
@@ -408,7 +430,10 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
         double e = 0.0;
         if (cb.nnarrow > 0) {
             const int32_t sm = al - lo < 64 ? small_max[al - lo] : ra.maxrows;
+            const int32_t lm = al - lo < 64 ? long_max[al - lo] : ra.maxrows;
             e = rounds * sm * row_cost_est(false, cb.maxw_n);
+            const double el = lm * row_cost_est(false, cb.maxw_n);
+            if (el > e) e = el;
             if (C.wide_rows >= 0 && ra.maxrows > C.wide_rows) {
                 const double eb = ra.maxrows * row_cost_est(true, cb.maxw_n);
                 if (eb > e) e = eb;
@@ -427,7 +452,7 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     E.nwide = (int32_t)wide;
     E.nnarrow = (int32_t)narrow;
     E.nhalf = (int32_t)half;
-    E.nntasks = (int32_t)((narrow + bundle - 1) / bundle);
+    E.nntasks = (int32_t)((narrow - nlong + bundle - 1) / bundle + nlong);
     E.ntasks = (int32_t)(wide + E.nntasks + (half + bundle_h - 1) / bundle_h);
     *est_out = est;
 }
@@ -462,7 +487,7 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
-            if (big_run(C, r)) continue;
+            if (big_run(C, r) || long_run_rows(C.runs[r].rows)) continue;
             for (int32_t c = cb.chunk_lo; c < cb.chunk_lo + cb.nnarrow; c++) {
                 if (bundle == 0) bundle_lo = u;
                 units[u++] = XUnit{r, c};
@@ -474,9 +499,23 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
         }
     }
     if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, (uint32_t)bundle, bundle_lo};
+    // Long runs, half-block and whole-block units are laid out from the row
+    // tree's deepest keyroots down (most rows first): claimers take a level's
+    // tasks of a kind in index order, so the longest units start first.
+    for (int al = hi; al >= lo; al--) {  // long runs: a narrow task per unit
+        const DDepth &ra = da[al], &cb = db[d - al];
+        for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            if (big_run(C, r) || !long_run_rows(C.runs[r].rows)) continue;
+            for (int32_t c = cb.chunk_lo; c < cb.chunk_lo + cb.nnarrow; c++) {
+                units[u] = XUnit{r, c};
+                tasks[t++] = XTask{E.pair, E.entry, 1u, u};
+                u++;
+            }
+        }
+    }
     const int32_t per_half = level_bundle_half(E.nhalf);
     bundle = 0;
-    for (int al = lo; al <= hi; al++) {
+    for (int al = hi; al >= lo; al--) {
         const DDepth &ra = da[al], &cb = db[d - al];
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
             for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nhalf; c++) {
@@ -494,7 +533,7 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
     if (bundle > 0)
         tasks[t++] = XTask{E.pair, E.entry, (bundle == 1 ? XTED_TASK_WIDE : XTED_TASK_HALF) | (uint32_t)bundle,
                            bundle_lo};
-    for (int al = lo; al <= hi; al++) {
+    for (int al = hi; al >= lo; al--) {
         const DDepth &ra = da[al], &cb = db[d - al];
         const int32_t cw_lo = cb.chunk_lo + cb.nnarrow + cb.nhalf, cw_hi = cw_lo + cb.nwide;
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
