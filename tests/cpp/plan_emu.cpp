@@ -38,10 +38,18 @@ struct HostPlan {
     std::vector<XEntry> entries;
     std::vector<XUnit> units;
     std::vector<XTask> tasks;
+    std::vector<XStripe> stripes;
     int stack_rows = 1;
 };
 
 static bool g_table = false;
+// striped units: built with -DXTED_STRIPE_MIN_WIDTH=<small>, wide units of
+// every size are planned as stripe tasks, whose layout the run checks
+#ifdef XTED_STRIPE_MIN_WIDTH
+static const bool g_stripes = true;
+#else
+static const bool g_stripes = false;
+#endif
 
 static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<std::vector<int32_t>> &O,
                  const std::vector<std::vector<int32_t>> &I, const std::vector<int> &nn,
@@ -122,6 +130,7 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     H.lv.resize((size_t)ent);
     LevelCtx C{H.ot.data(), H.depths.data(), H.runs.data(), H.chunks.data(), H.pairs.data(), narrow_width,
                wide_rows};
+    C.stripe_min_cells = g_stripes ? 1 : 0;
     std::vector<int64_t> chain((size_t)np, 0);
     int64_t chain_max = 0;
     for (int p = 0; p < np; p++) {
@@ -140,15 +149,19 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
         chain[(size_t)p] = acc;
         chain_max = std::max(chain_max, acc);
     }
-    int64_t toff = 0, uoff = 0;
+    int64_t toff = 0, uoff = 0, soff = 0, poff = 0;
     H.entries.resize(H.lv.size());
     for (size_t e = 0; e < H.lv.size(); e++) {
         DLevel &E = H.lv[e];
         E.task_off = (int32_t)toff;
         E.unit_off = (int32_t)uoff;
+        E.stripe_off = (int32_t)soff;
+        E.sprog_off = (int32_t)poff;
         E.entry = (int32_t)e;
         toff += E.ntasks;
         uoff += (int64_t)E.nwide + E.nnarrow + E.nhalf;
+        soff += E.nstriped;
+        poff += E.nstripes;
         XEntry &X = H.entries[e];
         X.task_off = E.task_off;
         X.ntasks = E.ntasks;
@@ -159,7 +172,18 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     }
     H.units.assign((size_t)uoff, XUnit{-1, -1});
     H.tasks.assign((size_t)toff, XTask{-1, -1, 0, -1});
-    for (auto &E : H.lv) level_fill(C, E, H.units.data(), H.tasks.data());
+    H.stripes.assign((size_t)soff + 1, XStripe{});
+    for (auto &E : H.lv) level_fill(C, E, H.units.data(), H.tasks.data(), H.stripes.data());
+    // stripes: progress words of consecutive striped units are consecutive
+    int64_t pcheck = 0;
+    for (int64_t i = 0; i < soff; i++) {
+        const XStripe &S = H.stripes[(size_t)i];
+        if (S.prog_off != pcheck || S.K != stripe_count(S.w) || S.unit < 0 || S.unit >= uoff)
+            FAIL("striped unit %lld: progress word %d (want %lld), %d stripes", (long long)i, S.prog_off,
+                 (long long)pcheck, S.K);
+        pcheck += S.K;
+    }
+    if (pcheck != poff) FAIL("progress words %lld, planned %lld", (long long)pcheck, (long long)poff);
 }
 
 static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int32_t> &lab,
@@ -255,9 +279,42 @@ int main(int argc, char **argv) {
             std::vector<int> order((size_t)X.ntasks);
             std::iota(order.begin(), order.end(), 0);
             std::shuffle(order.begin(), order.end(), g);
+            std::vector<int> stripe_seen;  // per striped unit of the entry: stripes seen (bit mask of the first 64)
             for (int k : order) {
                 const XTask &t = H.tasks[(size_t)(X.task_off + k)];
                 if (t.pair != E.pair || t.entry != e) FAIL("task of another entry in the range");
+                if (t.kind_n & XTED_TASK_STRIPED) {
+                    // stripe s of striped unit t.unit_lo: the unit's stripes are consecutive tasks,
+                    // rightmost first; the unit runs once, at its rightmost stripe
+                    const int si = t.unit_lo, s = (int)((t.kind_n >> XTED_STRIPE_SHIFT) & XTED_STRIPE_MASK);
+                    if (!(t.kind_n & XTED_TASK_WIDE) || (t.kind_n & 0xffff) != 1 || si < E.stripe_off ||
+                        si >= E.stripe_off + E.nstriped)
+                        FAIL("stripe task %d of entry %d: striped unit %d", k, e, si);
+                    const XStripe &S = H.stripes[(size_t)si];
+                    if (s >= S.K) FAIL("stripe %d of %d", s, S.K);
+                    const int first = X.task_off + k - (S.K - 1 - s);  // the task of stripe K - 1
+                    const XTask &t0 = H.tasks[(size_t)first];
+                    if (!(t0.kind_n & XTED_TASK_STRIPED) || t0.unit_lo != si ||
+                        (int)((t0.kind_n >> XTED_STRIPE_SHIFT) & XTED_STRIPE_MASK) != S.K - 1)
+                        FAIL("stripes of unit %d not consecutive from the rightmost", si);
+                    if (s != S.K - 1) continue;
+                    const XUnit &U = H.units[(size_t)S.unit];
+                    if (H.runs[(size_t)U.run].rows != S.R || H.chunks[(size_t)U.chunk].width != S.w)
+                        FAIL("striped unit %d: rows %d width %d", si, S.R, S.w);
+                    const DPair &q = H.pairs[(size_t)t.pair];
+                    XPair x;
+                    x.dt_off = q.dt_off;
+                    x.m = H.trees[(size_t)q.ta].n;
+                    x.n = H.trees[(size_t)q.tb].n;
+                    x.row_base = H.ot[2 * (size_t)q.ta + q.o].node_base;
+                    x.col_base = H.ot[2 * (size_t)q.tb + q.o].node_base;
+                    const emu::Pools EP{H.node.data(), H.krd.data(), H.cumw.data(), H.runs.data(), H.chunks.data(),
+                                        H.stack_rows};
+                    unit_seen[(size_t)S.unit]++;
+                    emu::run_unit(EP, x, U, dt, nw, true);
+                    stripes_checked++;
+                    continue;
+                }
                 const int nu = (int)(t.kind_n & 0xffff);
                 const bool full = (t.kind_n & XTED_TASK_WIDE) != 0, half = (t.kind_n & XTED_TASK_HALF) != 0;
                 // the narrow tasks of a level are the first X.nnarrow of its range (two claim rings)

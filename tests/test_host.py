@@ -120,13 +120,16 @@ def test_planner_emulation_matches_oracle(tmp_path):
     exe = tmp_path / "plan_emu"
     subprocess.run(["gcc", "-O2", "-c", os.path.join(REPO, "oracle", "xted_oracle.c"), "-o", str(obj)], check=True)
     # the second build makes runs of more than 30 rows "long" (single-unit
-    # narrow tasks), which the product reaches only on trees above 4,096 nodes
+    # narrow tasks), which the product reaches only on trees above 4,096 nodes;
+    # the third plans every whole-block unit wider than 40 columns as stripe
+    # tasks (the product: wider than 2,048), checking their layout
     exe_long = tmp_path / "plan_emu_long"
-    for flags, out in (([], exe), (["-DXTED_LONG_RUN_ROWS=30"], exe_long)):
+    exe_st = tmp_path / "plan_emu_stripes"
+    for flags, out in (([], exe), (["-DXTED_LONG_RUN_ROWS=30"], exe_long), (["-DXTED_STRIPE_MIN_WIDTH=40"], exe_st)):
         subprocess.run(["g++", "-O2", "-std=c++17", "-I/usr/local/cuda/include", *flags,
                         os.path.join(REPO, "tests", "cpp", "plan_emu.cpp"), str(obj), "-o", str(out), "-lpthread"],
                        check=True)
-    for prog, window in ((exe, "8"), (exe, "2"), (exe_long, "8")):  # "2": a tiny stack window that forces reloads
+    for prog, window in ((exe, "8"), (exe, "2"), (exe_long, "8"), (exe_st, "8")):  # "2": forces stack reloads
         r = subprocess.run([str(prog), "100", "250", "99", window], capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout + r.stderr
         assert r.stdout.startswith("ok")

@@ -128,19 +128,6 @@ int ctx_prepare(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npa
     K.error = cnt + 1;
     K.error_info = cnt + 2;
     K.timeout_ns = (uint64_t)(c->opts.wait_timeout_s * 1e9);
-    // Striped units: the gang blocks share one buffer (one striped unit at a
-    // time). Without it, or with stripes off, a striped unit runs on one block.
-    K.gang_blocks = 0;
-    K.gang_buf = nullptr;
-    K.gang_cap = 0;
-    if (max_wide > XTED_WIDE_REG_MAX && c->opts.stripe_min_cells >= 0 && c->grid >= 2) {
-        const int64_t cap = (int64_t)1 << 27;  // ints (512 MB)
-        if (ctx_dev_reserve(c, c->gang, (size_t)cap * sizeof(int32_t)) == XTED_OK) {
-            K.gang_blocks = std::min<int32_t>(XTED_GANG_MAX, c->grid);
-            K.gang_buf = (int32_t *)c->gang.p;
-            K.gang_cap = cap;
-        }
-    }
     // Optional per-task trace (XTED_TRACE=<file>): timestamps of every task,
     // written as raw uint64 quadruples after each run.
     const char *tr = std::getenv("XTED_TRACE");
@@ -176,7 +163,8 @@ static int enqueue_step(xted_ctx *c, bool events) {
           cudaMemsetAsync(K.rq, 0xff, ((size_t)XTED_RINGS << K.rq_log2) * sizeof(unsigned long long),
                           c->stream) != cudaSuccess ||
           cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_RINGS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
-          cudaMemsetAsync(K.gang_ctl, 0, XTED_GCTL_INTS * sizeof(int32_t), c->stream) != cudaSuccess ||
+          (K.nstripes > 0 &&
+           cudaMemsetAsync(K.sprog, 0, (size_t)K.nstripes * sizeof(int32_t), c->stream) != cudaSuccess) ||
           launch_rq_init(K, c->stream) != cudaSuccess)))
         return XTED_ECUDA;
     if (events && cudaEventRecord(c->evk0, c->stream) != cudaSuccess) return XTED_ECUDA;
@@ -386,7 +374,7 @@ int xted_destroy(xted_ctx *c) {
     xted::serve_shutdown(c);
     cudaStreamSynchronize(c->stream);
     ctx_drop_graph(c);
-    for (DevBuf *b : {&c->meta, &c->levels, &c->work, &c->dt, &c->scratch, &c->counters, &c->trace, &c->gang})
+    for (DevBuf *b : {&c->meta, &c->levels, &c->work, &c->dt, &c->scratch, &c->counters, &c->trace, &c->smap, &c->sbuf})
         if (b->p) cudaFree(b->p);
     for (HostBuf *b : {&c->stage, &c->result, &c->summary})
         if (b->p) cudaFreeHost(b->p);

@@ -36,7 +36,7 @@ struct xted_ctx {
     int grid = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evk0 = nullptr, evk1 = nullptr;
-    xted::DevBuf meta, levels, work, dt, scratch, counters, trace, gang;
+    xted::DevBuf meta, levels, work, dt, scratch, counters, trace, smap, sbuf;
     xted::HostBuf stage, result, summary;
     const int32_t *d_trivial = nullptr;
     int64_t held = 0;  // device bytes held by this context

@@ -605,10 +605,11 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 }
 
 // ---------------------------------------------------------------------------
-// Stripe s of a striped unit: columns [C0, C1) = [2048 s, min(2048 (s+1), w))
-// of a single column segment of width w, on the whole block (8 columns per
-// thread), concurrently with the other stripes on the other gang blocks. It
-// is run_group's row step with three additions:
+// Stripe s of a striped unit: columns [C0, C1) = [SW s, min(SW (s+1), w)),
+// SW = 256 W, of a single column segment of width w, on the whole block (W
+// columns per thread), concurrently with the unit's other stripes on other
+// blocks (or after them on this one). It is run_group's row step with three
+// additions:
 //   * the row's suffix minimum continues from the right: before the scan
 //     barrier the block waits for its right neighbour to finish the row and
 //     takes that stripe's carry (its minimum of A[k] + k over k >= C1);
@@ -619,7 +620,10 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 //     first column one row below.
 // Each stripe publishes per row its carry and first column, its exported
 // columns on pushed rows, then its progress (rows done, flat over the unit's
-// keyroots). Waits are bounded by the launch's timeout.
+// keyroots), every XTED_STRIPE_PUB rows. A stripe waits only for its right
+// neighbour, which was claimed before it (stripes are tasks, rightmost first)
+// and waits for nobody to its left; the waits are bounded by the launch's
+// timeout.
 // ---------------------------------------------------------------------------
 #ifndef XTED_STRIPE_PUB
 #define XTED_STRIPE_PUB 4
@@ -854,6 +858,30 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
         }
     }
     cp_async_wait<0>();
+}
+
+// A stripe task: stripe s of striped unit T.unit_lo, on the whole block. The
+// unit's buffer holds every stripe's carries and first columns per row, then
+// the exported far values per row; its progress words were zeroed by the run.
+template <bool UC>
+__device__ void run_striped(const XKernelParams &P, const XPair &pr, const XTask &T, int32_t *stk, WideShared &S,
+                            int32_t *ring, int32_t *cache, int32_t *cnode) {
+    const XStripe X = P.stripes[T.unit_lo];
+    const int s = (int)((T.kind_n >> XTED_STRIPE_SHIFT) & XTED_STRIPE_MASK);
+    const XUnit u = P.units[X.unit];
+    const int32_t *expmap = P.smap + X.map_off;
+    int32_t *prog = P.sprog + X.prog_off;
+    int32_t *CR = P.sbuf + X.buf_off;
+    int32_t *FC = CR + (int64_t)X.K * X.R;
+    int32_t *E = FC + (int64_t)X.K * X.R;
+    if (X.sww == 2)
+        run_stripe<2, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, prog, CR, FC, E);
+    else if (X.sww == 4)
+        run_stripe<4, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, prog, CR, FC, E);
+    else if (X.sww == 8)
+        run_stripe<8, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, prog, CR, FC, E);
+    else if (threadIdx.x == 0)
+        set_error(P, XTED_EINVAL, 13, X.sww, s);
 }
 
 template <bool UC>
@@ -1114,7 +1142,6 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int g, unsigned 
 #define CLAIM_EXIT (-1)
 #define CLAIM_RECORD (-2)
 #define CLAIM_NONE (-3)
-#define CLAIM_GANG (-4)  // a gang block: a striped unit waits for the gang
 
 // Returns a task index (and its entry), CLAIM_EXIT when the launch is over
 // (all tasks done, an error, or in a serving session the stop word or an
@@ -1138,7 +1165,6 @@ __device__ __forceinline__ int rq_entry(const XKernelParams &P, int g, unsigned 
 #define KINDS_NARROW 1u
 #define KINDS_ANY 3u
 
-template <bool STRIPES>
 __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lane, unsigned kinds, int prefer) {
     // Called by a whole warp; lane 0 claims, the warp reads every bucket's
     // head and tail in one coalesced load so that only non-empty buckets are
@@ -1155,10 +1181,6 @@ __device__ int claim_task(const XKernelParams &P, int *entry, bool wait, int lan
         if (lane == 0) {
             if (*(volatile int32_t *)P.error != 0) {
                 res = CLAIM_EXIT;
-            } else if (STRIPES && (int)blockIdx.x < P.gang_blocks &&
-                       ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_TAIL] > ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_HEAD]) {
-                if (idle_counted) atomicSub(&P.rq_ctl[CTL_IDLE], 1);
-                res = CLAIM_GANG;  // every gang block takes part in every striped unit
             } else if (P.serve) {
                 // admit posted queries first: their level-0 entries go to the new
                 // query's own (least urgent) bucket, and a busy launch would
@@ -1351,244 +1373,23 @@ __device__ void trace_task_end(const XKernelParams &P, int t) {
     asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
     const int nu = (int)(T.kind_n & 0xffff);
     unsigned long long cells = 0, wmax = 0;
-    for (int k = 0; k < nu; k++) {
-        const XUnit u = P.units[T.unit_lo + k];
-        const unsigned long long w = (unsigned)P.chunks[u.chunk].width;
-        cells += w * (unsigned)P.runs[u.run].rows;
-        if (w > wmax) wmax = w;
+    if (T.kind_n & XTED_TASK_STRIPED) {  // this stripe's columns of its unit
+        const XStripe X = P.stripes[T.unit_lo];
+        const int sw = XTED_CTA_THREADS * X.sww, s = (int)((T.kind_n >> XTED_STRIPE_SHIFT) & XTED_STRIPE_MASK);
+        wmax = (unsigned long long)min(sw, X.w - s * sw);
+        cells = wmax * (unsigned)X.R;
+    } else {
+        for (int k = 0; k < nu; k++) {
+            const XUnit u = P.units[T.unit_lo + k];
+            const unsigned long long w = (unsigned)P.chunks[u.chunk].width;
+            cells += w * (unsigned)P.runs[u.run].rows;
+            if (w > wmax) wmax = w;
+        }
     }
     P.trace[4 * (int64_t)t + 2] = global_ns();
     P.trace[4 * (int64_t)t + 3] = ((T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) ? 1ull : 0ull) |
                                   ((unsigned long long)(nu & 127) << 1) | ((unsigned long long)(sm & 255) << 8) |
                                   ((wmax & 0xffff) << 16) | ((cells & 0xffffffffull) << 32);
-}
-
-// ---- striped units: the gang ----
-// A block that claims a striped unit hands it to the gang ring instead of
-// running it (on one block when the ring is full or there is no gang); the
-// gang blocks (0 .. gang_blocks-1) notice pending units when they look for
-// work, meet at a barrier, the leader (block 0) lays the unit out, and each
-// block runs one stripe. One striped unit at a time.
-__device__ bool gang_push(const XKernelParams &P, int t, int e, bool small) {
-    volatile int32_t *g = P.gang_ctl;
-    const int limit = small ? XTED_GANG_SMALL_QUEUE : XTED_GANG_RING;
-    for (int it = 0; it < 1024; it++) {
-        const int tl = g[XTED_GCTL_TAIL], hd = g[XTED_GCTL_HEAD];
-        if (tl - hd >= limit) return false;
-        if (atomicCAS(&P.gang_ctl[XTED_GCTL_TAIL], tl, tl + 1) == tl) {
-            volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (tl & (XTED_GANG_RING - 1));
-            slot[1] = t;
-            slot[2] = e;
-            __threadfence();
-            slot[0] = tl + 1;  // the slot holds position tl
-            return true;
-        }
-    }
-    return false;
-}
-
-// Barrier of the gang blocks (a global arrival count; phases counted per
-// block, equal in every gang block). False after an error or a timeout.
-__device__ bool gang_barrier(const XKernelParams &P, int *s_phase, int *s_ok) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const int target = (*s_phase + 1) * P.gang_blocks;
-        atomicAdd(&P.gang_ctl[XTED_GCTL_BAR], 1);
-        bool ok = false;
-        const uint64_t t0 = global_ns();
-        for (long it = 0; it < (1L << 26); it++) {
-            if (((volatile int32_t *)P.gang_ctl)[XTED_GCTL_BAR] >= target) {
-                ok = true;
-                break;
-            }
-            if (*(volatile int32_t *)P.error != 0) break;
-            if (global_ns() - t0 > P.timeout_ns) {
-                set_error(P, XTED_ETIMEOUT, 9, target, ((volatile int32_t *)P.gang_ctl)[XTED_GCTL_BAR]);
-                break;
-            }
-            __nanosleep(64);
-        }
-        __threadfence();
-        *s_phase += 1;
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
-
-// One round of striped units, run by every gang block (all threads): block 0
-// takes the unit at the gang ring's head and, while they fit the gang's
-// blocks and buffer, the units queued behind it (independent tables, all
-// ready), lays each out in its own part of the gang buffer and gives it a
-// range of consecutive gang blocks; every block then runs its stripe of its
-// unit. Several narrow tables of one level then run side by side instead of
-// one after another.
-template <bool UC>
-__device__ void run_gang(const XKernelParams &P, int32_t *scratch, WideShared &S, int32_t *ring, int32_t *cache,
-                         int32_t *cnode, int *s_g) {
-    // s_g: [0] phase, [1] ok, [2] units in the round, [3..7] scratch, then
-    // XTED_GANG_UNITS descriptors of 8 ints: task, entry, stripes, exports,
-    // feasible, columns per thread, first block, buffer offset
-    int *desc = s_g + 8;
-    const int tid = threadIdx.x, b = blockIdx.x;
-    volatile int32_t *g = P.gang_ctl;
-    if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // A: every gang block is here
-    if (b == 0) {
-        int nunits = 0, blocks_used = 0;
-        int64_t buf_used = 0;
-        for (int ui = 0; ui < XTED_GANG_UNITS; ui++) {
-            if (tid == 0) {
-                const int hd = g[XTED_GCTL_HEAD] + ui;
-                volatile int32_t *slot = g + XTED_GCTL_RING + 4 * (hd & (XTED_GANG_RING - 1));
-                bool ok = false;
-                if (ui == 0) {  // the unit that called the gang: wait until its slot is written
-                    const uint64_t t0 = global_ns();
-                    for (long it = 0; it < (1L << 26); it++) {
-                        if (slot[0] == hd + 1) {
-                            ok = true;
-                            break;
-                        }
-                        if (global_ns() - t0 > P.timeout_ns) break;
-                        __nanosleep(32);
-                    }
-                    if (!ok) set_error(P, XTED_ETIMEOUT, 12, hd, 0);
-                } else {  // units behind it only if already queued
-                    ok = g[XTED_GCTL_TAIL] - hd > 0 && slot[0] == hd + 1;
-                }
-                __threadfence();
-                s_g[3] = ok ? slot[1] : -1;
-                s_g[4] = ok ? slot[2] : -1;
-            }
-            __syncthreads();
-            const int t = s_g[3];
-            if (t < 0) break;
-            const XTask T = P.tasks[t];
-            const XUnit u = P.units[T.unit_lo];
-            const XChunk ch = P.chunks[u.chunk];
-            const XPair pr = P.pairs[T.pair];
-            const int w = ch.width, R = P.runs[u.run].rows;
-            // the narrowest stripes (at least XTED_STRIPE_MIN_W columns per
-            // thread) that the gang's blocks cover: more stripes run a
-            // table's rows in parallel, each row passed right to left
-            int SWd = XTED_CTA_THREADS * XTED_STRIPE_MIN_W;
-            while (SWd < XTED_STRIPE && (w + SWd - 1) / SWd > P.gang_blocks) SWd *= 2;
-            const int K = (w + SWd - 1) / SWd;
-            if (ui > 0 && blocks_used + K > P.gang_blocks) break;  // the round is full
-            int32_t *expmap = P.gang_buf + buf_used;
-            // mark the far columns that cross a stripe boundary, then number them
-            for (int c = tid; c < w; c += XTED_CTA_THREADS) expmap[c] = 0;
-            __syncthreads();
-            {
-                const int2 *nodes = P.rowinfo + pr.col_base;
-                const int j0 = P.krd[ch.k_lo];
-                for (int c = tid; c < w; c += XTED_CTA_THREADS) {
-                    const int j = j0 + c;
-                    const int f = c + ((nodes[j].y & XTED_ROW_ORL_MASK) + 1 - j);
-                    if (f < w && f / SWd != c / SWd) expmap[f] = 1;
-                }
-            }
-            __syncthreads();
-            const int per = (w + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS;
-            const int a0 = min(tid * per, w), a1 = min(a0 + per, w);
-            int cnt = 0;
-            for (int c = a0; c < a1; c++) cnt += expmap[c];
-            // block exclusive scan of cnt (warp scan, then the warps' totals)
-            const int lane = tid & 31, warp = tid >> 5;
-            const int incl = warp_prefix_sum(cnt, lane);
-            if (lane == 31) S.ends[warp] = incl;
-            __syncthreads();
-            int before = incl - cnt;
-            for (int q = 0; q < warp; q++) before += S.ends[q];
-            int total = 0;
-            for (int q = 0; q < XTED_WARPS; q++) total += S.ends[q];
-            for (int c = a0; c < a1; c++) {
-                const int m = expmap[c];
-                expmap[c] = m ? before : -1;
-                before += m;
-            }
-            const int X = total;
-            const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
-            const int64_t need = (wal + XTED_GANG_MAX + 2 * (int64_t)K * R + (int64_t)R * X + 31) & ~(int64_t)31;
-            const bool fits = buf_used + need <= P.gang_cap;
-            if (ui > 0 && !fits) break;  // the buffer is full: the next round takes it
-            const int feasible = K <= P.gang_blocks && fits;
-            if (feasible && tid < XTED_GANG_MAX) expmap[wal + tid] = 0;  // progress words
-            if (tid == 0) {
-                int *d = desc + 8 * ui;
-                d[0] = t;
-                d[1] = s_g[4];
-                d[2] = K;
-                d[3] = X;
-                d[4] = feasible;
-                d[5] = SWd / XTED_CTA_THREADS;
-                d[6] = blocks_used;
-                d[7] = (int)(buf_used >> 5);  // in units of 32 ints
-            }
-            blocks_used += feasible ? K : 1;  // an infeasible unit runs alone on its first block
-            if (feasible) buf_used += need;
-            nunits++;
-            __syncthreads();
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) {
-            g[XTED_GCTL_DESC] = nunits;
-            for (int q = 0; q < 8 * nunits; q++) g[XTED_GCTL_UDESC + q] = desc[q];
-            __threadfence();
-        }
-    }
-    if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // B: the layout is ready
-    if (tid == 0) {
-        s_g[2] = g[XTED_GCTL_DESC];
-        for (int q = 0; q < 8 * s_g[2]; q++) desc[q] = g[XTED_GCTL_UDESC + q];
-    }
-    __syncthreads();
-    const int nunits = s_g[2];
-    for (int ui = 0; ui < nunits; ui++) {
-        const int *d = desc + 8 * ui;
-        const int t = d[0], K = d[2], X = d[3], feasible = d[4], SWW = d[5], base = d[6];
-        if (b < base || b >= base + (feasible ? K : 1)) continue;
-        __threadfence();  // acquire: the unit's inputs (complete before it was published) and the layout
-        const XTask T = P.tasks[t];
-        const XUnit u = P.units[T.unit_lo];
-        const XPair pr = P.pairs[T.pair];
-        if (P.trace && b == base && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
-        if (feasible) {
-            const int w = P.chunks[u.chunk].width, R = P.runs[u.run].rows;
-            const int64_t wal = ((int64_t)w + 31) & ~(int64_t)31;
-            int32_t *expmap = P.gang_buf + ((int64_t)d[7] << 5);
-            int32_t *prog = expmap + wal;
-            int32_t *CR = prog + XTED_GANG_MAX;
-            int32_t *FC = CR + (int64_t)K * R;
-            int32_t *E = FC + (int64_t)K * R;
-            const int st = b - base;
-            if (SWW == 1)
-                run_stripe<1, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
-            else if (SWW == 2)
-                run_stripe<2, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
-            else if (SWW == 4)
-                run_stripe<4, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
-            else
-                run_stripe<8, UC>(P, pr, u, scratch, S, ring, cache, cnode, st, K, X, R, expmap, prog, CR, FC, E);
-        } else {
-            dispatch_wide<UC>(P, pr, u, scratch, S, ring, cache, cnode);  // too wide or too many exports: one block
-        }
-        __threadfence();
-    }
-    if (b == 0 && tid == 0) {  // the round's ring slots are consumed before anyone looks for the next unit
-        g[XTED_GCTL_HEAD] = g[XTED_GCTL_HEAD] + nunits;
-        __threadfence();
-    }
-    if (!gang_barrier(P, &s_g[0], &s_g[1])) return;  // C: every stripe is done
-    if (b == 0 && tid == 0) {
-        for (int ui = 0; ui < nunits; ui++) {
-            const int t = desc[8 * ui];
-            complete_task(P, desc[8 * ui + 1], P.tasks[t].pair);
-            if (P.trace) trace_task_end(P, t);
-        }
-    }
-    __syncthreads();
 }
 
 // Narrow tasks open in a block. The block's warps take units one at a time
@@ -1614,15 +1415,14 @@ static_assert(XTED_TASK_UNITS + XTED_WARPS < 256, "unit counter of a flow slot")
 #define CHAIN_MAX 2  // group tasks run back to back while narrow units wait
 #define PARK_SLOTS 16  // parked narrow units (at most one per warp is ever in flight; spare room for races)
 
-// The persistent DP kernel. Two instantiations: without striped units (every
-// batch whose column segments fit the register paths: the gang code is left
-// out of the hot loop entirely), and with them.
+// The persistent DP kernel. Two instantiations per cost model: without
+// striped units (every batch whose column segments fit the register paths:
+// the stripe code is left out of the hot loop entirely), and with them.
 template <bool STRIPES, bool UC>
 __device__ __forceinline__ void dp_main(const XKernelParams &P) {
     __shared__ int s_next, s_k[2];
     __shared__ int s_mode, s_lock, s_gtask, s_gentry, s_progress, s_epoch, s_chain;
     __shared__ int s_role;  // XTED_KIND_* the block last claimed: the kind it prefers when idle
-    __shared__ int s_gang[8 + 8 * XTED_GANG_UNITS];  // gang protocol: barrier phase, status, unit descriptors
     __shared__ FlowSlot s_fs[FLOW_SLOTS];
     // narrow units parked between two keyroot tables while the block ran a
     // group task: x flow slot, y unit, z pair, w next keyroot
@@ -1651,7 +1451,6 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
         s_lock = -1;
         s_progress = 0;
         s_epoch = 0;
-        s_gang[0] = 0;
     }
     __syncthreads();
     volatile int *vmode = &s_mode, *vlock = &s_lock, *vprog = &s_progress, *vepoch = &s_epoch;
@@ -1682,21 +1481,13 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
         if (mode == FLOW_GROUP) {
             __syncwarp();
             __syncthreads();  // every warp is between units
-            if (STRIPES && s_gtask == CLAIM_GANG) {  // this gang block's part in a striped unit
-                run_gang<UC>(P, scratch, S[0], s_ring, s_cache, s_cnode, s_gang);
-                __syncthreads();
-                if (tid == 0) {
-                    s_progress++;
-                    *vmode = FLOW_RUN;
-                }
-                __syncthreads();
-                continue;
-            }
             const int t = s_gtask;
             const XTask T = P.tasks[t];
             const XPair pr = P.pairs[T.pair];
             if (P.trace && tid == 0) P.trace[4 * (int64_t)t + 1] = global_ns();
-            if (T.kind_n & XTED_TASK_WIDE) {
+            if (STRIPES && (T.kind_n & XTED_TASK_STRIPED)) {
+                run_striped<UC>(P, pr, T, scratch, S[0], s_ring, s_cache, s_cnode);
+            } else if (T.kind_n & XTED_TASK_WIDE) {
                 dispatch_wide<UC>(P, pr, P.units[T.unit_lo], scratch, S[0], s_ring, s_cache, s_cnode);
             } else {
                 // the block's two halves take the task's units one at a time
@@ -1719,8 +1510,8 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
             __syncthreads();
             if (warp == 0) {
                 // Every warp waits at the barrier below, so the block looks for
-                // its next task now: another group task (or a striped unit for
-                // a gang block) then runs without gathering the warps again,
+                // its next task now: another group task (a stripe among them)
+                // then runs without gathering the warps again,
                 // which costs them the tail of whatever they were running. A
                 // narrow task found here is opened as usual. While parked or
                 // open narrow units wait, at most CHAIN_MAX group tasks chain.
@@ -1738,20 +1529,13 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                     allow = room && (!waiting || s_chain < CHAIN_MAX);
                 }
                 if (__shfl_sync(FULLMASK, allow, 0))
-                    nt = claim_task<STRIPES>(P, &ne, false, lane, KINDS_ANY, XTED_KIND_GROUP);
+                    nt = claim_task(P, &ne, false, lane, KINDS_ANY, XTED_KIND_GROUP);
                 if (lane == 0) {
                     bool stay = false;
-                    if (nt == CLAIM_GANG) {
-                        s_gtask = CLAIM_GANG;
-                        stay = true;
-                    } else if (nt >= 0) {
+                    if (nt >= 0) {
                         const XTask T2 = P.tasks[nt];
                         if (P.trace) P.trace[4 * (int64_t)nt] = global_ns();
-                        if (STRIPES && (T2.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 &&
-                            gang_push(P, nt, ne, (int64_t)P.runs[P.units[T2.unit_lo].run].rows *
-                                                     P.chunks[P.units[T2.unit_lo].chunk].width < XTED_GANG_BIG_CELLS)) {
-                            // handed to the gang
-                        } else if (T2.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
+                        if (T2.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
                             s_gtask = nt;
                             s_gentry = ne;
                             s_next = 0;
@@ -1904,7 +1688,7 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                 if (stop) break;
                 // narrow units in flight: narrow tasks only; an idle block takes
                 // either kind, its role's first within a bucket
-                t = claim_task<STRIPES>(P, &e, !busy, lane, busy ? KINDS_NARROW : KINDS_ANY,
+                t = claim_task(P, &e, !busy, lane, busy ? KINDS_NARROW : KINDS_ANY,
                                         busy ? XTED_KIND_NARROW : *(volatile int *)&s_role);
                 if (t != CLAIM_NONE) break;
                 __nanosleep(ns);  // nothing ready while units of this block run: poll again soon
@@ -1912,19 +1696,11 @@ __device__ __forceinline__ void dp_main(const XKernelParams &P) {
                 if (ns < XTED_CLAIM_SLEEP_MAX) ns <<= 1;
             }
             if (lane == 0) {
-                if (t == CLAIM_GANG) {
-                    s_gtask = CLAIM_GANG;
-                    __threadfence_block();
-                    *vmode = FLOW_GROUP;
-                } else if (t >= 0) {
+                if (t >= 0) {
                     atomicAdd(&s_progress, 1);
                     const XTask T = P.tasks[t];
                     if (P.trace) P.trace[4 * (int64_t)t] = global_ns();
-                    if (STRIPES && (T.kind_n & XTED_TASK_STRIPED) && P.gang_blocks > 0 &&
-                        gang_push(P, t, e, (int64_t)P.runs[P.units[T.unit_lo].run].rows *
-                                                   P.chunks[P.units[T.unit_lo].chunk].width < XTED_GANG_BIG_CELLS)) {
-                        // handed to the gang: its blocks run it in stripes
-                    } else if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
+                    if (T.kind_n & (XTED_TASK_WIDE | XTED_TASK_HALF)) {
                         s_gtask = t;
                         s_gentry = e;
                         s_next = 0;
@@ -2050,7 +1826,7 @@ cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const bool unit = P.c_del == 1 && P.c_ins == 1 && P.c_ren == 1;
-    const void *k = P.gang_blocks > 0 ? (unit ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel_striped_costs)
+    const void *k = P.nstripes > 0 ? (unit ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel_striped_costs)
                                       : (unit ? (const void *)xted_dp_kernel : (const void *)xted_dp_kernel_costs);
     return cudaLaunchKernelExC(&cfg, k, args);
 }

@@ -67,6 +67,8 @@ struct DLevel {
     int32_t ntasks, entry;  // tasks at this level; this entry's index
     int32_t nntasks;        // its narrow tasks (the first ones of its range)
     int32_t task_off, unit_off;
+    int32_t nstriped, nstripes;    // striped units, and their stripes (tasks)
+    int32_t stripe_off, sprog_off; // its first striped unit and progress word
     int64_t key;            // estimate, then the earliest start of the level (see k_pair_rank)
 };
 
@@ -383,13 +385,38 @@ XT_HD inline bool big_run(const LevelCtx &C, int32_t run) {
     return C.wide_rows >= 0 && C.runs[run].rows > C.wide_rows;
 }
 
+// Columns per thread of a striped segment of w columns: the narrowest stripes
+// (512 columns) unless that makes more than XTED_STRIPES_MAX of them. Narrow
+// stripes run a table's rows on more blocks at once; a stripe row costs
+// little more at 512 columns than at 2,048.
+XT_HD inline int32_t stripe_sww(int32_t w) {
+    int32_t sww = XTED_STRIPE_MIN_W;
+    while (sww < XTED_STRIPE / XTED_CTA_THREADS &&
+           (w + XTED_CTA_THREADS * sww - 1) / (XTED_CTA_THREADS * sww) > XTED_STRIPES_MAX)
+        sww *= 2;
+    return sww;
+}
+XT_HD inline int32_t stripe_count(int32_t w) {
+    const int32_t sw = XTED_CTA_THREADS * stripe_sww(w);
+    return (w + sw - 1) / sw;
+}
+// A whole-block unit of `rows` rows over one segment of w columns runs in
+// column stripes (else on one block, the generic wide path).
+#ifndef XTED_STRIPE_MIN_WIDTH
+#define XTED_STRIPE_MIN_WIDTH XTED_WIDE_REG_MAX  // (tests of the plan's layout build with less)
+#endif
+XT_HD inline bool striped_unit(const LevelCtx &C, int32_t rows, int32_t w) {
+    return C.stripe_min_cells > 0 && w > XTED_STRIPE_MIN_WIDTH && stripe_count(w) <= XTED_STRIPES_MAX &&
+           (int64_t)rows * w >= C.stripe_min_cells;
+}
+
 // Units and tasks of level entry e (pair, level) and its time estimate.
 XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     const DPair &q = C.pairs[E.pair];
     const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
-    int64_t wide = 0, narrow = 0, half = 0, nlong = 0;
+    int64_t wide = 0, narrow = 0, half = 0, nlong = 0, nstriped = 0, nstripes = 0;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
     int32_t small_max[64];  // longest bundled run per depth (the first 64 depths; more use maxrows)
     int32_t long_max[64];   // longest run of single-unit narrow tasks per depth
@@ -416,6 +443,15 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
         }
         wide += nr * cb.nwide + nbig * cb.nnarrow;
         half += nr * cb.nhalf;
+        if (C.stripe_min_cells > 0 && cb.maxw_w > XTED_STRIPE_MIN_WIDTH) {
+            const int32_t cw_lo = cb.chunk_lo + cb.nnarrow + cb.nhalf;
+            for (int32_t r = ra.run_lo; r < ra.run_hi; r++)
+                for (int32_t c = cw_lo; c < cw_lo + cb.nwide; c++)
+                    if (striped_unit(C, C.runs[r].rows, C.chunks[c].width)) {
+                        nstriped++;
+                        nstripes += stripe_count(C.chunks[c].width);
+                    }
+        }
         narrow += (nr - nbig) * cb.nnarrow;
         nlong += nl * cb.nnarrow;
     }
@@ -453,7 +489,9 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     E.nnarrow = (int32_t)narrow;
     E.nhalf = (int32_t)half;
     E.nntasks = (int32_t)((narrow - nlong + bundle - 1) / bundle + nlong);
-    E.ntasks = (int32_t)(wide + E.nntasks + (half + bundle_h - 1) / bundle_h);
+    E.nstriped = (int32_t)nstriped;
+    E.nstripes = (int32_t)nstripes;
+    E.ntasks = (int32_t)(wide - nstriped + nstripes + E.nntasks + (half + bundle_h - 1) / bundle_h);
     *est_out = est;
 }
 
@@ -475,12 +513,13 @@ XT_HD inline int32_t level_bucket(int64_t remaining, int64_t chain_max) {
 }
 
 // Writes the units and tasks of level entry E (offsets already assigned).
-XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, XTask *tasks) {
+XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, XTask *tasks,
+                             XStripe *stripes = nullptr) {
     const DPair &q = C.pairs[E.pair];
     const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
-    int32_t u = E.unit_off, t = E.task_off;
+    int32_t u = E.unit_off, t = E.task_off, so = E.stripe_off, po = E.sprog_off;
     const int32_t per_task = level_bundle(E.nnarrow);
     int32_t bundle = 0, bundle_lo = u;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
@@ -545,12 +584,30 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
                 }
             for (int32_t c = cw_lo; c < cw_hi; c++) {
                 units[u] = XUnit{r, c};
-                uint32_t kind = XTED_TASK_WIDE | 1u;
-                const int32_t w = C.chunks[c].width;
-                if (C.stripe_min_cells > 0 && w > XTED_WIDE_REG_MAX && w <= XTED_GANG_MAX * XTED_STRIPE &&
-                    (int64_t)C.runs[r].rows * w >= C.stripe_min_cells)
-                    kind |= XTED_TASK_STRIPED;
-                tasks[t++] = XTask{E.pair, E.entry, kind, u};
+                const int32_t w = C.chunks[c].width, rows = C.runs[r].rows;
+                if (stripes && striped_unit(C, rows, w)) {
+                    // one task per stripe, rightmost first
+                    const int32_t K = stripe_count(w);
+                    XStripe X;
+                    X.unit = u;
+                    X.K = K;
+                    X.sww = stripe_sww(w);
+                    X.X = 0;
+                    X.w = w;
+                    X.R = rows;
+                    X.prog_off = po;
+                    X.pair = E.pair;
+                    X.map_off = 0;
+                    X.buf_off = 0;
+                    stripes[so] = X;
+                    for (int32_t k = K - 1; k >= 0; k--)
+                        tasks[t++] = XTask{E.pair, E.entry,
+                                           XTED_TASK_WIDE | XTED_TASK_STRIPED | ((uint32_t)k << XTED_STRIPE_SHIFT) | 1u, so};
+                    so++;
+                    po += K;
+                } else {
+                    tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
+                }
                 u++;
             }
         }

@@ -157,6 +157,8 @@ __global__ void k_scan64(const int64_t *v, const int32_t *perm, int n, int64_t *
 struct Summary {
     int64_t entries, dt_elems;
     int64_t tasks, units;
+    int64_t nstriped, nstripes;  // striped units and their stripes
+    int64_t stripe_buf;          // ints of the striped units' buffers
     int32_t stack_rows, max_wide;
     int64_t cells, cells_right;
     int32_t levels_max, pad;
@@ -196,7 +198,8 @@ __global__ void k_level_expand(const DPair *pairs, int npairs, DLevel *lv) {
     }
 }
 
-__global__ void k_level_count(LevelCtx C, DLevel *lv, int64_t nent, int64_t *units, int64_t *tasks) {
+__global__ void k_level_count(LevelCtx C, DLevel *lv, int64_t nent, int64_t *units, int64_t *tasks,
+                              int64_t *striped, int64_t *stripes) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nent) return;
     DLevel E = lv[e];
@@ -206,6 +209,8 @@ __global__ void k_level_count(LevelCtx C, DLevel *lv, int64_t nent, int64_t *uni
     lv[e] = E;
     units[e] = (int64_t)E.nwide + E.nnarrow + E.nhalf;
     tasks[e] = E.ntasks;
+    striped[e] = E.nstriped;
+    stripes[e] = E.nstripes;
 }
 
 // Per pair: est(d) is the estimated time of level d's slowest task; EST(d) =
@@ -228,16 +233,21 @@ __global__ void k_pair_rank(const DPair *pairs, int npairs, DLevel *lv, int64_t 
 }
 
 __global__ void k_level_offsets(DLevel *lv, int64_t nent, const int64_t *task_scan, const int64_t *unit_scan,
-                                const int64_t *chain, const DPair *pairs, XEntry *entries, Summary *sum) {
+                                const int64_t *striped_scan, const int64_t *stripes_scan, const int64_t *chain,
+                                const DPair *pairs, XEntry *entries, Summary *sum) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e == 0) {
         sum->tasks = task_scan[nent];
         sum->units = unit_scan[nent];
+        sum->nstriped = striped_scan[nent];
+        sum->nstripes = stripes_scan[nent];
     }
     if (e >= nent) return;
     DLevel &E = lv[e];
     E.task_off = (int32_t)task_scan[e];
     E.unit_off = (int32_t)unit_scan[e];
+    E.stripe_off = (int32_t)striped_scan[e];
+    E.sprog_off = (int32_t)stripes_scan[e];
     E.entry = (int32_t)e;
     XEntry X;
     X.task_off = E.task_off;
@@ -249,9 +259,68 @@ __global__ void k_level_offsets(DLevel *lv, int64_t nent, const int64_t *task_sc
     entries[e] = X;
 }
 
-__global__ void k_level_fill(LevelCtx C, const DLevel *lv, int64_t nent, XUnit *units, XTask *tasks) {
+__global__ void k_level_fill(LevelCtx C, const DLevel *lv, int64_t nent, XUnit *units, XTask *tasks,
+                             XStripe *stripes) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nent) level_fill(C, lv[e], units, tasks);
+    if (e < nent) level_fill(C, lv[e], units, tasks, stripes);
+}
+
+// One block per striped unit: its export map, the far columns that a stripe
+// reads from a stripe to its right (f = orl(j) + 1 in another stripe), numbered
+// in column order (-1 elsewhere), and the ints its buffer needs: carries and
+// first columns of every stripe and row, and the exported values of every row.
+__global__ void k_stripe_prep(XStripe *stripes, int32_t *smap, int64_t map_stride, const XUnit *units,
+                              const XChunk *chunks, const XPair *pairs, const int2 *rowinfo, const int32_t *krd,
+                              int64_t *need) {
+    __shared__ int ends[XTED_WARPS];
+    const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const XStripe S = stripes[i];
+    const XChunk ch = chunks[units[S.unit].chunk];
+    const XPair pr = pairs[S.pair];
+    const int w = S.w, SW = XTED_CTA_THREADS * S.sww;
+    int32_t *expmap = smap + (int64_t)i * map_stride;
+    for (int c = tid; c < w; c += XTED_CTA_THREADS) expmap[c] = 0;
+    __syncthreads();
+    const int2 *nodes = rowinfo + pr.col_base;
+    const int j0 = krd[ch.k_lo];
+    for (int c = tid; c < w; c += XTED_CTA_THREADS) {
+        const int j = j0 + c;
+        const int f = c + ((nodes[j].y & XTED_ROW_ORL_MASK) + 1 - j);
+        if (f < w && f / SW != c / SW) expmap[f] = 1;
+    }
+    __syncthreads();
+    const int per = (w + XTED_CTA_THREADS - 1) / XTED_CTA_THREADS;
+    const int a0 = min(tid * per, w), a1 = min(a0 + per, w);
+    int cnt = 0;
+    for (int c = a0; c < a1; c++) cnt += expmap[c];
+    int incl = cnt;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
+    }
+    if (lane == 31) ends[warp] = incl;
+    __syncthreads();
+    int before = incl - cnt, total = 0;
+    for (int q = 0; q < XTED_WARPS; q++) {
+        if (q < warp) before += ends[q];
+        total += ends[q];
+    }
+    for (int c = a0; c < a1; c++) {
+        const int m = expmap[c];
+        expmap[c] = m ? before : -1;
+        before += m;
+    }
+    if (tid == 0) {
+        stripes[i].X = total;
+        stripes[i].map_off = (int64_t)i * map_stride;
+        need[i] = (2 * (int64_t)S.K * S.R + (int64_t)S.R * total + 31) & ~(int64_t)31;
+    }
+}
+
+__global__ void k_stripe_bufoff(XStripe *stripes, int64_t n, const int64_t *scan, Summary *sum) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) sum->stripe_buf = scan[n];
+    if (i < n) stripes[i].buf_off = scan[i];
 }
 
 __global__ void k_pair_finalize(const DPair *pairs, const DTree *trees, const DOTree *ot, int npairs, XPair *xp,
@@ -439,7 +508,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     if (nent > INT32_MAX / XTED_BUCKETS) return XTED_ENOMEM;
     // ---- buffer B: level entries and scans ----
     const size_t E1 = (size_t)nent + 1;
-    size_t needB = sizeof(DLevel) * E1 + sizeof(XEntry) * E1 + 4 * 8 * E1 + 12 * 256;
+    size_t needB = sizeof(DLevel) * E1 + sizeof(XEntry) * E1 + 8 * 8 * E1 + 16 * 256;
     rc = ctx_dev_reserve(c, c->levels, needB);
     if (rc) return rc;
     Carver cb{(char *)c->levels.p};
@@ -447,6 +516,8 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     XEntry *d_entries = cb.take<XEntry>(E1);
     int64_t *d_units = cb.take<int64_t>(E1), *d_tasks = cb.take<int64_t>(E1);
     int64_t *d_uscan = cb.take<int64_t>(E1), *d_tscan = cb.take<int64_t>(E1);
+    int64_t *d_striped = cb.take<int64_t>(E1), *d_stripes = cb.take<int64_t>(E1);
+    int64_t *d_sdscan = cb.take<int64_t>(E1), *d_spscan = cb.take<int64_t>(E1);
     LevelCtx C;
     C.ot = P.otrees;
     C.depths = P.depths;
@@ -456,15 +527,17 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     C.narrow_width = c->opts.narrow_width;
     C.wide_rows = c->opts.wide_rows > 0 ? c->opts.wide_rows : -1;
     C.stripe_min_cells = c->opts.stripe_min_cells < 0 ? 0
-                         : (c->opts.stripe_min_cells > 0 ? c->opts.stripe_min_cells : XTED_GANG_MIN_CELLS_DEFAULT);
+                         : (c->opts.stripe_min_cells > 0 ? c->opts.stripe_min_cells : XTED_STRIPE_MIN_CELLS_DEFAULT);
     if (nent > 0) {
         k_level_expand<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv);
-        k_level_count<<<blocks_for(nent, BS), BS, 0, s>>>(C, d_lv, nent, d_units, d_tasks);
+        k_level_count<<<blocks_for(nent, BS), BS, 0, s>>>(C, d_lv, nent, d_units, d_tasks, d_striped, d_stripes);
         k_pair_rank<<<blocks_for(npairs, BS), BS, 0, s>>>(d_pairs, npairs, d_lv, d_chain, d_sum);
         k_scan64<<<1, 1024, 0, s>>>(d_tasks, nullptr, (int)nent, d_tscan);
         k_scan64<<<1, 1024, 0, s>>>(d_units, nullptr, (int)nent, d_uscan);
-        k_level_offsets<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_tscan, d_uscan, d_chain, d_pairs,
-                                                              d_entries, d_sum);
+        k_scan64<<<1, 1024, 0, s>>>(d_striped, nullptr, (int)nent, d_sdscan);
+        k_scan64<<<1, 1024, 0, s>>>(d_stripes, nullptr, (int)nent, d_spscan);
+        k_level_offsets<<<blocks_for(nent, BS), BS, 0, s>>>(d_lv, nent, d_tscan, d_uscan, d_sdscan, d_spscan,
+                                                              d_chain, d_pairs, d_entries, d_sum);
     }
     cudaMemcpyAsync(hs, d_sum, sizeof(Summary), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) {
@@ -472,15 +545,16 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
         return XTED_ECUDA;
     }
     const int64_t ntasks = nent > 0 ? hs->tasks : 0, nunits = nent > 0 ? hs->units : 0;
-    if (ntasks > INT32_MAX / 2 || nunits > INT32_MAX / 2) return XTED_ENOMEM;
+    const int64_t nstriped = nent > 0 ? hs->nstriped : 0, nstripes = nent > 0 ? hs->nstripes : 0;
+    if (ntasks > INT32_MAX / 2 || nunits > INT32_MAX / 2 || nstripes > INT32_MAX / 2) return XTED_ENOMEM;
     // ---- buffer C: units, tasks and the ready queue's state ----
     int rq_log2 = 0;
     while (((int64_t)1 << rq_log2) < (int64_t)E1) rq_log2++;
     const size_t rq_slots = (size_t)XTED_RINGS << rq_log2;
     rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
                                          8 * rq_slots + 4 * (XTED_ESTATE * E1 + (size_t)npairs + 2 * XTED_RINGS + 8) +
-                                         4 * XTED_GCTL_INTS +
-                                         8 * 256);
+                                         sizeof(XStripe) * (size_t)(nstriped + 1) + 4 * (size_t)(nstripes + 1) +
+                                         8 * 2 * (size_t)(nstriped + 1) + 12 * 256);
     if (rc) return rc;
     Carver cw{(char *)c->work.p};
     XUnit *d_units_out = cw.take<XUnit>((size_t)nunits);
@@ -489,11 +563,35 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     int32_t *d_state = cw.take<int32_t>(XTED_ESTATE * E1);  // narrow claimed, group claimed, done per entry
     unsigned long long *d_rq = cw.take<unsigned long long>(rq_slots);
     int32_t *d_ctl = cw.take<int32_t>(2 * XTED_RINGS + 8);  // heads/tails, then the done counter
-    int32_t *d_gctl = cw.take<int32_t>(XTED_GCTL_INTS);       // striped units: ring, barrier, descriptor
-    if (nent > 0) k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out);
+    XStripe *d_st = cw.take<XStripe>((size_t)nstriped + 1);
+    int32_t *d_sprog = cw.take<int32_t>((size_t)nstripes + 1);
+    int64_t *d_need = cw.take<int64_t>((size_t)nstriped + 1), *d_needscan = cw.take<int64_t>((size_t)nstriped + 1);
+    if (nent > 0)
+        k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out, d_st);
     k_pair_finalize<<<blocks_for(std::max(npairs, 1), BS), BS, 0, s>>>(d_pairs, d_trees, P.otrees, npairs, d_xpairs,
                                                                        d_trivial, d_first);
     if (cudaGetLastError() != cudaSuccess) return XTED_ECUDA;
+    // striped units: export maps (one stride of the widest segment each), then
+    // the buffers, whose sizes the maps give
+    int64_t stripe_buf = 0;
+    if (nstriped > 0) {
+        const int64_t map_stride = ((int64_t)hs->max_wide + 31) & ~(int64_t)31;
+        rc = ctx_dev_reserve(c, c->smap, (size_t)(nstriped * map_stride) * sizeof(int32_t));
+        if (rc) return rc;
+        k_stripe_prep<<<(unsigned)nstriped, XTED_CTA_THREADS, 0, s>>>(d_st, (int32_t *)c->smap.p, map_stride,
+                                                                      d_units_out, P.chunks, d_xpairs, P.node,
+                                                                      P.krd, d_need);
+        k_scan64<<<1, 1024, 0, s>>>(d_need, nullptr, (int)nstriped, d_needscan);
+        k_stripe_bufoff<<<blocks_for(nstriped, BS), BS, 0, s>>>(d_st, nstriped, d_needscan, d_sum);
+        cudaMemcpyAsync(hs, d_sum, sizeof(Summary), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            cudaGetLastError();
+            return XTED_ECUDA;
+        }
+        stripe_buf = hs->stripe_buf;
+        rc = ctx_dev_reserve(c, c->sbuf, (size_t)std::max<int64_t>(stripe_buf, 1) * sizeof(int32_t));
+        if (rc) return rc;
+    }
 
     std::memset(&K, 0, sizeof(K));
     K.rowinfo = P.node;
@@ -514,7 +612,11 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.rq_log2 = rq_log2;
     K.rq_ctl = d_ctl;
     K.done_total = d_ctl + 2 * XTED_RINGS;
-    K.gang_ctl = d_gctl;
+    K.stripes = d_st;
+    K.sprog = d_sprog;
+    K.nstripes = (int32_t)nstripes;
+    K.smap = nstriped > 0 ? (const int32_t *)c->smap.p : nullptr;
+    K.sbuf = nstriped > 0 ? (int32_t *)c->sbuf.p : nullptr;
     K.hold_pair = -1;
     c->d_trivial = d_trivial;
     c->plan_dt_elems = hs->dt_elems;

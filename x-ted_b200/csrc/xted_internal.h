@@ -81,33 +81,34 @@ struct XUnit {
 };
 
 #define XTED_TASK_WIDE 0x80000000u  // one unit run by the whole block
-#define XTED_TASK_STRIPED 0x20000000u  // (with WIDE) the unit runs in column stripes on the gang blocks
-// Striped units: a single column segment wider than the register paths split
-// into XTED_STRIPE-column stripes, one per gang block (blocks 0 .. gang_blocks-1
-// of the launch), run concurrently with the stripes' row carries passed right
-// to left through the gang buffer.
+#define XTED_TASK_STRIPED 0x20000000u  // (with WIDE) one column stripe of a striped unit
+// Striped units: a single column segment wider than the register paths
+// (XTED_WIDE_REG_MAX columns) is split into column stripes of 256 * sww
+// columns, and every stripe is a task of its own: kind_n = WIDE | STRIPED |
+// (stripe << XTED_STRIPE_SHIFT) | 1, unit_lo = the striped unit's index in
+// XKernelParams::stripes. The K stripes of a unit are consecutive tasks of
+// its level, rightmost first, and blocks claim a level's tasks in index order:
+// the stripe a block waits for (its right neighbour, which passes it the row
+// carries) has always been claimed before, by a block that is running it or
+// has finished it. Any block runs any stripe, one block runs them all in turn.
+#define XTED_STRIPE_SHIFT 16
+#define XTED_STRIPE_MASK 0xfffu
 #define XTED_STRIPE 2048        // widest stripe (8 columns per thread)
 #define XTED_STRIPE_MIN_W 2     // narrowest stripe: 2 columns per thread (512 columns)
-#define XTED_GANG_MAX 128
-#define XTED_GANG_RING 256
-#define XTED_GANG_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
-// Units under XTED_GANG_BIG_CELLS go to the gang only while fewer than
-// XTED_GANG_SMALL_QUEUE units wait for it (a gang round runs at most
-// XTED_GANG_UNITS units side by side; when many more are ready, one block
-// each in parallel is faster); bigger ones always queue.
-#define XTED_GANG_BIG_CELLS ((int64_t)1 << 24)
-#define XTED_GANG_SMALL_QUEUE XTED_GANG_UNITS
-// gang control words: ring tail, ring head, barrier count, the round's unit
-// count and descriptors, then the ring (XTED_GANG_RING slots of 4 ints: tag,
-// task, entry, 0)
-#define XTED_GCTL_TAIL 0
-#define XTED_GCTL_HEAD 1
-#define XTED_GCTL_BAR 2
-#define XTED_GCTL_DESC 4   // units in the current round
-#define XTED_GANG_UNITS 16  // striped units one gang round may run side by side
-#define XTED_GCTL_UDESC 8  // their descriptors, 8 ints each
-#define XTED_GCTL_RING (XTED_GCTL_UDESC + 8 * XTED_GANG_UNITS)
-#define XTED_GCTL_INTS (XTED_GCTL_RING + 4 * XTED_GANG_RING)
+#define XTED_STRIPES_MAX 128    // stripes of one unit: a wider segment takes wider stripes
+#define XTED_STRIPE_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
+
+struct XStripe {       // a striped unit
+    int32_t unit;      // its unit
+    int32_t K;         // stripes
+    int32_t sww;       // columns per thread: a stripe is 256 * sww columns
+    int32_t X;         // far columns read across a stripe boundary (exported on every pushed row)
+    int32_t w, R;      // width (one segment) and rows
+    int32_t prog_off;  // its K progress words
+    int32_t pair;
+    int64_t map_off;   // its export map (w ints): column -> export index, or -1
+    int64_t buf_off;   // carries [K][R], first columns [K][R], exports [R][X]
+};
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
 #define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
 #define XTED_HALF_DEFAULT 512       // default limit: wider chunks run faster on the whole block
@@ -188,11 +189,12 @@ struct XKernelParams {
     int32_t *error_info;  // [4] diagnostics of the first error
     uint64_t timeout_ns;  // bound on every idle wait
     unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, info
-    // ---- striped units (gang_blocks = 0: a striped unit runs on one block) ----
-    int32_t gang_blocks;    // blocks 0 .. gang_blocks-1 run striped units together
-    int32_t *gang_ctl;      // XTED_GCTL_INTS words, zeroed per run
-    int32_t *gang_buf;      // export map, progress, carries, first columns, exported far values
-    int64_t gang_cap;       // ints in gang_buf
+    // ---- striped units (nstripes = 0: none) ----
+    const XStripe *stripes;
+    int32_t *sprog;        // [nstripes] rows each stripe has finished (flat over its unit's keyroots), zeroed per run
+    const int32_t *smap;   // export maps
+    int32_t *sbuf;         // carries, first columns, exports
+    int32_t nstripes;
     // ---- serving session (serve = 1); a batch launch leaves these zero ----
     int32_t serve;
     int32_t serve_pairs;    // pairs per query slot (the corpus size)
