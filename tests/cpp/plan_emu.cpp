@@ -156,7 +156,6 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
         E.task_off = (int32_t)toff;
         E.unit_off = (int32_t)uoff;
         E.stripe_off = (int32_t)soff;
-        E.sprog_off = (int32_t)poff;
         E.entry = (int32_t)e;
         toff += E.ntasks;
         uoff += (int64_t)E.nwide + E.nnarrow + E.nhalf;
@@ -174,16 +173,15 @@ static void plan(const std::vector<std::vector<int32_t>> &L, const std::vector<s
     H.tasks.assign((size_t)toff, XTask{-1, -1, 0, -1});
     H.stripes.assign((size_t)soff + 1, XStripe{});
     for (auto &E : H.lv) level_fill(C, E, H.units.data(), H.tasks.data(), H.stripes.data());
-    // stripes: progress words of consecutive striped units are consecutive
+    // stripes: every striped unit recorded, its stripes counted as planned
     int64_t pcheck = 0;
     for (int64_t i = 0; i < soff; i++) {
         const XStripe &S = H.stripes[(size_t)i];
-        if (S.prog_off != pcheck || S.K != stripe_count(S.w) || S.unit < 0 || S.unit >= uoff)
-            FAIL("striped unit %lld: progress word %d (want %lld), %d stripes", (long long)i, S.prog_off,
-                 (long long)pcheck, S.K);
+        if (S.K != stripe_count(S.w) || S.unit < 0 || S.unit >= uoff)
+            FAIL("striped unit %lld: unit %d, %d stripes", (long long)i, S.unit, S.K);
         pcheck += S.K;
     }
-    if (pcheck != poff) FAIL("progress words %lld, planned %lld", (long long)pcheck, (long long)poff);
+    if (pcheck != poff) FAIL("stripes %lld, planned %lld", (long long)pcheck, (long long)poff);
 }
 
 static void gen(int n, std::mt19937_64 &g, int alpha, int shape, std::vector<int32_t> &lab,

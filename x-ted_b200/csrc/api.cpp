@@ -163,8 +163,8 @@ static int enqueue_step(xted_ctx *c, bool events) {
           cudaMemsetAsync(K.rq, 0xff, ((size_t)XTED_RINGS << K.rq_log2) * sizeof(unsigned long long),
                           c->stream) != cudaSuccess ||
           cudaMemsetAsync(K.rq_ctl, 0, (2 * XTED_RINGS + 8) * sizeof(int32_t), c->stream) != cudaSuccess ||
-          (K.nstripes > 0 &&
-           cudaMemsetAsync(K.sprog, 0, (size_t)K.nstripes * sizeof(int32_t), c->stream) != cudaSuccess) ||
+          (K.nstriped > 0 &&
+           cudaMemsetAsync(K.sbuf, 0, (size_t)K.sbuf_words * sizeof(unsigned long long), c->stream) != cudaSuccess) ||
           launch_rq_init(K, c->stream) != cudaSuccess)))
         return XTED_ECUDA;
     if (events && cudaEventRecord(c->evk0, c->stream) != cudaSuccess) return XTED_ECUDA;

@@ -41,10 +41,6 @@ __device__ __forceinline__ int ld_acquire(const int32_t *p) {
     return v;
 }
 
-__device__ __forceinline__ void st_release(int32_t *p, int v) {
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -442,8 +438,6 @@ struct __align__(16) WideShared {
     int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
     int ends[XTED_WARPS];
     int cin;                    // stripes: the right neighbour's carry for the current row
-    int cbuf[16], fbuf[16];     // stripes: the right neighbour's carries and first columns of rows
-                                // [pf_lo, pf_hi), read in one batch while it is ahead (thread 0)
 };
 static_assert(XTED_WARPS == 8, "carry combination reads the warp minima as two int4");
 
@@ -618,32 +612,48 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 //     is ahead, and its stack slot may since hold another row);
 //   * the tree rows' diagonal at the last column is the right neighbour's
 //     first column one row below.
-// Each stripe publishes per row its carry and first column, its exported
-// columns on pushed rows, then its progress (rows done, flat over the unit's
-// keyroots), every XTED_STRIPE_PUB rows. A stripe waits only for its right
-// neighbour, which was claimed before it (stripes are tasks, rightmost first)
-// and waits for nobody to its left; the waits are bounded by the launch's
-// timeout.
+// Everything a stripe hands to another is a 64-bit word (flat row + 1) << 32
+// | value, written with one relaxed store: its carry and first column per row
+// (for the stripe to its left), and its exported columns on pushed rows (for
+// any stripe to its left). A reader checks the tag, so it needs no fence and
+// no progress counter: it loads the word early (the latency hides behind the
+// row's own work) and waits only if the tag is not there yet. The unit's
+// buffer is zeroed before every run. A stripe waits only for stripes to its
+// right, claimed before it (stripes are tasks, rightmost first), which wait
+// for nobody to their left; the waits are bounded by the launch's timeout.
 // ---------------------------------------------------------------------------
-#ifndef XTED_STRIPE_PUB
-#define XTED_STRIPE_PUB 4
-#endif
-__device__ __forceinline__ bool wait_progress(const XKernelParams &P, volatile int32_t *prog, int want) {
+__device__ __forceinline__ unsigned long long ld_tagged(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st_tagged(unsigned long long *p, unsigned tag, int value) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(((unsigned long long)tag << 32) | (unsigned)value));
+}
+// The value of the word at p once it carries `tag` (XTED_INF after an error
+// or the timeout); called only when an early load missed.
+__device__ __forceinline__ int wait_tagged(const XKernelParams &P, const unsigned long long *p, unsigned tag) {
     const uint64_t t0 = global_ns();
     for (long it = 0; it < (1L << 26); it++) {
-        if (ld_acquire((const int32_t *)prog) >= want) return true;  // acquire: the neighbour's row outputs
-        if (*(volatile int32_t *)P.error != 0) return false;
+        const unsigned long long v = ld_tagged(p);
+        if ((unsigned)(v >> 32) == tag) return (int)(unsigned)v;
+        if (*(volatile int32_t *)P.error != 0) return XTED_INF;
         if (global_ns() - t0 > P.timeout_ns) break;
         __nanosleep(32);
     }
-    set_error(P, XTED_ETIMEOUT, 10, want, prog[0]);
-    return false;
+    set_error(P, XTED_ETIMEOUT, 10, (int)tag, 0);
+    return XTED_INF;
+}
+__device__ __forceinline__ int tagged_value(const XKernelParams &P, const unsigned long long *p, unsigned long long v,
+                                            unsigned tag) {
+    return (unsigned)(v >> 32) == tag ? (int)(unsigned)v : wait_tagged(P, p, tag);
 }
 
 template <int W, bool UC>
 __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                            int32_t *ring, int32_t *cache, int32_t *cnode, int s, int K, int X, int R,
-                           const int32_t *expmap, int32_t *prog, int32_t *CR, int32_t *FC, int32_t *E) {
+                           const int32_t *expmap, unsigned long long *CR, unsigned long long *FC,
+                           unsigned long long *E) {
     constexpr int G = XTED_WARPS, SW = XTED_CTA_THREADS * W;  // stripe width: W columns per thread
     constexpr int GROW = 256 * G + 8 * G;  // padded row of the stack cache
     // the ring holds stripe rows only (SW columns): narrow stripes keep more
@@ -695,22 +705,9 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const int32_t *dt_in = P.dt + pr.dt_off;
     int32_t *dt_out = P.dt + pr.dt_off;
     const int2 *rows = P.rowinfo + pr.row_base;
-    volatile int32_t *prog_right = prog + s + 1;
-    int tflat = 0;
-    // thread 0: the right neighbour's carries and first columns, read in
-    // batches of up to 16 rows once that stripe is past them (one L2 round
-    // trip per batch instead of an acquire and two dependent loads per row)
-    int pf_lo = 0, pf_hi = 0, fc_pf = 0;
-    auto refill = [&](int avail) {
-        const int nb = min(min(avail - tflat, 16), R - tflat);
-        const int32_t *cr = CR + (int64_t)(s + 1) * R + tflat, *fc = FC + (int64_t)(s + 1) * R + tflat;
-        for (int q = 0; q < nb; q++) {
-            S.cbuf[q] = __ldcg(cr + q);
-            S.fbuf[q] = __ldcg(fc + q);
-        }
-        pf_lo = tflat;
-        pf_hi = tflat + nb;
-    };
+    const unsigned long long *cr_right = CR + (int64_t)(s + 1) * R, *fc_right = FC + (int64_t)(s + 1) * R;
+    unsigned long long *cr_mine = CR + (int64_t)s * R, *fc_mine = FC + (int64_t)s * R;
+    int tflat = 0, fc_next = 0;
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = P.krd[kr];
         const int imax = (rows[i0].y & XTED_ROW_ORL_MASK) + 1;
@@ -740,9 +737,12 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                              gtid == 0);
                 cp_async_commit();
             }
-            if (gtid == 0 && right && tflat >= pf_hi) {
-                const int avail = ld_acquire((const int32_t *)prog_right);
-                if (avail > tflat) refill(avail);
+            // thread 0: the right neighbour's carry and first column of this
+            // row, checked at the scan barrier
+            unsigned long long cw = 0, fw = 0;
+            if (gtid == 0 && right) {
+                cw = ld_tagged(cr_right + tflat);
+                fw = ld_tagged(fc_right + tflat);
             }
             const int32_t *slot = ring + (i & (PF - 1)) * SSLOT;
             const int2 ri = *(const int2 *)(slot + SROW);
@@ -754,7 +754,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             if (!trow) {
                 // forest row: far values from the stack top, or exported by the stripe that owns them
                 const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
-                const int32_t *erow = E + (int64_t)(tbase + (imax - 1 - (ro + 1))) * X;
+                const int efl = tbase + (imax - 1 - (ro + 1));  // flat row of the far row
+                const unsigned long long *erow = E + (int64_t)efl * X;
                 const int32_t *cur = slot + pbase;
                 const int rowfar = (imax - ro - 1) * KC.del, bord1 = bord + KC.ins;
                 int run_min = XTED_INF;
@@ -763,7 +764,10 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                     int far;
                     if ((C.tcol >> k) & 1u) far = rowfar;
                     else if (C.fidx[k] >= 0) far = top[C.fidx[k]];
-                    else far = __ldcg(erow + (-1 - C.fidx[k]));
+                    else {
+                        const unsigned long long *ep = erow + (-1 - C.fidx[k]);
+                        far = tagged_value(P, ep, ld_tagged(ep), (unsigned)efl + 1);
+                    }
                     int A = __viaddmin_s32(prev[k], KC.del, cur[k] + far);
                     A = min(A, bord1 | C.segor[k]);
                     run_min = __viaddmin_s32(A, C.key[k], run_min);
@@ -780,12 +784,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             if (gtid == 0) {
                 int cin = XTED_INF;
                 if (right) {
-                    if (tflat >= pf_hi && wait_progress(P, prog_right, tflat + 1))
-                        refill(ld_acquire((const int32_t *)prog_right));
-                    if (tflat < pf_hi) {
-                        cin = S.cbuf[tflat - pf_lo];
-                        fc_pf = S.fbuf[tflat - pf_lo];
-                    }
+                    cin = tagged_value(P, cr_right + tflat, cw, (unsigned)tflat + 1);
+                    fc_next = tagged_value(P, fc_right + tflat, fw, (unsigned)tflat + 1);
                 }
                 S.cin = cin;
             }
@@ -812,8 +812,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             }
             if (lane == 0) S.first[warp] = prev[0];
             if (gtid == 0 && left) {  // for the left neighbour: carry at C0 and D[i][C0]
-                CR[(int64_t)s * R + tflat] = prev[0] + C.key[0];
-                FC[(int64_t)s * R + tflat] = prev[0];
+                st_tagged(cr_mine + tflat, (unsigned)tflat + 1, prev[0] + C.key[0]);
+                st_tagged(fc_mine + tflat, (unsigned)tflat + 1, prev[0]);
             }
             if (i != i0 && (ri.y & XTED_ROW_ISKR)) {
                 sp--;
@@ -839,22 +839,18 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                     set_error(P, XTED_ENOMEM, 11, sp, stack_rows);
                 }
                 if (expm) {  // a pushed row is a far row: export the columns stripes to the left read
-                    int32_t *erow = E + (int64_t)tflat * X;
+                    unsigned long long *erow = E + (int64_t)tflat * X;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((expm >> k) & 1u) erow[__ldcg(&expmap[c0 + k])] = prev[k];
+                        if ((expm >> k) & 1u) st_tagged(erow + __ldcg(&expmap[c0 + k]), (unsigned)tflat + 1, prev[k]);
                 }
                 sp++;
                 if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
             }
             // the next row's diagonal at C1: the right neighbour's first column of this row
-            if (gtid == 0 && right) S.first[G] = fc_pf;
+            if (gtid == 0 && right) S.first[G] = fc_next;
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
-            __syncthreads();          // ... and everyone's, the record and the stack push; this row's outputs
-            // one release after the barrier orders the whole block's outputs;
-            // published every XTED_STRIPE_PUB rows (and at the unit's end)
-            if (gtid == 0 && left && ((tflat + 1) % XTED_STRIPE_PUB == 0 || tflat + 1 == R))
-                st_release(prog + s, tflat + 1);
+            __syncthreads();          // ... and everyone's, the record and the stack push
         }
     }
     cp_async_wait<0>();
@@ -862,7 +858,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
 
 // A stripe task: stripe s of striped unit T.unit_lo, on the whole block. The
 // unit's buffer holds every stripe's carries and first columns per row, then
-// the exported far values per row; its progress words were zeroed by the run.
+// the exported far values per row, as tagged words.
 template <bool UC>
 __device__ void run_striped(const XKernelParams &P, const XPair &pr, const XTask &T, int32_t *stk, WideShared &S,
                             int32_t *ring, int32_t *cache, int32_t *cnode) {
@@ -870,16 +866,15 @@ __device__ void run_striped(const XKernelParams &P, const XPair &pr, const XTask
     const int s = (int)((T.kind_n >> XTED_STRIPE_SHIFT) & XTED_STRIPE_MASK);
     const XUnit u = P.units[X.unit];
     const int32_t *expmap = P.smap + X.map_off;
-    int32_t *prog = P.sprog + X.prog_off;
-    int32_t *CR = P.sbuf + X.buf_off;
-    int32_t *FC = CR + (int64_t)X.K * X.R;
-    int32_t *E = FC + (int64_t)X.K * X.R;
+    unsigned long long *CR = P.sbuf + X.buf_off;
+    unsigned long long *FC = CR + (int64_t)X.K * X.R;
+    unsigned long long *E = FC + (int64_t)X.K * X.R;
     if (X.sww == 2)
-        run_stripe<2, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, prog, CR, FC, E);
+        run_stripe<2, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
     else if (X.sww == 4)
-        run_stripe<4, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, prog, CR, FC, E);
+        run_stripe<4, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
     else if (X.sww == 8)
-        run_stripe<8, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, prog, CR, FC, E);
+        run_stripe<8, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
     else if (threadIdx.x == 0)
         set_error(P, XTED_EINVAL, 13, X.sww, s);
 }
@@ -1826,7 +1821,7 @@ cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const bool unit = P.c_del == 1 && P.c_ins == 1 && P.c_ren == 1;
-    const void *k = P.nstripes > 0 ? (unit ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel_striped_costs)
+    const void *k = P.nstriped > 0 ? (unit ? (const void *)xted_dp_kernel_striped : (const void *)xted_dp_kernel_striped_costs)
                                       : (unit ? (const void *)xted_dp_kernel : (const void *)xted_dp_kernel_costs);
     return cudaLaunchKernelExC(&cfg, k, args);
 }

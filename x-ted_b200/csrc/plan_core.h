@@ -68,7 +68,7 @@ struct DLevel {
     int32_t nntasks;        // its narrow tasks (the first ones of its range)
     int32_t task_off, unit_off;
     int32_t nstriped, nstripes;    // striped units, and their stripes (tasks)
-    int32_t stripe_off, sprog_off; // its first striped unit and progress word
+    int32_t stripe_off;            // its first striped unit
     int64_t key;            // estimate, then the earliest start of the level (see k_pair_rank)
 };
 
@@ -519,7 +519,7 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
     const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
-    int32_t u = E.unit_off, t = E.task_off, so = E.stripe_off, po = E.sprog_off;
+    int32_t u = E.unit_off, t = E.task_off, so = E.stripe_off;
     const int32_t per_task = level_bundle(E.nnarrow);
     int32_t bundle = 0, bundle_lo = u;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
@@ -595,8 +595,8 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
                     X.X = 0;
                     X.w = w;
                     X.R = rows;
-                    X.prog_off = po;
                     X.pair = E.pair;
+                    X.pad = 0;
                     X.map_off = 0;
                     X.buf_off = 0;
                     stripes[so] = X;
@@ -604,7 +604,6 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
                         tasks[t++] = XTask{E.pair, E.entry,
                                            XTED_TASK_WIDE | XTED_TASK_STRIPED | ((uint32_t)k << XTED_STRIPE_SHIFT) | 1u, so};
                     so++;
-                    po += K;
                 } else {
                     tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, u};
                 }

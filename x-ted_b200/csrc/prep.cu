@@ -158,7 +158,7 @@ struct Summary {
     int64_t entries, dt_elems;
     int64_t tasks, units;
     int64_t nstriped, nstripes;  // striped units and their stripes
-    int64_t stripe_buf;          // ints of the striped units' buffers
+    int64_t stripe_buf;          // 64-bit words of the striped units' buffers
     int32_t stack_rows, max_wide;
     int64_t cells, cells_right;
     int32_t levels_max, pad;
@@ -247,7 +247,6 @@ __global__ void k_level_offsets(DLevel *lv, int64_t nent, const int64_t *task_sc
     E.task_off = (int32_t)task_scan[e];
     E.unit_off = (int32_t)unit_scan[e];
     E.stripe_off = (int32_t)striped_scan[e];
-    E.sprog_off = (int32_t)stripes_scan[e];
     E.entry = (int32_t)e;
     XEntry X;
     X.task_off = E.task_off;
@@ -267,7 +266,7 @@ __global__ void k_level_fill(LevelCtx C, const DLevel *lv, int64_t nent, XUnit *
 
 // One block per striped unit: its export map, the far columns that a stripe
 // reads from a stripe to its right (f = orl(j) + 1 in another stripe), numbered
-// in column order (-1 elsewhere), and the ints its buffer needs: carries and
+// in column order (-1 elsewhere), and the words its buffer needs: carries and
 // first columns of every stripe and row, and the exported values of every row.
 __global__ void k_stripe_prep(XStripe *stripes, int32_t *smap, int64_t map_stride, const XUnit *units,
                               const XChunk *chunks, const XPair *pairs, const int2 *rowinfo, const int32_t *krd,
@@ -313,7 +312,7 @@ __global__ void k_stripe_prep(XStripe *stripes, int32_t *smap, int64_t map_strid
     if (tid == 0) {
         stripes[i].X = total;
         stripes[i].map_off = (int64_t)i * map_stride;
-        need[i] = (2 * (int64_t)S.K * S.R + (int64_t)S.R * total + 31) & ~(int64_t)31;
+        need[i] = (2 * (int64_t)S.K * S.R + (int64_t)S.R * total + 15) & ~(int64_t)15;
     }
 }
 
@@ -553,8 +552,8 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     const size_t rq_slots = (size_t)XTED_RINGS << rq_log2;
     rc = ctx_dev_reserve(c, c->work, sizeof(XUnit) * (size_t)(nunits + 1) + sizeof(XTask) * (size_t)(ntasks + 1) +
                                          8 * rq_slots + 4 * (XTED_ESTATE * E1 + (size_t)npairs + 2 * XTED_RINGS + 8) +
-                                         sizeof(XStripe) * (size_t)(nstriped + 1) + 4 * (size_t)(nstripes + 1) +
-                                         8 * 2 * (size_t)(nstriped + 1) + 12 * 256);
+                                         sizeof(XStripe) * (size_t)(nstriped + 1) + 8 * 2 * (size_t)(nstriped + 1) +
+                                         12 * 256);
     if (rc) return rc;
     Carver cw{(char *)c->work.p};
     XUnit *d_units_out = cw.take<XUnit>((size_t)nunits);
@@ -564,7 +563,6 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     unsigned long long *d_rq = cw.take<unsigned long long>(rq_slots);
     int32_t *d_ctl = cw.take<int32_t>(2 * XTED_RINGS + 8);  // heads/tails, then the done counter
     XStripe *d_st = cw.take<XStripe>((size_t)nstriped + 1);
-    int32_t *d_sprog = cw.take<int32_t>((size_t)nstripes + 1);
     int64_t *d_need = cw.take<int64_t>((size_t)nstriped + 1), *d_needscan = cw.take<int64_t>((size_t)nstriped + 1);
     if (nent > 0)
         k_level_fill<<<blocks_for(nent, 64), 64, 0, s>>>(C, d_lv, nent, d_units_out, d_tasks_out, d_st);
@@ -589,7 +587,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
             return XTED_ECUDA;
         }
         stripe_buf = hs->stripe_buf;
-        rc = ctx_dev_reserve(c, c->sbuf, (size_t)std::max<int64_t>(stripe_buf, 1) * sizeof(int32_t));
+        rc = ctx_dev_reserve(c, c->sbuf, (size_t)std::max<int64_t>(stripe_buf, 1) * sizeof(unsigned long long));
         if (rc) return rc;
     }
 
@@ -613,10 +611,10 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     K.rq_ctl = d_ctl;
     K.done_total = d_ctl + 2 * XTED_RINGS;
     K.stripes = d_st;
-    K.sprog = d_sprog;
-    K.nstripes = (int32_t)nstripes;
+    K.nstriped = (int32_t)nstriped;
     K.smap = nstriped > 0 ? (const int32_t *)c->smap.p : nullptr;
-    K.sbuf = nstriped > 0 ? (int32_t *)c->sbuf.p : nullptr;
+    K.sbuf = nstriped > 0 ? (unsigned long long *)c->sbuf.p : nullptr;
+    K.sbuf_words = stripe_buf;
     K.hold_pair = -1;
     c->d_trivial = d_trivial;
     c->plan_dt_elems = hs->dt_elems;

@@ -104,10 +104,9 @@ struct XStripe {       // a striped unit
     int32_t sww;       // columns per thread: a stripe is 256 * sww columns
     int32_t X;         // far columns read across a stripe boundary (exported on every pushed row)
     int32_t w, R;      // width (one segment) and rows
-    int32_t prog_off;  // its K progress words
-    int32_t pair;
+    int32_t pair, pad;
     int64_t map_off;   // its export map (w ints): column -> export index, or -1
-    int64_t buf_off;   // carries [K][R], first columns [K][R], exports [R][X]
+    int64_t buf_off;   // carries [K][R], first columns [K][R], exports [R][X]: 64-bit tagged words
 };
 #define XTED_TASK_HALF 0x40000000u  // units run by the block's two halves (4 warps each)
 #define XTED_HALF_MAX 1024          // widest chunk one half block holds in registers (8 per thread)
@@ -189,12 +188,12 @@ struct XKernelParams {
     int32_t *error_info;  // [4] diagnostics of the first error
     uint64_t timeout_ns;  // bound on every idle wait
     unsigned long long *trace; // optional, 4 words per task: claim ns, start ns, end ns, info
-    // ---- striped units (nstripes = 0: none) ----
+    // ---- striped units (nstriped = 0: none) ----
     const XStripe *stripes;
-    int32_t *sprog;        // [nstripes] rows each stripe has finished (flat over its unit's keyroots), zeroed per run
-    const int32_t *smap;   // export maps
-    int32_t *sbuf;         // carries, first columns, exports
-    int32_t nstripes;
+    const int32_t *smap;        // export maps
+    unsigned long long *sbuf;   // carries, first columns, exports (zeroed per run)
+    int64_t sbuf_words;
+    int32_t nstriped;
     // ---- serving session (serve = 1); a batch launch leaves these zero ----
     int32_t serve;
     int32_t serve_pairs;    // pairs per query slot (the corpus size)
