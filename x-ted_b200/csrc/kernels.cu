@@ -292,6 +292,22 @@ __device__ __forceinline__ void issue_row(const int32_t *cnode, int width, const
     if (rec) cp_async8(slot + rec_at, rows + r);
 }
 
+// The same copies with the thread's copy plan held in registers for the whole
+// unit: cpn[j] is the column tree's node of column me + nthr j (nthr = 32 G,
+// G warps), bit j of cpm says that column exists, and the column's padded
+// place in the slot is pbase + (nthr + G) j with pbase = pad(me). Per row this
+// leaves one address and one copy per column.
+template <int W, int G>
+__device__ __forceinline__ void issue_row_planned(const int (&cpn)[W], unsigned cpm, int pbase, const int32_t *dt,
+                                                  int n, const int2 *rows, int r, int32_t *slot, int rec_at,
+                                                  bool rec) {
+    const int32_t *drow = dt + (int64_t)r * n;
+#pragma unroll
+    for (int j = 0; j < W; j++)
+        if ((cpm >> j) & 1u) cp_async4(slot + pbase + (32 * G + G) * j, drow + cpn[j]);
+    if (rec) cp_async8(slot + rec_at, rows + r);
+}
+
 // ---------------------------------------------------------------------------
 // Narrow unit: one warp, chunk width <= 32*W.
 // ---------------------------------------------------------------------------
@@ -315,6 +331,17 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
     for (int k = 0; k < W; k++)
         if ((C.valid >> k) & 1u) cnode[c0 + k] = C.node[k];
     __syncwarp();
+    // this lane's copy plan (nodes of columns lane + 32 j) in registers; the
+    // widest units keep reading it from the shared column table (registers)
+    constexpr bool PLAN = W <= 4;
+    int cpn[W];
+    unsigned cpm = 0;
+#pragma unroll
+    for (int j = 0; j < W && PLAN; j++) {
+        const int c = lane + 32 * j;
+        cpn[j] = c < width ? cnode[c] : 0;
+        if (c < width) cpm |= 1u << j;
+    }
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -351,17 +378,27 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
-            if (r >= i0)
-                issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, lane,
-                             32, lane == 0);
+            if (r >= i0) {
+                if (PLAN)
+                    issue_row_planned<W, 1>(cpn, cpm, lane, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT,
+                                            NARROW_ROW, lane == 0);
+                else
+                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW,
+                                 lane, 32, lane == 0);
+            }
             cp_async_commit();
         }
         for (int i = imax - 1; i >= i0; i--) {
             {
                 const int r = i - (PF - 1);
-                if (r >= i0)
-                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW,
-                                 lane, 32, lane == 0);
+                if (r >= i0) {
+                    if (PLAN)
+                        issue_row_planned<W, 1>(cpn, cpm, lane, dt_in, n, rows, r,
+                                                ring + (r & (PF - 1)) * NARROW_SLOT, NARROW_ROW, lane == 0);
+                    else
+                        issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * NARROW_SLOT,
+                                     NARROW_ROW, lane, 32, lane == 0);
+                }
                 cp_async_commit();
             }
             cp_async_wait<PF - 1>();
@@ -474,6 +511,18 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 #pragma unroll
     for (int k = 0; k < W; k++)
         if ((C.valid >> k) & 1u) cnode[c0 + k] = C.node[k];
+    group_sync<G>(gid);  // the whole column table is written
+    // this thread's copy plan (nodes of columns gtid + 32 G j) in registers;
+    // the widest units keep reading it from the shared column table
+    constexpr bool PLAN = W <= 4;
+    int cpn[W];
+    unsigned cpm = 0;
+#pragma unroll
+    for (int j = 0; j < W && PLAN; j++) {
+        const int c = gtid + 32 * G * j;
+        cpn[j] = c < width ? cnode[c] : 0;
+        if (c < width) cpm |= 1u << j;
+    }
     {
         const int e = count_ends<W>(C);
         const int incl = warp_prefix_sum(e, lane);
@@ -501,9 +550,14 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
-            if (r >= i0)
-                issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
-                             gtid == 0);
+            if (r >= i0) {
+                if (PLAN)
+                    issue_row_planned<W, G>(cpn, cpm, gtid + warp, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT,
+                                            GROW, gtid == 0);
+                else
+                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
+                                 gtid == 0);
+            }
             cp_async_commit();
         }
         cp_async_wait<PF - 2>();
@@ -511,9 +565,14 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
         for (int i = imax - 1; i >= i0; i--) {
             {
                 const int r = i - (PF - 1);
-                if (r >= i0)
-                    issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid, 32 * G,
-                             gtid == 0);
+                if (r >= i0) {
+                    if (PLAN)
+                        issue_row_planned<W, G>(cpn, cpm, gtid + warp, dt_in, n, rows, r,
+                                                ring + (r & (PF - 1)) * GSLOT, GROW, gtid == 0);
+                    else
+                        issue_row<W>(cnode, width, dt_in, n, rows, r, ring + (r & (PF - 1)) * GSLOT, GROW, gtid,
+                                     32 * G, gtid == 0);
+                }
                 cp_async_commit();
             }
             const int32_t *slot = ring + (i & (PF - 1)) * GSLOT;
@@ -655,12 +714,15 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                            const int32_t *expmap, unsigned long long *CR, unsigned long long *FC,
                            unsigned long long *E) {
     constexpr int G = XTED_WARPS, SW = XTED_CTA_THREADS * W;  // stripe width: W columns per thread
-    constexpr int GROW = 256 * G + 8 * G;  // padded row of the stack cache
-    // the ring holds stripe rows only (SW columns): narrow stripes keep more
-    // rows in flight in the same shared memory (8 at 512 columns, 4 at 1,024)
+    // the ring and the stack window hold stripe rows only (SW columns):
+    // narrow stripes keep more rows in the same shared memory (at 512 columns
+    // 8 rows in flight and a 32-row window of the far-row stack, so a deep
+    // table rarely reloads a stack row from global memory)
     constexpr int SROW = SW + SW / 32, SSLOT = SROW + 8;
     constexpr int PF = 8 * SSLOT <= RING_INTS ? 8 : 4 * SSLOT <= RING_INTS ? 4 : 2;
     static_assert(PF * SSLOT <= RING_INTS, "stripe ring");
+    constexpr int SC = 32 * SROW <= CACHE_INTS ? 32 : 16 * SROW <= CACHE_INTS ? 16 : XTED_STACK_CACHE;
+    static_assert(SC * SROW <= CACHE_INTS, "stripe stack window");
     const int gtid = threadIdx.x, lane = gtid & 31, warp = gtid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
@@ -669,12 +731,16 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const bool right = s + 1 < K, left = s > 0;
     const int lc0 = gtid * W, c0 = C0 + lc0;  // this thread's first column: local, in the segment
     const int pbase = pad(lc0);
-    const bool deep = run.depth > XTED_STACK_CACHE;
+    const bool deep = run.depth > SC;
     const int stack_rows = P.stack_rows;
     const Costs KC = costs_of<UC>(P);
     Cols<W> C;
     load_cols<W>(P, pr, ch, c0, C, w - 1);
-    unsigned expm = 0;  // this thread's columns that stripes to the left read as far columns
+    // this thread's columns that stripes to the left read as far columns, and
+    // the export index of the first of them (exports are numbered in column
+    // order, so the k-th is ebase + the exported columns before it)
+    unsigned expm = 0;
+    int ebase = -1;
 #pragma unroll
     for (int k = 0; k < W; k++) {
         const int c = c0 + k;
@@ -693,7 +759,11 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             if (f >= w) C.fidx[k] = pad(lc0 + k);     // the border: a tree-path column (rowfar)
             else if (f < C1) C.fidx[k] = pad(f - C0);
             else C.fidx[k] = -1 - __ldcg(&expmap[f]);  // exported by a stripe to the right
-            if (__ldcg(&expmap[c]) >= 0) expm |= 1u << k;
+            const int ex = __ldcg(&expmap[c]);
+            if (ex >= 0) {
+                if (ebase < 0) ebase = ex;
+                expm |= 1u << k;
+            }
         }
     }
     __syncthreads();  // the block's previous unit is done with cnode and S
@@ -701,6 +771,19 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     for (int k = 0; k < W; k++)
         if ((C.valid >> k) & 1u) cnode[lc0 + k] = C.node[k];
     set_keys<W>(C, c0, 0, KC.ins);  // one segment: key = ins * segment column
+    // this thread's copy plan: one segment, so column c is node j0 + C0 + c
+    constexpr bool PLAN = W <= 4;
+    int cpn[W];
+    unsigned cpm = 0;
+    {
+        const int jc = P.krd[ch.k_lo] + C0;
+#pragma unroll
+        for (int j = 0; j < W && PLAN; j++) {
+            const int c = gtid + SW * j / W;  // columns gtid + 256 j
+            cpn[j] = jc + c;
+            if (c < C1 - C0) cpm |= 1u << j;
+        }
+    }
     const int n = pr.n;
     const int32_t *dt_in = P.dt + pr.dt_off;
     int32_t *dt_out = P.dt + pr.dt_off;
@@ -722,9 +805,14 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
 #pragma unroll
         for (int q = 0; q < PF - 1; q++) {
             const int r = imax - 1 - q;
-            if (r >= i0)
-                issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT, SROW, gtid, 32 * G,
-                             gtid == 0);
+            if (r >= i0) {
+                if (PLAN)
+                    issue_row_planned<W, G>(cpn, cpm, gtid + warp, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT,
+                                            SROW, gtid == 0);
+                else
+                    issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT, SROW, gtid,
+                                 32 * G, gtid == 0);
+            }
             cp_async_commit();
         }
         cp_async_wait<PF - 2>();
@@ -732,9 +820,14 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
         for (int i = imax - 1; i >= i0; i--, tflat++) {
             {
                 const int r = i - (PF - 1);
-                if (r >= i0)
-                    issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT, SROW, gtid, 32 * G,
-                             gtid == 0);
+                if (r >= i0) {
+                    if (PLAN)
+                        issue_row_planned<W, G>(cpn, cpm, gtid + warp, dt_in, n, rows, r,
+                                                ring + (r & (PF - 1)) * SSLOT, SROW, gtid == 0);
+                    else
+                        issue_row<W>(cnode, C1 - C0, dt_in, n, rows, r, ring + (r & (PF - 1)) * SSLOT, SROW, gtid,
+                                     32 * G, gtid == 0);
+                }
                 cp_async_commit();
             }
             // thread 0: the right neighbour's carry and first column of this
@@ -753,7 +846,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             int mine;
             if (!trow) {
                 // forest row: far values from the stack top, or exported by the stripe that owns them
-                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (SC - 1)) * SROW;
                 const int efl = tbase + (imax - 1 - (ro + 1));  // flat row of the far row
                 const unsigned long long *erow = E + (int64_t)efl * X;
                 const int32_t *cur = slot + pbase;
@@ -819,7 +912,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (int64_t)(sp - 1) * SW + lc0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * GROW + pbase;
+                    int32_t *dst = cache + ((sp - 1) & (SC - 1)) * SROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = src[k];
                     lo = sp - 1;
@@ -827,7 +920,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * GROW + pbase;
+                    int32_t *dst = cache + (sp & (SC - 1)) * SROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = prev[k];
                     if (deep) {
@@ -842,10 +935,11 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                     unsigned long long *erow = E + (int64_t)tflat * X;
 #pragma unroll
                     for (int k = 0; k < W; k++)
-                        if ((expm >> k) & 1u) st_tagged(erow + __ldcg(&expmap[c0 + k]), (unsigned)tflat + 1, prev[k]);
+                        if ((expm >> k) & 1u)
+                            st_tagged(erow + ebase + __popc(expm & ((1u << k) - 1)), (unsigned)tflat + 1, prev[k]);
                 }
                 sp++;
-                if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
+                if (sp - lo > SC) lo = sp - SC;
             }
             // the next row's diagonal at C1: the right neighbour's first column of this row
             if (gtid == 0 && right) S.first[G] = fc_next;
