@@ -83,9 +83,10 @@ typedef struct xted_opts {
     int64_t mem_limit;      /* device bytes the context may hold (0 = none) */
     int64_t stripe_min_cells; /* a table whose column segment is wider than
                                2,048 and whose unit has at least this many
-                               cells runs in column stripes (512 to 2,048
-                               columns) on up to 64 blocks at once
-                               (0 = 2^20; < 0: one block)                   */
+                               cells runs in column stripes of 512 columns
+                               (wider past 128 stripes), each stripe a task
+                               that any block may run (0 = 2^20; < 0: the
+                               whole table on one block)                    */
     int32_t cost_del;       /* edit costs (integers >= 0): deleting a node of */
     int32_t cost_ins;       /* the first tree, inserting a node of the second */
     int32_t cost_ren;       /* tree, and mapping two nodes whose labels differ
