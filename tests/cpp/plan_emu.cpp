@@ -277,7 +277,7 @@ int main(int argc, char **argv) {
             std::vector<int> order((size_t)X.ntasks);
             std::iota(order.begin(), order.end(), 0);
             std::shuffle(order.begin(), order.end(), g);
-            std::vector<int> stripe_seen;  // per striped unit of the entry: stripes seen (bit mask of the first 64)
+            int lone_seen = 0;
             for (int k : order) {
                 const XTask &t = H.tasks[(size_t)(X.task_off + k)];
                 if (t.pair != E.pair || t.entry != e) FAIL("task of another entry in the range");
@@ -322,9 +322,9 @@ int main(int argc, char **argv) {
                 for (int u = 0; u < nu && !g_table; u++) {
                     const int w = H.chunks[(size_t)H.units[(size_t)(t.unit_lo + u)].chunk].width;
                     if (half && (w <= nw || w > XTED_HALF_MAX || w > hw)) FAIL("half unit of width %d", w);
-                    // a level's last half-width unit, alone in its task, runs on the whole block
-                    const bool lone = E.nhalf % level_bundle_half(E.nhalf) == 1;
-                    if (full && w <= XTED_HALF_MAX && w > nw && hw >= w && !lone)
+                    // a half-width unit alone in its task runs on the whole block: at most the
+                    // last of the paired units of long runs and the last of the bundled ones
+                    if (full && w <= XTED_HALF_MAX && w > nw && hw >= w && ++lone_seen > 2)
                         FAIL("whole-block unit of width %d", w);
                 }
                 const DPair &q = H.pairs[(size_t)t.pair];

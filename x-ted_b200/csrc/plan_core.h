@@ -416,31 +416,33 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     const DOTree &A = C.ot[2 * q.ta + q.o], &B = C.ot[2 * q.tb + q.o];
     const DDepth *da = C.depths + A.depth_base, *db = C.depths + B.depth_base;
     const int d = E.level;
-    int64_t wide = 0, narrow = 0, half = 0, nlong = 0, nstriped = 0, nstripes = 0;
+    int64_t wide = 0, narrow = 0, half = 0, nlong = 0, nstriped = 0, nstripes = 0, nhlong = 0;
     const int lo = d - B.D > 0 ? d - B.D : 0, hi = A.D < d ? A.D : d;
     int32_t small_max[64];  // longest bundled run per depth (the first 64 depths; more use maxrows)
-    int32_t long_max[64];   // longest run of single-unit narrow tasks per depth
+    int32_t long_max[64];   // longest run of single-unit narrow tasks (or paired half units) per depth
+    int32_t half_max[64];   // longest run of bundled half units per depth
     for (int al = lo; al <= hi; al++) {
         const DDepth &ra = da[al], &cb = db[d - al];
         const int64_t nr = ra.run_hi - ra.run_lo;
-        int64_t nbig = 0, nl = 0;
-        int32_t sm = 0, lm = 0;
-        if (cb.nnarrow > 0)
+        int64_t nbig = 0, nl = 0, nlh = 0;
+        int32_t sm = 0, lm = 0, hm = 0;
+        if (cb.nnarrow > 0 || cb.nhalf > 0)
             for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
                 const int32_t rows = C.runs[r].rows;
-                if (big_run(C, r)) {
-                    nbig++;
-                } else if (long_run_rows(rows)) {
-                    nl++;
-                    if (rows > lm) lm = rows;
-                } else if (rows > sm) {
-                    sm = rows;
-                }
+                const bool lr = long_run_rows(rows);
+                if (lr && rows > lm) lm = rows;
+                if (lr) nlh++;
+                else if (rows > hm) hm = rows;
+                if (big_run(C, r)) nbig++;
+                else if (lr) nl++;
+                else if (rows > sm) sm = rows;
             }
         if (al - lo < 64) {
             small_max[al - lo] = sm;
             long_max[al - lo] = lm;
+            half_max[al - lo] = hm;
         }
+        nhlong += nlh * cb.nhalf;
         wide += nr * cb.nwide + nbig * cb.nnarrow;
         half += nr * cb.nhalf;
         if (C.stripe_min_cells > 0 && cb.maxw_w > XTED_STRIPE_MIN_WIDTH) {
@@ -476,8 +478,11 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
             }
         }
         if (cb.nhalf > 0) {
-            const double eh = rounds_h * ra.maxrows * row_cost_half(cb.maxw_h);
+            const int32_t hm = al - lo < 64 ? half_max[al - lo] : ra.maxrows;
+            const int32_t lm = al - lo < 64 ? long_max[al - lo] : ra.maxrows;
+            const double eh = rounds_h * hm * row_cost_half(cb.maxw_h), el = lm * row_cost_half(cb.maxw_h);
             if (eh > e) e = eh;
+            if (el > e) e = el;
         }
         if (cb.nwide > 0) {
             const double ew = ra.maxrows * row_cost_est(true, cb.maxw_w);
@@ -491,7 +496,9 @@ XT_HD inline void level_count(const LevelCtx &C, DLevel &E, double *est_out) {
     E.nntasks = (int32_t)((narrow - nlong + bundle - 1) / bundle + nlong);
     E.nstriped = (int32_t)nstriped;
     E.nstripes = (int32_t)nstripes;
-    E.ntasks = (int32_t)(wide - nstriped + nstripes + E.nntasks + (half + bundle_h - 1) / bundle_h);
+    // half units of long runs go two to a task (one per half), the others in bundles
+    E.ntasks = (int32_t)(wide - nstriped + nstripes + E.nntasks + (nhlong + 1) / 2 +
+                         (half - nhlong + bundle_h - 1) / bundle_h);
     *est_out = est;
 }
 
@@ -552,11 +559,31 @@ XT_HD inline void level_fill(const LevelCtx &C, const DLevel &E, XUnit *units, X
             }
         }
     }
+    // half-block units: those of runs over XTED_LONG_RUN_ROWS rows two to a task
+    // (one per half, so the level's longest units do not queue behind each
+    // other in one block), then the rest in bundles
     const int32_t per_half = level_bundle_half(E.nhalf);
     bundle = 0;
     for (int al = hi; al >= lo; al--) {
         const DDepth &ra = da[al], &cb = db[d - al];
         for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            if (!long_run_rows(C.runs[r].rows)) continue;
+            for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nhalf; c++) {
+                if (bundle == 0) bundle_lo = u;
+                units[u++] = XUnit{r, c};
+                if (++bundle == 2) {
+                    tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_HALF | 2u, bundle_lo};
+                    bundle = 0;
+                }
+            }
+        }
+    }
+    if (bundle > 0) tasks[t++] = XTask{E.pair, E.entry, XTED_TASK_WIDE | 1u, bundle_lo};  // a lone one: the whole block
+    bundle = 0;
+    for (int al = hi; al >= lo; al--) {
+        const DDepth &ra = da[al], &cb = db[d - al];
+        for (int32_t r = ra.run_lo; r < ra.run_hi; r++) {
+            if (long_run_rows(C.runs[r].rows)) continue;
             for (int32_t c = cb.chunk_lo + cb.nnarrow; c < cb.chunk_lo + cb.nnarrow + cb.nhalf; c++) {
                 if (bundle == 0) bundle_lo = u;
                 units[u++] = XUnit{r, c};
