@@ -4,11 +4,12 @@
 // for every depth level fetches, sizes, sorts and bins tables with host
 // round trips (X-TED_CPU/TED.cpp:163-166, X-TED_GPU/parallel_X_TED.cu:184-224,
 // 304-387). Here the raw trees go up once and everything else is built on the
-// device, one thread per tree / oriented tree / pair / (pair, level):
+// device, one warp per tree / oriented tree, one thread per pair / (pair, level):
 //
-//   k_tree_basic_warp  sizes, depths, parents, keyroot-size sums (both decompositions), a warp per tree
-//   k_orient       per orientation: node records, kdepth, keyroots by depth,
-//                  column-list positions, row runs, column chunks
+//   k_tree_basic_warp  sizes, depths, parents, keyroot-size sums (both decompositions)
+//   k_orient_warp  per orientation: node records, kdepth, keyroots by depth,
+//                  column-list positions, row runs, column chunks (the records
+//                  plan_core.h's orient_tree builds for the host planners)
 //   k_pair_setup   decomposition choice, level count
 //   k_level_*      unit/task counts and estimates per (pair, level), ready-
 //                  queue priority, then the units and tasks themselves
@@ -45,7 +46,7 @@ __global__ void k_tree_basic_warp(PlanPools P, DTree *trees_out) {
     const int n = T.n;
     const int32_t *off = P.raw + T.raw + n, *idx = P.raw + T.raw + 2 * n + 1;
     int32_t *size = P.size + T.nbase, *depth = P.depth + T.nbase, *par = P.parent + T.nbase;
-    int32_t *jump = P.opar + 2 * (int64_t)T.nbase;  // scratch: this tree's orientation pool, unused until k_orient
+    int32_t *jump = P.opar + 2 * (int64_t)T.nbase;  // scratch: this tree's orientation pool, unused until k_orient_warp
     T.S[0] = T.S[1] = 0;
     if (n > 0) {
         for (int v = lane; v < n; v += 32) {
@@ -115,9 +116,253 @@ __global__ void k_tree_basic_warp(PlanPools P, DTree *trees_out) {
     if (lane == 0) trees_out[t] = T;
 }
 
-__global__ void k_orient(PlanPools P) {
-    const int ot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ot < 2 * P.ntrees) orient_tree(P, ot);
+__device__ __forceinline__ int warp_incl_sum(int v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += o;
+    }
+    return v;
+}
+
+// One warp per oriented tree: the same records as orient_tree (plan_core.h,
+// which the host planners run), with its passes spread over the lanes (a
+// thread per oriented tree took 10 ms for the 8,192 trees of the 4,096-pair
+// batch, its passes waiting on one global load after another; this takes 1.8).
+//   * node records and the previous-node-is-leaf flags: one node per lane;
+//   * A(x), the keyroots on x's root path (x included): a prefix sum over
+//     preorder of +1 at each keyroot and -1 just past its subtree;
+//   * keyroot depth kd(u) = (max of A over u's subtree) - A(u), the height of u
+//     among the keyroots nested in it: each lane scans the subtrees of its
+//     keyroots (the keyroot-size sum of the tree in all);
+//   * keyroots grouped by depth in preorder: a counting sort, 32 nodes at a time,
+//     lanes of one depth ranked by lane;
+//   * row runs and column chunks per depth: sizes and column positions loaded
+//     and summed 32 keyroots at a time, the greedy packing then decided by the
+//     whole warp from shuffled sizes (every lane holds the same packing state).
+__global__ void k_orient_warp(PlanPools P) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int ot = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (ot >= 2 * P.ntrees) return;  // whole warps
+    const int t = ot >> 1, o = ot & 1;
+    const DTree T = P.trees[t];
+    const int n = T.n;
+    DOTree O;
+    O.n = n;
+    O.node_base = 2 * T.nbase + o * n;
+    O.depth_base = 2 * (T.nbase + t) + o * (n + 1);
+    O.D = -1;
+    O.maxka = 0;
+    O.maxw_wide = 0;
+    O.S = T.S[o];
+    if (n == 0) {
+        if (lane == 0) P.otrees[ot] = O;
+        return;
+    }
+    const int32_t *lab = P.raw + T.raw;
+    const int32_t *off = P.raw + T.raw + n;
+    const int32_t *idx = P.raw + T.raw + 2 * n + 1;
+    const int32_t *size = P.size + T.nbase, *depth = P.depth + T.nbase, *par = P.parent + T.nbase;
+    int2 *node = P.node + O.node_base;
+    int32_t *opar = P.opar + O.node_base, *okd = P.okd + O.node_base, *oka = P.oka + O.node_base;
+    // node records in this orientation
+    for (int v = lane; v < n; v += 32) {
+        const int32_t u = o ? mirror_id(v, n, size, depth) : v;
+        bool kr = true;
+        if (v > 0) {
+            const int32_t p = par[v];
+            kr = o ? idx[off[p]] != v : idx[off[p + 1] - 1] != v;
+            opar[u] = o ? mirror_id(p, n, size, depth) : p;
+        } else {
+            opar[u] = -1;
+        }
+        node[u].x = lab[v];
+        node[u].y = (int32_t)((uint32_t)(u + size[v] - 1) | (kr ? XTED_ROW_ISKR : 0u));
+        oka[u] = 0;
+    }
+    __syncwarp();
+    for (int u = 1 + lane; u < n; u += 32) {
+        const int32_t prev_orl = node[u - 1].y & XTED_ROW_ORL_MASK;  // (its flag bits may change meanwhile)
+        if (prev_orl == u - 1) node[u].y = (int32_t)((uint32_t)node[u].y | XTED_ROW_PREVLEAF);
+    }
+    // A(x): +1 at a keyroot, -1 just past its subtree, summed over preorder
+    for (int u = lane; u < n; u += 32) {
+        const int32_t y = node[u].y;
+        if (y & XTED_ROW_ISKR) {
+            atomicAdd(&oka[u], 1);
+            const int e = (y & XTED_ROW_ORL_MASK) + 1;
+            if (e < n) atomicSub(&oka[e], 1);
+        }
+    }
+    __syncwarp();
+    int carry = 0, maxa = 1;
+    for (int base = 0; base < n; base += 32) {
+        const int x = base + lane;
+        const int dv = x < n ? __ldcg(&oka[x]) : 0;
+        const int a = carry + warp_incl_sum(dv, lane);
+        if (x < n) {
+            oka[x] = a;
+            maxa = max(maxa, a);
+        }
+        carry = __shfl_sync(FULL, a, 31);
+    }
+    for (int d = 16; d > 0; d >>= 1) maxa = max(maxa, __shfl_xor_sync(FULL, maxa, d));
+    O.maxka = maxa;
+    __syncwarp();
+    // keyroot depths
+    for (int u = lane; u < n; u += 32) {
+        const int32_t y = node[u].y;
+        int kd = -1;
+        if (y & XTED_ROW_ISKR) {
+            const int e = y & XTED_ROW_ORL_MASK, au = oka[u];
+            int m = au;
+            for (int x = u + 1; x <= e; x++) m = max(m, oka[x]);
+            kd = m - au;
+        }
+        okd[u] = kd;
+    }
+    __syncwarp();
+    const int D = okd[0];  // the root is a keyroot
+    O.D = D;
+    // keyroots grouped by depth (counting sort, preorder inside a depth)
+    DDepth *dep = P.depths + O.depth_base;
+    for (int d = lane; d <= D; d += 32) {
+        dep[d].krd_lo = 0;
+        dep[d].krd_hi = 0;
+    }
+    __syncwarp();
+    for (int u = lane; u < n; u += 32)
+        if (okd[u] >= 0) atomicAdd(&dep[okd[u]].krd_hi, 1);
+    __syncwarp();
+    carry = O.node_base;
+    for (int base = 0; base <= D; base += 32) {
+        const int d = base + lane;
+        const int c = d <= D ? __ldcg(&dep[d].krd_hi) : 0;
+        const int incl = warp_incl_sum(c, lane);
+        if (d <= D) {
+            dep[d].krd_lo = carry + incl - c;
+            dep[d].krd_hi = carry + incl - c;  // fill cursor
+        }
+        carry += __shfl_sync(FULL, incl, 31);
+    }
+    __syncwarp();
+    const unsigned below = (1u << lane) - 1u;
+    for (int base = 0; base < n; base += 32) {
+        const int u = base + lane;
+        const int kd = u < n ? okd[u] : -1;
+        const unsigned same = __match_any_sync(FULL, kd);  // lanes holding keyroots of this depth
+        if (kd >= 0) {
+            const int leader = __ffs(same) - 1;
+            int at = 0;
+            if (lane == leader) {
+                at = dep[kd].krd_hi;
+                dep[kd].krd_hi = at + __popc(same);
+            }
+            at = __shfl_sync(same, at, leader);
+            P.krd[at + __popc(same & below)] = u;
+        }
+        __syncwarp();
+    }
+    // column-list positions, row runs and chunks per depth
+    int run_rows, nw, hw;
+    tree_granularity(P, n, &run_rows, &nw, &hw);
+    const int group_w = nw > 0 ? nw : XTED_NARROW_MAX;
+    const int half_w = hw > nw ? (hw < XTED_HALF_MAX ? hw : XTED_HALF_MAX) : nw;
+    int32_t run_cur = O.node_base, chunk_cur = O.node_base;
+    for (int d = 0; d <= D; d++) {
+        DDepth dd = dep[d];  // krd_lo, krd_hi
+        const int klo = dd.krd_lo, khi = dd.krd_hi;
+        // runs
+        dd.run_lo = run_cur;
+        dd.maxrows = 0;
+        int pos = 0, r_lo = -1, r_hi = -1, r_rows = 0;
+        for (int kb = klo; kb < khi; kb += 32) {
+            const int k = kb + lane;
+            int sz = 0;
+            if (k < khi) {
+                const int32_t u = P.krd[k];
+                sz = (node[u].y & XTED_ROW_ORL_MASK) - u + 1;
+            }
+            const int incl = warp_incl_sum(sz, lane);
+            if (k < khi) P.cumw[k] = pos + incl - sz;
+            pos += __shfl_sync(FULL, incl, 31);
+            const int cnt = min(32, khi - kb);
+            for (int j = 0; j < cnt; j++) {
+                const int szj = __shfl_sync(FULL, sz, j);
+                if (r_lo >= 0 && r_rows + szj > run_rows) {
+                    if (r_rows > dd.maxrows) dd.maxrows = r_rows;
+                    if (lane == 0) P.runs[run_cur] = XRun{r_lo, r_hi, r_rows, d};
+                    run_cur++;
+                    r_lo = -1;
+                    r_rows = 0;
+                }
+                if (r_lo < 0) r_lo = kb + j;
+                r_hi = kb + j + 1;
+                r_rows += szj;
+            }
+        }
+        if (r_lo >= 0) {
+            if (r_rows > dd.maxrows) dd.maxrows = r_rows;
+            if (lane == 0) P.runs[run_cur] = XRun{r_lo, r_hi, r_rows, d};
+            run_cur++;
+        }
+        dd.run_hi = run_cur;
+        // chunks: three passes, narrow chunks first, then half-block ones, then whole-block ones
+        dd.chunk_lo = chunk_cur;
+        dd.nnarrow = dd.nwide = dd.nhalf = 0;
+        dd.maxw_n = dd.maxw_w = dd.maxw_h = 0;
+        for (int pass = 0; pass < 3; pass++) {
+            int c_lo = -1, c_w = 0, c_n = 0;
+            bool done = false;
+            for (int kb = klo; kb <= khi && !done; kb += 32) {
+                const int k = kb + lane;
+                int w = 0;
+                if (k < khi) {
+                    const int32_t u = P.krd[k];
+                    w = (node[u].y & XTED_ROW_ORL_MASK) - u + 1;
+                }
+                const int cnt = min(32, khi + 1 - kb);
+                for (int j = 0; j < cnt; j++) {
+                    const int kk = kb + j;
+                    const int wj = __shfl_sync(FULL, w, j);
+                    const bool flush = c_n > 0 && (kk == khi || c_w + wj > group_w);
+                    if (flush) {
+                        const int kind = c_w <= nw ? 0 : (c_w <= half_w ? 1 : 2);
+                        if (kind == pass) {
+                            if (lane == 0) P.chunks[chunk_cur] = XChunk{c_lo, c_w, d, c_n};
+                            chunk_cur++;
+                            if (kind == 2) {
+                                dd.nwide++;
+                                if (c_w > dd.maxw_w) dd.maxw_w = c_w;
+                            } else if (kind == 1) {
+                                dd.nhalf++;
+                                if (c_w > dd.maxw_h) dd.maxw_h = c_w;
+                            } else {
+                                dd.nnarrow++;
+                                if (c_w > dd.maxw_n) dd.maxw_n = c_w;
+                            }
+                        }
+                        c_lo = -1;
+                        c_w = 0;
+                        c_n = 0;
+                    }
+                    if (kk == khi) {
+                        done = true;
+                        break;
+                    }
+                    if (c_n == 0) c_lo = kk;  // first segment (keyroot pool index)
+                    c_w += wj;
+                    c_n += 1;
+                }
+            }
+        }
+        if (dd.maxw_h > O.maxw_wide) O.maxw_wide = dd.maxw_h;
+        if (dd.maxw_w > O.maxw_wide) O.maxw_wide = dd.maxw_w;
+        if (lane == 0) dep[d] = dd;
+        __syncwarp();
+    }
+    if (lane == 0) P.otrees[ot] = O;
 }
 
 __global__ void k_pair_setup(const DTree *trees, const DOTree *ot, const int32_t *pair_trees, int orientation,
@@ -488,7 +733,7 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     const int BS = 128;
     cudaMemsetAsync(d_sum, 0, sizeof(Summary), s);
     k_tree_basic_warp<<<blocks_for(32 * (int64_t)T, BS), BS, 0, s>>>(P, d_trees);
-    k_orient<<<blocks_for(2 * (int64_t)T, BS), BS, 0, s>>>(P);
+    k_orient_warp<<<blocks_for(64 * (int64_t)T, BS), BS, 0, s>>>(P);
     k_pair_setup<<<blocks_for(npairs, BS), BS, 0, s>>>(d_trees, P.otrees, d_pt, c->opts.orientation, npairs,
                                                        d_pairs, d_L, d_cells);
     k_scan64<<<1, 1024, 0, s>>>(d_L, nullptr, npairs, d_Ls);
