@@ -325,7 +325,12 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
     const int width = ch.width;
     const Costs K = costs_of<UC>(P);
     Cols<W> C;
-    load_cols<W>(P, pr, ch, c0, C, XTED_NARROW_MAX - 1);
+    // the stack window holds rows of 32 W columns (padded: 33 W ints), so
+    // narrower units keep more rows of it in the warp's shared memory
+    constexpr int CROW = 33 * W, SC0 = XTED_STACK_CACHE * NARROW_ROW / CROW;
+    constexpr int SC = SC0 >= 32 ? 32 : SC0 >= 16 ? 16 : XTED_STACK_CACHE;
+    static_assert(SC * CROW <= XTED_STACK_CACHE * NARROW_ROW, "narrow stack window");
+    load_cols<W>(P, pr, ch, c0, C, 32 * W - 1);
     __syncwarp();  // the previous unit's copies have drained (cp_async_wait<0> at its end)
 #pragma unroll
     for (int k = 0; k < W; k++)
@@ -356,7 +361,7 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
     constexpr int PF = XTED_PREFETCH;
     // a table at keyroot depth d nests at most d stack rows (nested keyroots have
     // strictly smaller depths), so only deep runs need the global copy of the stack
-    const bool deep = run.depth > XTED_STACK_CACHE;
+    const bool deep = run.depth > SC;
     const int stack_rows = P.stack_rows;
 
     for (int kr = kr_start < 0 ? run.kr_lo : kr_start; kr < run.kr_hi; kr++) {
@@ -411,7 +416,7 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
             int loc[W];
             int mine;
             if (!trow) {
-                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * NARROW_ROW;
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (SC - 1)) * CROW;
                 mine = row_forest<W>(C, prev, slot + pbase, top, bord + K.ins, (imax - ro - 1) * K.del, K.del, loc);
             } else {
                 const int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
@@ -433,7 +438,7 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * NARROW_ROW + pbase;
+                    int32_t *dst = cache + ((sp - 1) & (SC - 1)) * CROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = src[k];
                     lo = sp - 1;
@@ -443,7 +448,7 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
                 if (sp < stack_rows) {
                     // whole rows: only far columns are ever read back, and the
                     // others (inert ones included) hold this row's bounded values
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * NARROW_ROW + pbase;
+                    int32_t *dst = cache + (sp & (SC - 1)) * CROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = prev[k];
                     if (deep) {
@@ -455,7 +460,7 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
                     set_error(P, XTED_ENOMEM, 1, sp, stack_rows);
                 }
                 sp++;
-                if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
+                if (sp - lo > SC) lo = sp - SC;
             }
             __syncwarp();
         }
@@ -502,11 +507,16 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
     const int width = ch.width;
     const int pbase = pad(c0);  // pad(c0 + k) == pbase + k for k < W (W divides 32)
     constexpr int PF = XTED_PREFETCH;
-    const bool deep = run.depth > XTED_STACK_CACHE;  // see run_narrow
+    // stack window rows of 32 G W columns (33 G W ints padded): narrower units
+    // keep more rows of it in the group's shared memory
+    constexpr int CROW = 33 * G * W, SC0 = XTED_STACK_CACHE * GROW / CROW;
+    constexpr int SC = SC0 >= 32 ? 32 : SC0 >= 16 ? 16 : XTED_STACK_CACHE;
+    static_assert(SC * CROW <= XTED_STACK_CACHE * GROW, "group stack window");
+    const bool deep = run.depth > SC;  // see run_narrow
     const int stack_rows = P.stack_rows;
     const Costs K = costs_of<UC>(P);
     Cols<W> C;
-    load_cols<W>(P, pr, ch, c0, C, 256 * G - 1);
+    load_cols<W>(P, pr, ch, c0, C, 32 * G * W - 1);
     group_sync<G>(gid);  // the group's previous unit is done with cnode and S
 #pragma unroll
     for (int k = 0; k < W; k++)
@@ -583,7 +593,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
             int loc[W];
             int mine;
             if (!trow) {
-                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (XTED_STACK_CACHE - 1)) * GROW;
+                const int32_t *top = cache + ((sp > 0 ? sp - 1 : 0) & (SC - 1)) * CROW;
                 mine = row_forest<W>(C, prev, slot + pbase, top, bord + K.ins, (imax - ro - 1) * K.del, K.del, loc);
             } else {
                 int dnext = __shfl_down_sync(FULLMASK, prev[0], 1);
@@ -626,7 +636,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
                 sp--;
                 if (sp > 0 && sp - 1 < lo) {  // the new top left the window: reload it
                     const int32_t *src = stk + (int64_t)(sp - 1) * stride + c0;
-                    int32_t *dst = cache + ((sp - 1) & (XTED_STACK_CACHE - 1)) * GROW + pbase;
+                    int32_t *dst = cache + ((sp - 1) & (SC - 1)) * CROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++)
                         if ((C.far >> k) & 1u) dst[k] = src[k];
@@ -635,7 +645,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
             }
             if (i > i0 && (ri.y & XTED_ROW_PREVLEAF)) {
                 if (sp < stack_rows) {
-                    int32_t *dst = cache + (sp & (XTED_STACK_CACHE - 1)) * GROW + pbase;
+                    int32_t *dst = cache + (sp & (SC - 1)) * CROW + pbase;
 #pragma unroll
                     for (int k = 0; k < W; k++) dst[k] = prev[k];  // whole rows in shared memory, as in run_narrow
                     if (deep) {
@@ -648,7 +658,7 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
                     set_error(P, XTED_ENOMEM, 2, sp, stack_rows);
                 }
                 sp++;
-                if (sp - lo > XTED_STACK_CACHE) lo = sp - XTED_STACK_CACHE;
+                if (sp - lo > SC) lo = sp - SC;
             }
             cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
             group_sync<G>(gid);       // ... and everyone's, the record and the stack push
