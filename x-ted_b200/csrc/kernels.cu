@@ -476,12 +476,12 @@ __device__ int run_narrow(const XKernelParams &P, const XPair &pr, const XUnit &
 // shared memory, with the group's own named barrier.
 // ---------------------------------------------------------------------------
 struct __align__(16) WideShared {
-    int wtot[XTED_WARPS];       // per-warp suffix minima of the current row (16-byte aligned: vector reads)
+    int wtot[XTED_WARPS];       // per-warp suffix minima of the current row
     int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
     int ends[XTED_WARPS];
     int cin;                    // stripes: the right neighbour's carry for the current row
 };
-static_assert(XTED_WARPS == 8, "carry combination reads the warp minima as two int4");
+static_assert(XTED_WARPS <= 32, "the warp minima are read one per lane");
 
 template <int G>
 __device__ __forceinline__ void group_sync(int gid) {
@@ -606,22 +606,10 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
             if (lane == 31) carry = XTED_INF;
             {
-                // minima of the warps to the right: independent vector reads,
-                // then a select-min per warp (no chain of dependent loads)
-                const int4 lo4 = *reinterpret_cast<const int4 *>(&S.wtot[0]);
-                int v[XTED_WARPS] = {lo4.x, lo4.y, lo4.z, lo4.w, 0, 0, 0, 0};
-                if (G > 4) {
-                    const int4 hi4 = *reinterpret_cast<const int4 *>(&S.wtot[4]);
-                    v[4] = hi4.x;
-                    v[5] = hi4.y;
-                    v[6] = hi4.z;
-                    v[7] = hi4.w;
-                }
-                int right = XTED_INF;
-#pragma unroll
-                for (int w = 1; w < G; w++)
-                    if (w > warp) right = min(right, v[w]);
-                carry = min(carry, right);
+                // minimum of the warps to the right: lane w reads warp w's row
+                // minimum, then one warp-wide reduction
+                const int mv = (lane > warp && lane < G) ? S.wtot[lane] : XTED_INF;
+                carry = min(carry, __reduce_min_sync(FULLMASK, mv));
             }
             int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
@@ -896,14 +884,10 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             int carry = __shfl_down_sync(FULLMASK, incl, 1);
             if (lane == 31) carry = XTED_INF;
             {
-                const int4 lo4 = *reinterpret_cast<const int4 *>(&S.wtot[0]);
-                const int4 hi4 = *reinterpret_cast<const int4 *>(&S.wtot[4]);
-                const int v[XTED_WARPS] = {lo4.x, lo4.y, lo4.z, lo4.w, hi4.x, hi4.y, hi4.z, hi4.w};
-                int rmin = S.cin;
-#pragma unroll
-                for (int q = 1; q < G; q++)
-                    if (q > warp) rmin = min(rmin, v[q]);
-                carry = min(carry, rmin);
+                // minimum of the warps to the right (one warp-wide reduction) and
+                // of the stripe to the right
+                const int mv = (lane > warp && lane < G) ? S.wtot[lane] : XTED_INF;
+                carry = min(carry, min(S.cin, __reduce_min_sync(FULLMASK, mv)));
             }
             int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
