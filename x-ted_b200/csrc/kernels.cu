@@ -971,8 +971,9 @@ template <bool UC>
 __device__ int dispatch_narrow(const XKernelParams &P, const XPair &pr, const XUnit &u, int lane, int32_t *stk,
                                int32_t *ring, int32_t *cache, int32_t *cnode, int kr_start,
                                const volatile int *yield) {
+    // Two columns per lane at the least: a one-column row loop would be one more
+    // instantiation competing for the instruction cache for little gain.
     const int width = P.chunks[u.chunk].width;
-    if (width <= 32) return run_narrow<1, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
     if (width <= 64) return run_narrow<2, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
     if (width <= 128) return run_narrow<4, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
     return run_narrow<8, UC>(P, pr, u, lane, stk, ring, cache, cnode, kr_start, yield);
@@ -1140,8 +1141,7 @@ __device__ void dispatch_wide(const XKernelParams &P, const XPair &pr, const XUn
                               WideShared &S, int32_t *ring, int32_t *cache, int32_t *cnode) {
     const int width = P.chunks[u.chunk].width;
     const int tid = threadIdx.x;
-    if (width <= 256) run_group<1, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
-    else if (width <= 512) run_group<2, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
+    if (width <= 512) run_group<2, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
     else if (width <= 1024) run_group<4, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
     else if (width <= XTED_WIDE_REG_MAX) run_group<8, XTED_WARPS, UC>(P, pr, u, stk, S, ring, cache, cnode, tid, 0);
     else if (P.chunks[u.chunk].nseg == 1) run_wide_big<UC>(P, pr, u, stk, S, ring);
@@ -1153,8 +1153,7 @@ template <bool UC>
 __device__ void dispatch_half(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                               int32_t *ring, int32_t *cache, int32_t *cnode, int gtid, int gid) {
     const int width = P.chunks[u.chunk].width;
-    if (width <= 128) run_group<1, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
-    else if (width <= 256) run_group<2, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
+    if (width <= 256) run_group<2, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
     else if (width <= 512) run_group<4, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
     else if (width <= XTED_HALF_MAX) run_group<8, 4, UC>(P, pr, u, stk, S, ring, cache, cnode, gtid, gid);
     else if (gtid == 0) set_error(P, XTED_EINVAL, 6, width, 0);
