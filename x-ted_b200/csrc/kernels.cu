@@ -480,6 +480,7 @@ struct __align__(16) WideShared {
     int first[XTED_WARPS + 1];  // prev[0] of lane 0 of each warp (cross-warp diagonal)
     int ends[XTED_WARPS];
     int cin;                    // stripes: the right neighbour's carry for the current row
+    int cinb[2], fcb[2];        // pipelined stripes: its carry and first column, by flat-row parity
 };
 static_assert(XTED_WARPS <= 32, "the warp minima are read one per lane");
 
@@ -678,6 +679,13 @@ __device__ void run_group(const XKernelParams &P, const XPair &pr, const XUnit &
 // buffer is zeroed before every run. A stripe waits only for stripes to its
 // right, claimed before it (stripes are tasks, rightmost first), which wait
 // for nobody to their left; the waits are bounded by the launch's timeout.
+// PIPED (tables with many rows per stripe): thread 0 loads the neighbour's
+// words of the NEXT flat row when a row starts and takes them at its end
+// (into S.cinb / S.fcb by row parity), so the round trip of the load leaves
+// the row's critical path; a stripe then stays a row behind its neighbour,
+// and a thread whose far column is exported by a stripe to the right loads
+// the next row's value after the scan barrier, a row before it is used. The
+// cost is a row of pipeline fill per stripe, which short tables do not repay.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long ld_tagged(const unsigned long long *p) {
     unsigned long long v;
@@ -706,7 +714,7 @@ __device__ __forceinline__ int tagged_value(const XKernelParams &P, const unsign
     return (unsigned)(v >> 32) == tag ? (int)(unsigned)v : wait_tagged(P, p, tag);
 }
 
-template <int W, bool UC>
+template <int W, bool UC, bool PIPED>
 __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit &u, int32_t *stk, WideShared &S,
                            int32_t *ring, int32_t *cache, int32_t *cnode, int s, int K, int X, int R,
                            const int32_t *expmap, unsigned long long *CR, unsigned long long *FC,
@@ -721,6 +729,10 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     static_assert(PF * SSLOT <= RING_INTS, "stripe ring");
     constexpr int SC = 32 * SROW <= CACHE_INTS ? 32 : 16 * SROW <= CACHE_INTS ? 16 : XTED_STACK_CACHE;
     static_assert(SC * SROW <= CACHE_INTS, "stripe stack window");
+    // the exported-value prefetch reads the next row's record, so rows i and
+    // i-1 must have landed when row i runs: one row less in flight
+    constexpr bool XPF = PIPED && PF >= 4;
+    constexpr int WAITN = XPF ? PF - 3 : PF - 2;
     const int gtid = threadIdx.x, lane = gtid & 31, warp = gtid >> 5;
     const XRun run = P.runs[u.run];
     const XChunk ch = P.chunks[u.chunk];
@@ -764,6 +776,10 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             }
         }
     }
+    unsigned xfar = 0;  // bit k: column k's far column is exported by a stripe to the right (prefetched)
+#pragma unroll
+    for (int k = 0; k < W; k++)
+        if (XPF && !((C.tcol >> k) & 1u) && C.fidx[k] < 0) xfar |= 1u << k;
     __syncthreads();  // the block's previous unit is done with cnode and S
 #pragma unroll
     for (int k = 0; k < W; k++)
@@ -789,6 +805,11 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
     const unsigned long long *cr_right = CR + (int64_t)(s + 1) * R, *fc_right = FC + (int64_t)(s + 1) * R;
     unsigned long long *cr_mine = CR + (int64_t)s * R, *fc_mine = FC + (int64_t)s * R;
     int tflat = 0, fc_next = 0;
+    if (PIPED && gtid == 0) {  // flat row 0's words; the rightmost stripe's carry stays infinite
+        S.cinb[0] = right ? wait_tagged(P, cr_right, 1u) : XTED_INF;
+        S.cinb[1] = XTED_INF;
+        S.fcb[0] = right ? wait_tagged(P, fc_right, 1u) : 0;
+    }
     for (int kr = run.kr_lo; kr < run.kr_hi; kr++) {
         const int i0 = P.krd[kr];
         const int imax = (rows[i0].y & XTED_ROW_ORL_MASK) + 1;
@@ -797,6 +818,10 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
 #pragma unroll
         for (int k = 0; k < W; k++) prev[k] = C.dend[k] * KC.ins;
         int sp = 0, lo = 0;
+        int pf_efl = -1;  // flat far row whose exported values pfw holds
+        unsigned long long pfw[W];
+#pragma unroll
+        for (int k = 0; k < W; k++) pfw[k] = 0;
         __syncthreads();  // the ring's and S's previous readers are done
         if (lane == 0) S.first[warp] = prev[0];
         if (gtid == 0) S.first[G] = right ? (w - C1) * KC.ins : 0;  // D[imax][C1]: the bottom border
@@ -813,7 +838,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             }
             cp_async_commit();
         }
-        cp_async_wait<PF - 2>();
+        cp_async_wait<WAITN>();
         __syncthreads();
         for (int i = imax - 1; i >= i0; i--, tflat++) {
             {
@@ -829,11 +854,12 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                 cp_async_commit();
             }
             // thread 0: the right neighbour's carry and first column of this
-            // row, checked at the scan barrier
+            // row, checked at the scan barrier (PIPED: of the next row, taken
+            // at the end of this one)
             unsigned long long cw = 0, fw = 0;
-            if (gtid == 0 && right) {
-                cw = ld_tagged(cr_right + tflat);
-                fw = ld_tagged(fc_right + tflat);
+            if (gtid == 0 && right && (!PIPED || tflat + 1 < R)) {
+                cw = ld_tagged(cr_right + tflat + (PIPED ? 1 : 0));
+                fw = ld_tagged(fc_right + tflat + (PIPED ? 1 : 0));
             }
             const int32_t *slot = ring + (i & (PF - 1)) * SSLOT;
             const int2 ri = *(const int2 *)(slot + SROW);
@@ -857,7 +883,8 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                     else if (C.fidx[k] >= 0) far = top[C.fidx[k]];
                     else {
                         const unsigned long long *ep = erow + (-1 - C.fidx[k]);
-                        far = tagged_value(P, ep, ld_tagged(ep), (unsigned)efl + 1);
+                        const unsigned long long v = ((xfar >> k) & 1u) && pf_efl == efl ? pfw[k] : ld_tagged(ep);
+                        far = tagged_value(P, ep, v, (unsigned)efl + 1);
                     }
                     int A = __viaddmin_s32(prev[k], KC.del, cur[k] + far);
                     A = min(A, bord1 | C.segor[k]);
@@ -872,7 +899,7 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
             }
             const int incl = warp_suffix_min(mine, lane);
             if (lane == 0) S.wtot[warp] = incl;
-            if (gtid == 0) {
+            if (!PIPED && gtid == 0) {
                 int cin = XTED_INF;
                 if (right) {
                     cin = tagged_value(P, cr_right + tflat, cw, (unsigned)tflat + 1);
@@ -887,7 +914,17 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                 // minimum of the warps to the right (one warp-wide reduction) and
                 // of the stripe to the right
                 const int mv = (lane > warp && lane < G) ? S.wtot[lane] : XTED_INF;
-                carry = min(carry, min(S.cin, __reduce_min_sync(FULLMASK, mv)));
+                carry = min(carry, min(PIPED ? S.cinb[tflat & 1] : S.cin, __reduce_min_sync(FULLMASK, mv)));
+            }
+            if (XPF && xfar && i > i0) {  // the next row's exported far values (its record has landed)
+                const int ron = ((const int2 *)(ring + ((i - 1) & (PF - 1)) * SSLOT + SROW))->y & XTED_ROW_ORL_MASK;
+                if (ron != imax - 1) {
+                    pf_efl = tbase + (imax - 1 - (ron + 1));
+                    const unsigned long long *prow = E + (int64_t)pf_efl * X;
+#pragma unroll
+                    for (int k = 0; k < W; k++)
+                        if ((xfar >> k) & 1u) pfw[k] = ld_tagged(prow + (-1 - C.fidx[k]));
+                }
             }
             int32_t *orow = dt_out + (int64_t)i * n;
 #pragma unroll
@@ -936,9 +973,19 @@ __device__ void run_stripe(const XKernelParams &P, const XPair &pr, const XUnit 
                 if (sp - lo > SC) lo = sp - SC;
             }
             // the next row's diagonal at C1: the right neighbour's first column of this row
-            if (gtid == 0 && right) S.first[G] = fc_next;
-            cp_async_wait<PF - 2>();  // row i-1 has landed (this thread's copies)
-            __syncthreads();          // ... and everyone's, the record and the stack push
+            if (gtid == 0 && right) {
+                if (!PIPED) {
+                    S.first[G] = fc_next;
+                } else {  // this row's first column, then the next row's words (slot (t+1)&1 is unread now)
+                    S.first[G] = S.fcb[tflat & 1];
+                    if (tflat + 1 < R) {
+                        S.cinb[(tflat + 1) & 1] = tagged_value(P, cr_right + tflat + 1, cw, (unsigned)tflat + 2);
+                        S.fcb[(tflat + 1) & 1] = tagged_value(P, fc_right + tflat + 1, fw, (unsigned)tflat + 2);
+                    }
+                }
+            }
+            cp_async_wait<WAITN>();  // row i-1 (with the prefetch: and i-2) has landed (this thread's copies)
+            __syncthreads();         // ... and everyone's, the records and the stack push
         }
     }
     cp_async_wait<0>();
@@ -957,12 +1004,15 @@ __device__ void run_striped(const XKernelParams &P, const XPair &pr, const XTask
     unsigned long long *CR = P.sbuf + X.buf_off;
     unsigned long long *FC = CR + (int64_t)X.K * X.R;
     unsigned long long *E = FC + (int64_t)X.K * X.R;
-    if (X.sww == 2)
-        run_stripe<2, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
+    // a table with many rows per stripe pipelines the hand-off (a row of fill per stripe)
+    if (X.sww == 2 && X.R >= XTED_STRIPE_PIPE_ROWS * X.K)
+        run_stripe<2, UC, true>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
+    else if (X.sww == 2)
+        run_stripe<2, UC, false>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
     else if (X.sww == 4)
-        run_stripe<4, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
+        run_stripe<4, UC, false>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
     else if (X.sww == 8)
-        run_stripe<8, UC>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
+        run_stripe<8, UC, false>(P, pr, u, stk, S, ring, cache, cnode, s, X.K, X.X, X.R, expmap, CR, FC, E);
     else if (threadIdx.x == 0)
         set_error(P, XTED_EINVAL, 13, X.sww, s);
 }

@@ -96,6 +96,7 @@ struct XUnit {
 #define XTED_STRIPE 2048        // widest stripe (8 columns per thread)
 #define XTED_STRIPE_MIN_W 2     // narrowest stripe: 2 columns per thread (512 columns)
 #define XTED_STRIPES_MAX 128    // stripes of one unit: a wider segment takes wider stripes
+#define XTED_STRIPE_PIPE_ROWS 32  // 512-column stripes of a unit with R >= this * K rows pipeline the hand-off
 #define XTED_STRIPE_MIN_CELLS_DEFAULT ((int64_t)1 << 20)
 
 struct XStripe {       // a striped unit
