@@ -148,6 +148,18 @@ int xted_run_prepared(xted_ctx *ctx, int32_t *out);
 
 int xted_last_stats(const xted_ctx *ctx, xted_stats *out);
 
+/* Replaces, for this context, the size-bucket granularity table compiled
+ * into the library (the autotuner's output) with nrows rows of four int32:
+ * max_n (> 0, strictly increasing), run_rows (>= 1), narrow_width (0..256)
+ * and half_width (-1..1024). Row k applies to trees with fewer than max_n
+ * nodes, the last row to all larger trees. nrows == 0 restores the compiled
+ * table. Applies, while the `tuned` option is set, to batches planned and
+ * corpora loaded after the call; a prepared batch keeps its plan. At most 8
+ * rows; a malformed table returns XTED_EINVAL and changes nothing. The
+ * autotuner uses it to time a whole table on mixed batches without a
+ * rebuild. */
+int xted_set_tune_table(xted_ctx *ctx, const int32_t *rows, int32_t nrows);
+
 /* All pairs of ntrees trees: out[i*ntrees + j] = TED(trees[i], trees[j]),
  * symmetric with a zero diagonal. The reference harness allocates this
  * matrix but fills only pair (0, 1) (X-TED_CPU/TED_test.cpp:26-47); here the

@@ -89,6 +89,32 @@ def test_forced_granularities(orientation, narrow_width, run_rows, half_width):
     assert list(got) == want
 
 
+def test_runtime_tune_table():
+    """xted_set_tune_table: a size-bucket table set on the context plans the
+    batches after it (here each bucket with a granularity of the forced cases
+    above), the distances stay the oracle's, a malformed table is refused with
+    XTED_EINVAL and leaves the table in force, and an empty one restores the
+    compiled table."""
+    rng = random.Random(4242)
+    pairs = []
+    for _ in range(24):
+        pairs.append((_rand_tree(rng, rng.choice([0, 1, 2, 5, 30, 90, 200, 420]), rng.randint(1, 6), rng.randrange(3)),
+                      _rand_tree(rng, rng.choice([1, 3, 8, 50, 130, 300, 700, 1100]), rng.randint(1, 6),
+                                 rng.randrange(3))))
+    want = [oracle.distance(a, b) for a, b in pairs]
+    with xted.Context() as c:
+        c.set_tune_table([(40, 3, 7, 100), (300, 1, 0, -1), (1 << 30, 64, 256, 512)])
+        assert list(c.distance_batch(pairs)) == want
+        for bad in ([(0, 1, 1, 1)], [(50, 1, 1, 1), (50, 2, 2, 2)], [(1 << 30, 0, 1, 1)], [(1 << 30, 1, 257, 1)],
+                    [(1 << 30, 1, 1, 1025)], [(1 << 30, 1, 1, -2)], [(k + 1, 1, 1, 1) for k in range(9)]):
+            with pytest.raises(xted.XtedError) as e:
+                c.set_tune_table(bad)
+            assert e.value.code == xted.XTED_EINVAL
+        assert list(c.distance_batch(pairs)) == want
+        c.set_tune_table([])
+        assert list(c.distance_batch(pairs)) == want
+
+
 def test_brute_force_small(ctx):
     rng = random.Random(3)
     pairs = [(_rand_tree(rng, rng.randint(0, 9), rng.randint(1, 3), rng.randrange(3)),

@@ -164,6 +164,34 @@ def test_tune_table_well_formed():
         assert 1 <= int(rr) <= 4096 and 0 <= int(nw) <= 256 and int(hw) <= 1024
 
 
+def test_autotune_guard_keeps_rows_that_help_every_batch():
+    """The autotuner's mixed-batch guard (xted.autotune.guarded_merge) on a fake
+    timer: a proposed row is taken only if the batches get faster in total and
+    none slows by more than the tolerance, one bucket at a time."""
+    from xted import autotune as A
+    current = A.read_header()
+    assert [r[0] for r in current] == [b[0] for b in A.BUCKETS]
+    # the (1,024, 2,048, 4,096)-pair times each proposed row would cause, as deltas in ms
+    effect = {1: (-2.0, -1.0, -3.0),   # faster everywhere: taken
+              2: (+5.0, +1.0, -10.0),  # faster in total, 5% slower on 1,024 pairs (coarse tasks): refused
+              4: (-0.5, +0.1, -0.5)}   # 0.1 ms slower on 2,048 pairs, inside 1%: taken
+    proposed = [r if k not in effect else (r[0], r[1] * 2, r[2], r[3]) for k, r in enumerate(current)]
+
+    def fake(rows):
+        t = [100.0, 125.0, 230.0]
+        for k, d in effect.items():
+            if tuple(rows[k]) == tuple(proposed[k]):
+                t = [a + b for a, b in zip(t, d)]
+        return t
+    table, times, taken = A.guarded_merge(current, proposed, fake, tol=0.01)
+    assert taken == [1, 4]
+    assert table[2] == current[2] and table[1] == proposed[1] and table[4] == proposed[4]
+    assert times == fake(table)
+    assert A.accept([1.0, 1.0], [0.9, 1.009]) and not A.accept([1.0, 1.0], [0.8, 1.02])
+    with pytest.raises(ValueError):
+        A.guarded_merge(current, proposed[:-1], fake)
+
+
 def _bracket_cases():
     import gzip
     import json

@@ -23,6 +23,7 @@
 #include "../../include/xted.h"
 #include "ctx.h"
 #include "plan.h"
+#include "tune_table.h"
 
 namespace xted {
 int dp_occupancy(int *blocks_per_sm);
@@ -281,6 +282,15 @@ int ctx_run(xted_ctx *c, int32_t *out, bool allow_graph) {
     return XTED_OK;
 }
 
+const XTuneRow *ctx_tune_table(const xted_ctx *c, int *nrows) {
+    if (c->ntune > 0) {
+        *nrows = c->ntune;
+        return c->tune;
+    }
+    *nrows = kTuneRows;
+    return kTuneTable;
+}
+
 void fill_stats(xted_ctx *c, double plan_ms) {
     c->stats.pairs = c->npairs;
     c->stats.cells = c->plan_cells;
@@ -490,6 +500,19 @@ int xted_test_fault(xted_ctx *c, int32_t kind) {
 int xted_last_stats(const xted_ctx *c, xted_stats *out) {
     if (!c || !out) return XTED_EINVAL;
     *out = c->stats;
+    return XTED_OK;
+}
+
+int xted_set_tune_table(xted_ctx *c, const int32_t *rows, int32_t nrows) {
+    if (!c || nrows < 0 || nrows > XTED_TUNE_ROWS || (nrows > 0 && !rows)) return XTED_EINVAL;
+    for (int k = 0; k < nrows; k++) {
+        const int32_t *r = rows + 4 * k;
+        if (r[0] <= 0 || (k > 0 && r[0] <= rows[4 * (k - 1)]) || r[1] < 1 || r[2] < 0 || r[2] > XTED_NARROW_MAX ||
+            r[3] < -1 || r[3] > XTED_HALF_MAX)
+            return XTED_EINVAL;
+    }
+    for (int k = 0; k < nrows; k++) c->tune[k] = XTuneRow{rows[4 * k], rows[4 * k + 1], rows[4 * k + 2], rows[4 * k + 3]};
+    c->ntune = nrows > 0 ? nrows : -1;
     return XTED_OK;
 }
 

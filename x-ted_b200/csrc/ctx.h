@@ -43,6 +43,9 @@ struct xted_ctx {
     xted_stats stats{};
     int32_t err_info[4] = {0, 0, 0, 0};
     int32_t fault = 0;  // armed test fault (xted_test_fault), taken by the next batch or posted query
+    // size-bucket granularity set by xted_set_tune_table (ntune < 0: the compiled table)
+    XTuneRow tune[XTED_TUNE_ROWS] = {};
+    int32_t ntune = -1;
     xted::ServeState *serve = nullptr;  // owned; released by serve_shutdown
     // device planning: host-side bookkeeping of the current batch
     std::unordered_map<xted::TreeKey, int, xted::TreeKeyHash> tree_ids;
@@ -74,6 +77,9 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
 int ctx_run(xted_ctx *c, int32_t *out, bool allow_graph);
 void ctx_drop_graph(xted_ctx *c);
 void fill_stats(xted_ctx *c, double plan_ms);
+// The size-bucket granularity table the context plans with: the one set by
+// xted_set_tune_table, else the autotuned table compiled into the library.
+const XTuneRow *ctx_tune_table(const xted_ctx *c, int *nrows);
 void serve_shutdown(xted_ctx *c);
 std::mutex &serve_mutex(xted_ctx *c);  // the serving state's lock (c->serve must be set)
 

@@ -24,7 +24,6 @@
 
 #include "ctx.h"
 #include "plan_core.h"
-#include "tune_table.h"
 
 namespace xted {
 
@@ -717,8 +716,11 @@ int dev_plan(xted_ctx *c, const xted_tree *a, const xted_tree *b, int32_t npairs
     P.narrow_width = c->opts.narrow_width;
     P.half_width = c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width;
     P.ntune = 0;
-    if (c->opts.tuned)
-        for (int k = 0; k < kTuneRows && k < XTED_TUNE_ROWS; k++) P.tune[P.ntune++] = kTuneTable[k];
+    if (c->opts.tuned) {
+        int nt = 0;
+        const XTuneRow *tt = ctx_tune_table(c, &nt);
+        for (int k = 0; k < nt && k < XTED_TUNE_ROWS; k++) P.tune[P.ntune++] = tt[k];
+    }
     DPair *d_pairs = cv.take<DPair>((size_t)npairs);
     XPair *d_xpairs = cv.take<XPair>((size_t)npairs);
     int32_t *d_trivial = cv.take<int32_t>((size_t)npairs);

@@ -46,7 +46,6 @@
 #include "plan.h"
 #include "plan_core.h"
 #include "serve_plan.h"
-#include "tune_table.h"
 
 namespace xted {
 cudaError_t launch_dp(const XKernelParams &P, int grid, cudaStream_t s);
@@ -756,9 +755,11 @@ int load(xted_ctx *c, ServeState *s, const xted_tree *tr, int32_t ntrees) {
         for (int v2 = 0; v2 < tr[t].n; v2++)
             d[(size_t)v2] = s->dense.emplace(tr[t].labels[v2], (int32_t)s->dense.size()).first->second;
     }
+    int ntune = 0;
+    const XTuneRow *tune = ctx_tune_table(c, &ntune);
     serve_pools_build(s->pools, tr, T, S, Qm, c->opts.run_rows, c->opts.narrow_width,
                       c->opts.half_width == 0 ? XTED_HALF_DEFAULT : c->opts.half_width,
-                      c->opts.tuned ? kTuneTable : nullptr, c->opts.tuned ? kTuneRows : 0);
+                      c->opts.tuned ? tune : nullptr, c->opts.tuned ? ntune : 0);
     const ServePools &H = s->pools;
     const size_t n2 = H.node.size();
     // device memory

@@ -109,6 +109,7 @@ def lib():
             "xted_parse_bracket": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int32, _i32p, _i32p,
                                                   _i64p, _i32p, _i32p, _i64p]),
             "xted_test_fault": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+            "xted_set_tune_table": (ctypes.c_int, [ctypes.c_void_p, _i32p, ctypes.c_int32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

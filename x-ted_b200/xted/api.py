@@ -124,6 +124,15 @@ class Context:
         _lib.check(_lib.lib().xted_run_prepared(self._h, out.ctypes.data_as(_lib._i32p)), "xted_run_prepared")
         return out[:self._prepared_n]
 
+    def set_tune_table(self, rows: Sequence[Tuple[int, int, int, int]]) -> None:
+        """Plans later batches and corpora with this size-bucket table instead
+        of the compiled one (xted_set_tune_table): rows of (max_n, run_rows,
+        narrow_width, half_width), max_n strictly increasing; an empty list
+        restores the compiled table. Needs the context's `tuned` option."""
+        arr = np.ascontiguousarray(np.asarray(list(rows), np.int32).reshape(-1, 4))
+        _lib.check(_lib.lib().xted_set_tune_table(self._h, arr.ctypes.data_as(_lib._i32p), int(arr.shape[0])),
+                   "xted_set_tune_table")
+
     def test_fault(self, kind: int = _lib.XTED_FAULT_HOLD_PAIR) -> None:
         """Arms one host-side fault for the next batch call or posted serving
         query (xted_test_fault): with XTED_FAULT_HOLD_PAIR one pair's first

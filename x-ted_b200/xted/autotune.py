@@ -8,6 +8,14 @@ chunk, widest half-block chunk) and keeps the fastest. The result is written as
 each tree with the row of its size bucket unless the caller sets the
 granularity explicitly.
 
+A bucket's best row is tuned on a batch large enough to fill the GPU, which
+favours coarse tasks; a smaller batch is bound by its last levels, where coarse
+tasks leave blocks idle. So before the header is written each changed row is
+tried on mixed batches of several sizes (``MIXED_SIZES``, through
+``Context.set_tune_table``, no rebuild) against the table already in the
+header, and kept only if the batches are faster in total and none of them is
+slower by more than ``--tolerance``.
+
     python -m xted.autotune            # needs an sm_100 GPU; rebuild afterwards
     python -m xted.autotune --quick    # fewer candidates, for a smoke run
 """
@@ -34,6 +42,7 @@ BUCKETS = [  # (max_n, tree sizes drawn log-uniformly from [lo, hi), pairs in th
     (2048, 1024, 2048, 384),
     (1 << 30, 2048, 4096, 96),
 ]
+MIXED_SIZES = (1024, 2048, 4096)  # pairs of gen.mixed_batch(n, seed=4) the guard times
 RUN_ROWS = [16, 32, 64, 128]
 NARROW = [128, 256]
 HALF = [-1, 384, 512, 768, 1024]
@@ -65,6 +74,62 @@ def time_config(pairs, run_rows, narrow, half, reps=2, device=0):
     return best
 
 
+def read_header(path=HEADER):
+    """The (max_n, run_rows, narrow_width, half_width) rows of a tune_table.h."""
+    rows = []
+    for line in open(path):
+        t = line.strip()
+        if t.startswith("{") and t.endswith("},"):
+            f = [x.strip() for x in t[1:-2].split(",")]
+            rows.append((1 << 30 if f[0] == "1 << 30" else int(f[0]), int(f[1]), int(f[2]), int(f[3])))
+    return rows
+
+
+def accept(base, cand, tol=0.01):
+    """A table is better when the batches are faster in total and none is slower by more than tol."""
+    return sum(cand) < sum(base) and all(c <= b * (1 + tol) for b, c in zip(base, cand))
+
+
+def guarded_merge(current, proposed, time_fn, tol=0.01):
+    """Adopts the proposed rows into the current table one bucket at a time, each
+    only if accept() holds on time_fn(table) (a list of batch times); returns the
+    table, its times and the indices of the rows taken from the proposal."""
+    if [r[0] for r in current] != [r[0] for r in proposed]:
+        raise ValueError("the two tables have different size buckets")
+    table = [tuple(r) for r in current]
+    base = time_fn(table)
+    taken = []
+    for k, row in enumerate(proposed):
+        if tuple(row) == table[k]:
+            continue
+        trial = table[:k] + [tuple(row)] + table[k + 1:]
+        t = time_fn(trial)
+        if accept(base, t, tol):
+            table, base = trial, t
+            taken.append(k)
+    return table, base, taken
+
+
+def mixed_timer(sizes=MIXED_SIZES, reps=2, device=0):
+    """time_fn for guarded_merge: best DP time of each mixed batch under a table."""
+    batches = [gen.mixed_batch(n, seed=4) for n in sizes]
+
+    def time_fn(rows):
+        out = []
+        with Context(device=device) as c:
+            c.set_tune_table(rows)
+            for pairs in batches:
+                c.prepare_batch(pairs)
+                c.run_prepared()
+                best = math.inf
+                for _ in range(reps):
+                    c.run_prepared()
+                    best = min(best, c.stats()["dp_ms"])
+                out.append(best)
+        return out
+    return time_fn
+
+
 def write_header(rows, notes, path=HEADER):
     lines = [
         "// tune_table.h -- granularity per tree-size bucket, written by",
@@ -88,6 +153,9 @@ def main(argv=None):
     ap.add_argument("--quick", action="store_true", help="default-adjacent candidates only")
     ap.add_argument("--out", default=HEADER)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--tolerance", type=float, default=0.01,
+                    help="largest slowdown of one mixed batch a changed row may cause")
+    ap.add_argument("--no-guard", action="store_true", help="write the per-bucket bests unchecked")
     args = ap.parse_args(argv)
     cands = list(itertools.product(RUN_ROWS, NARROW, HALF))
     if args.quick:
@@ -108,6 +176,11 @@ def main(argv=None):
         rows.append((max_n, best[1], best[2], best[3]))
         notes.append(f"sizes [{lo}, {hi}), {npairs} pairs: best {best[0]:.2f} ms (run_rows {best[1]}, narrow "
                      f"{best[2]}, half {best[3]})" + (f", untuned default {default[0]:.2f} ms" if default else ""))
+    if not args.no_guard:
+        current = read_header(args.out if os.path.exists(args.out) else HEADER)
+        rows, times, taken = guarded_merge(current, rows, mixed_timer(device=args.device), args.tolerance)
+        notes.append(f"mixed batches {list(MIXED_SIZES)} pairs: {[round(t, 2) for t in times]} ms; "
+                     f"rows taken from this run: {taken} (the others kept from the previous table)")
     notes.append(f"{len(cands)} candidates per bucket, {time.time() - t_all:.0f} s on "
                  f"{os.environ.get('XTED_TUNE_GPU', 'a B200')}")
     write_header(rows, notes, args.out)
