@@ -178,9 +178,17 @@ def main(argv=None):
                      f"{best[2]}, half {best[3]})" + (f", untuned default {default[0]:.2f} ms" if default else ""))
     if not args.no_guard:
         current = read_header(args.out if os.path.exists(args.out) else HEADER)
-        rows, times, taken = guarded_merge(current, rows, mixed_timer(device=args.device), args.tolerance)
-        notes.append(f"mixed batches {list(MIXED_SIZES)} pairs: {[round(t, 2) for t in times]} ms; "
-                     f"rows taken from this run: {taken} (the others kept from the previous table)")
+        timer, seen = mixed_timer(device=args.device), []
+
+        def timed(table):
+            t = timer(table)
+            seen.append(t)
+            print(json.dumps({"mixed_pairs": list(MIXED_SIZES), "table": table, "dp_ms": t}), flush=True)
+            return t
+        rows, times, taken = guarded_merge(current, rows, timed, args.tolerance)
+        notes.append(f"mixed batches of {list(MIXED_SIZES)} pairs: {[round(t, 2) for t in seen[0]]} ms with the "
+                     f"previous table, {[round(t, 2) for t in times]} ms with this one; rows taken from this "
+                     f"run: {taken} (the others kept)")
     notes.append(f"{len(cands)} candidates per bucket, {time.time() - t_all:.0f} s on "
                  f"{os.environ.get('XTED_TUNE_GPU', 'a B200')}")
     write_header(rows, notes, args.out)
