@@ -192,6 +192,17 @@ def test_autotune_guard_keeps_rows_that_help_every_batch():
         A.guarded_merge(current, proposed[:-1], fake)
 
 
+def test_autotune_header_round_trip(tmp_path):
+    """What the autotuner writes is what it (and the library build) reads back."""
+    from xted import autotune as A
+    rows = [(128, 16, 128, -1), (1024, 64, 256, 768), (1 << 30, 128, 128, 512)]
+    path = str(tmp_path / "tune_table.h")
+    A.write_header(rows, ["a note"], path)
+    assert A.read_header(path) == rows
+    src = open(path).read()
+    assert "// a note" in src and "static const XTuneRow kTuneTable[]" in src
+
+
 def _bracket_cases():
     import gzip
     import json
